@@ -1,0 +1,57 @@
+// pb_internal.h -- declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pb_b200.h"
+#include "pb_device.cuh"
+
+namespace pb {
+
+// Records an error message for pb_last_error() and returns `code`.
+PbStatus set_error(PbStatus code, const char *fmt, ...);
+
+// Checks the last launch; on failure records the CUDA error text.
+PbStatus check_launch(const char *what);
+PbStatus check_cuda(cudaError_t e, const char *what);
+
+// cos/sin of the six smoothing directions, angle i*pi/3 in FP32 as the
+// reference forms it (IMPTClasses.cu:177), evaluated on the host.
+void smooth_dirs(float *c, float *s);
+
+int ray_step_cap(const PbGrid &g);
+
+PbStatus launch_rlsp(const float *hu, int64_t n, const double *xh,
+                     const double *yh, int m, float *out, cudaStream_t st);
+
+PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
+                    const PbBeamGeom *beams, int n_beams, float *raw, float *wet, int *status,
+                    cudaStream_t st);
+
+PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st);
+PbStatus texture_update(uint64_t h, const float *rlsp, cudaStream_t st);
+bool texture_matches(uint64_t h, const PbGrid &g);
+cudaTextureObject_t texture_object(uint64_t h);
+void texture_destroy(uint64_t h);
+
+PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
+                     const float *wet, const PbLayer *layers,
+                     const float *geo, const float *mu, float scale,
+                     float *dose, float *beam_dose, cudaStream_t st);
+
+PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
+                        const float *wet, const PbLayer *layers,
+                        const float *geo, const float *w, float scale,
+                        float *grad, cudaStream_t st);
+
+PbStatus launch_objective(const float *dose, const float *presc,
+                          const float *weight, int64_t n, double *obj,
+                          float *resid, void *work, cudaStream_t st);
+size_t objective_work_size();
+
+PbStatus launch_count_pairs(const PbGrid &g, const PbBeam *beams, int n_beams,
+                            const float *wet, const PbLayer *layers,
+                            unsigned long long *count, cudaStream_t st);
+
+}  // namespace pb

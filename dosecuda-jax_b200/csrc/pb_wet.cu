@@ -1,0 +1,357 @@
+// pb_wet.cu -- HU -> RLSP conversion and the water-equivalent-thickness
+// (WET) pass: ray trace toward the source and lateral smoothing.
+//
+//   HU -> RLSP            DoseCUDA/plan_impt.py:158-168 (numpy.interp)
+//   ray trace             DoseCUDA/dose_kernels/CudaClasses.cu:180-228
+//   smoothing             DoseCUDA/dose_kernels/IMPTClasses.cu:139-202
+//
+// Layout: every volume is x-fastest; one thread per voxel; blocks are 8x4x4
+// voxel bricks so that a warp covers an 8x4 patch whose rays have similar
+// lengths whatever the beam direction, and each row of 8 voxels is one
+// 32-byte sector.  Several beams share one launch (grid z = z-bricks x beams).
+#include <new>
+
+#include "pb_internal.h"
+
+namespace pb {
+
+// ------------------------------------------------------------------ HU->RLSP
+
+struct HuCurve {
+    double x[PB_MAX_CURVE];
+    double y[PB_MAX_CURVE];
+    double slope[PB_MAX_CURVE];
+    int n;
+};
+
+// numpy.interp: left of the first point -> first value, right of the last
+// -> last value, on a knot -> the knot's value, else slope*(x-x_j)+y_j in
+// FP64 with no contraction; the result is rounded to FP32 as np.array(...,
+// dtype=single) does.
+__global__ void k_rlsp(const float *__restrict__ hu, int64_t n,
+                       const __grid_constant__ HuCurve c,
+                       float *__restrict__ out)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const double x = (double)hu[q];
+        double r;
+        if (x != x) {
+            r = x;
+        } else if (x < c.x[0]) {
+            r = c.y[0];
+        } else if (x > c.x[c.n - 1]) {
+            r = c.y[c.n - 1];
+        } else {
+            int j = 0;
+            while (j + 1 < c.n && c.x[j + 1] <= x) ++j;
+            if (j == c.n - 1 || c.x[j] == x) {
+                r = c.y[j];
+            } else {
+                r = __dadd_rn(__dmul_rn(c.slope[j], __dsub_rn(x, c.x[j])), c.y[j]);
+            }
+        }
+        out[q] = __double2float_rn(r);
+    }
+}
+
+PbStatus launch_rlsp(const float *hu, int64_t n, const double *xh,
+                     const double *yh, int m, float *out, cudaStream_t st)
+{
+    HuCurve c;
+    c.n = m;
+    for (int i = 0; i < m; ++i) {
+        c.x[i] = xh[i];
+        c.y[i] = yh[i];
+    }
+    for (int i = 0; i + 1 < m; ++i) c.slope[i] = (yh[i + 1] - yh[i]) / (xh[i + 1] - xh[i]);
+    c.slope[m - 1] = 0.0;
+    if (n == 0) return PB_OK;
+    int blocks = (int)((n + 255) / 256);
+    const int cap = 148 * 16;
+    if (blocks > cap) blocks = cap;
+    k_rlsp<<<blocks, 256, 0, st>>>(hu, n, c, out);
+    return check_launch("k_rlsp");
+}
+
+// ----------------------------------------------------------------- ray trace
+
+// Trilinear sample at voxel-index coordinates with 0 outside the grid
+// (the reference samples a border-0 texture with linear filtering).
+__device__ __forceinline__ float trilinear(const float *__restrict__ rho,
+                                           int nx, int ny, int nz, float xb,
+                                           float yb, float zb)
+{
+    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
+    const int i0 = (int)fx, j0 = (int)fy, k0 = (int)fz;
+    const float ax = xb - fx, ay = yb - fy, az = zb - fz;
+    const int64_t sy = nx, sz = (int64_t)nx * ny;
+    float c000, c100, c010, c110, c001, c101, c011, c111;
+    if (i0 >= 0 && j0 >= 0 && k0 >= 0 && i0 + 1 < nx && j0 + 1 < ny && k0 + 1 < nz) {
+        const float *p = rho + i0 + sy * j0 + sz * k0;
+        c000 = __ldg(p);
+        c100 = __ldg(p + 1);
+        c010 = __ldg(p + sy);
+        c110 = __ldg(p + sy + 1);
+        c001 = __ldg(p + sz);
+        c101 = __ldg(p + sz + 1);
+        c011 = __ldg(p + sz + sy);
+        c111 = __ldg(p + sz + sy + 1);
+    } else {
+        const bool xi0 = i0 >= 0 && i0 < nx, xi1 = i0 + 1 >= 0 && i0 + 1 < nx;
+        const bool yj0 = j0 >= 0 && j0 < ny, yj1 = j0 + 1 >= 0 && j0 + 1 < ny;
+        const bool zk0 = k0 >= 0 && k0 < nz, zk1 = k0 + 1 >= 0 && k0 + 1 < nz;
+        auto at = [&](bool ok, int i, int j, int k) -> float {
+            return ok ? __ldg(rho + i + sy * j + sz * k) : 0.0f;
+        };
+        c000 = at(xi0 && yj0 && zk0, i0, j0, k0);
+        c100 = at(xi1 && yj0 && zk0, i0 + 1, j0, k0);
+        c010 = at(xi0 && yj1 && zk0, i0, j0 + 1, k0);
+        c110 = at(xi1 && yj1 && zk0, i0 + 1, j0 + 1, k0);
+        c001 = at(xi0 && yj0 && zk1, i0, j0, k0 + 1);
+        c101 = at(xi1 && yj0 && zk1, i0 + 1, j0, k0 + 1);
+        c011 = at(xi0 && yj1 && zk1, i0, j0 + 1, k0 + 1);
+        c111 = at(xi1 && yj1 && zk1, i0 + 1, j0 + 1, k0 + 1);
+    }
+    const float c00 = fmaf(ax, c100 - c000, c000);
+    const float c10 = fmaf(ax, c110 - c010, c010);
+    const float c01 = fmaf(ax, c101 - c001, c001);
+    const float c11 = fmaf(ax, c111 - c011, c011);
+    const float c0 = fmaf(ay, c10 - c00, c00);
+    const float c1 = fmaf(ay, c11 - c01, c01);
+    return fmaf(az, c1 - c0, c0);
+}
+
+// Raw WET (cm) per voxel: samples every 1 mm from the voxel toward the
+// source while the texture coordinate stays inside [0, n); WET = -0.05 +
+// 0.1 * sum(max(RLSP, 0)).  The sum is carried in FP64 (FP32 partials of 16
+// samples).  A ray that exceeds the grid-diagonal step cap stops and raises
+// PB_ERR_RAY_CAP in *status.
+//
+// TEX = true samples RLSP through a border-0, linearly filtered 3-D texture
+// and forms the ray direction with rnorm3df, as the reference does
+// (CudaClasses.cuh:41-52, TextureClasses.cu:14-41), so the samples are the
+// reference's own.  TEX = false interpolates with exact FP32 trilinear
+// weights from global memory and forms the direction in FP64, the CPU
+// oracle's arithmetic.
+template <bool TEX>
+__global__ void __launch_bounds__(128)
+k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
+           const __grid_constant__ BeamGeomSet bs, int zbricks, int cap,
+           float *__restrict__ raw, int *status)
+{
+    const int b = blockIdx.z / zbricks;
+    const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
+    const int j = blockIdx.y * 4 + threadIdx.y;
+    const int i = blockIdx.x * 8 + threadIdx.x;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const PbBeamGeom &B = bs.b[b];
+    float px, py, pz, ux, uy, uz;
+    vox_mm(B, g.spacing, i, j, k, px, py, pz);
+    if (TEX) {
+        ux = __fsub_rn(B.src[0], px);
+        uy = __fsub_rn(B.src[1], py);
+        uz = __fsub_rn(B.src[2], pz);
+        const float nrm = rnorm3df(ux, uy, uz);
+        ux = __fmul_rn(ux, nrm);
+        uy = __fmul_rn(uy, nrm);
+        uz = __fmul_rn(uz, nrm);
+    } else {
+        unit_to_source(B, px, py, pz, ux, uy, uz);
+    }
+    const float inv_s = __fdiv_rn(1.0f, g.spacing);
+    const float fnx = (float)g.nx, fny = (float)g.ny, fnz = (float)g.nz;
+    double acc = 0.0;
+    float part = 0.0f;
+    int inpart = 0;
+    float t = 0.0f;
+    for (int n = 0;; ++n) {
+        const float qx = __fmaf_rn(ux, t, px);
+        const float qy = __fmaf_rn(uy, t, py);
+        const float qz = __fmaf_rn(uz, t, pz);
+        const float x = __fmaf_rn(inv_s, __fadd_rn(qx, B.iso[0]), 0.5f);
+        const float y = __fmaf_rn(inv_s, __fadd_rn(qy, B.iso[1]), 0.5f);
+        const float z = __fmaf_rn(inv_s, __fadd_rn(qz, B.iso[2]), 0.5f);
+        if (!(x >= 0.0f && x < fnx && y >= 0.0f && y < fny && z >= 0.0f && z < fnz))
+            break;
+        if (n >= cap) {
+            if (status) atomicOr(status, (int)PB_ERR_RAY_CAP);
+            break;
+        }
+        float r;
+        if (TEX)
+            r = tex3D<float>(tex, x, y, z);
+        else
+            r = trilinear(rho, g.nx, g.ny, g.nz, __fsub_rn(x, 0.5f), __fsub_rn(y, 0.5f),
+                          __fsub_rn(z, 0.5f));
+        part += fmaxf(r, 0.0f);
+        if (++inpart == 16) {
+            acc += (double)part;
+            part = 0.0f;
+            inpart = 0;
+        }
+        t = __fadd_rn(t, 1.0f);
+    }
+    acc += (double)part;
+    const int64_t V = (int64_t)g.nx * g.ny * g.nz;
+    const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
+    raw[b * V + v] = __double2float_rn(fma(0.1, acc, -0.05));
+}
+
+// Smoothed WET: mean of the voxel's raw WET and the in-grid nearest-voxel
+// samples at 1..9 mm along six BEV-lateral directions, taking radius dr
+// while dr < 10*WET(cm) (IMPTClasses.cu:166-198).
+__global__ void __launch_bounds__(128)
+k_smooth(const float *__restrict__ raw, PbGrid g,
+         const __grid_constant__ BeamGeomSet bs, SmoothDirs d, int zbricks,
+         float *__restrict__ wet)
+{
+    const int b = blockIdx.z / zbricks;
+    const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
+    const int j = blockIdx.y * 4 + threadIdx.y;
+    const int i = blockIdx.x * 8 + threadIdx.x;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const PbBeamGeom &B = bs.b[b];
+    const int64_t V = (int64_t)g.nx * g.ny * g.nz;
+    const float *R = raw + b * V;
+    const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
+    const float center = R[v];
+    float sum = center;
+    int n = 1;
+    float px, py, pz, hx, hy, hz;
+    vox_mm(B, g.spacing, i, j, k, px, py, pz);
+    image_to_head(B, px, py, pz, hx, hy, hz);
+    const float lim = __fmul_rn(center, 10.0f);
+    const float s = g.spacing;
+    for (int dd = 0; dd < 6; ++dd) {
+        const float c = d.c[dd], sn = d.s[dd];
+        for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f)) {
+            float qx, qy, qz;
+            head_to_image(B, __fadd_rn(hx, __fmul_rn(dr, c)),
+                          __fadd_rn(hy, __fmul_rn(dr, sn)), hz, qx, qy, qz);
+            const int ii = (int)roundf(__fdiv_rn(__fadd_rn(qx, B.iso[0]), s));
+            const int jj = (int)roundf(__fdiv_rn(__fadd_rn(qy, B.iso[1]), s));
+            const int kk = (int)roundf(__fdiv_rn(__fadd_rn(qz, B.iso[2]), s));
+            if (ii >= 0 && ii < g.nx && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz) {
+                sum += __ldg(R + ii + (int64_t)g.nx * (jj + (int64_t)g.ny * kk));
+                n += 1;
+            }
+        }
+    }
+    wet[b * V + v] = __fdiv_rn(sum, (float)n);
+}
+
+int ray_step_cap(const PbGrid &g)
+{
+    const double diag = g.spacing * sqrt((double)g.nx * g.nx + (double)g.ny * g.ny +
+                                         (double)g.nz * g.nz);
+    return (int)ceil(diag) + 2;
+}
+
+PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
+                    const PbBeamGeom *beams, int n_beams, float *raw, float *wet, int *status,
+                    cudaStream_t st)
+{
+    BeamGeomSet bs;
+    for (int b = 0; b < n_beams; ++b) bs.b[b] = beams[b];
+    SmoothDirs d;
+    smooth_dirs(d.c, d.s);
+    const int zb = (g.nz + 3) / 4;
+    dim3 block(8, 4, 4);
+    dim3 grid((g.nx + 7) / 8, (g.ny + 3) / 4, zb * n_beams);
+    if (tex)
+        k_raytrace<true><<<grid, block, 0, st>>>(rlsp, tex, g, bs, zb, ray_step_cap(g), raw,
+                                                 status);
+    else
+        k_raytrace<false><<<grid, block, 0, st>>>(rlsp, tex, g, bs, zb, ray_step_cap(g), raw,
+                                                  status);
+    PbStatus s = check_launch("k_raytrace");
+    if (s != PB_OK) return s;
+    k_smooth<<<grid, block, 0, st>>>(raw, g, bs, d, zb, wet);
+    return check_launch("k_smooth");
+}
+
+// 3-D texture over an RLSP volume: float channel, linear filter, border 0,
+// unnormalised coordinates (TextureClasses.cu:14-41).
+struct RlspTexture {
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    int nx = 0, ny = 0, nz = 0;
+};
+
+PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st)
+{
+    RlspTexture *t = new (std::nothrow) RlspTexture;
+    if (!t) return set_error(PB_ERR_NOMEM, "host allocation failed");
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+    cudaExtent ext = make_cudaExtent(g.nx, g.ny, g.nz);
+    PbStatus s = check_cuda(cudaMalloc3DArray(&t->arr, &ch, ext, cudaArrayDefault),
+                            "cudaMalloc3DArray");
+    if (s != PB_OK) {
+        delete t;
+        return s;
+    }
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<float *>(rlsp), sizeof(float) * (size_t)g.nx, g.nx,
+                                   g.ny);
+    p.dstArray = t->arr;
+    p.extent = ext;
+    p.kind = cudaMemcpyDeviceToDevice;
+    s = check_cuda(cudaMemcpy3DAsync(&p, st), "cudaMemcpy3DAsync");
+    if (s == PB_OK) {
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = t->arr;
+        cudaTextureDesc td{};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        s = check_cuda(cudaCreateTextureObject(&t->tex, &rd, &td, nullptr),
+                       "cudaCreateTextureObject");
+    }
+    if (s != PB_OK) {
+        cudaFreeArray(t->arr);
+        delete t;
+        return s;
+    }
+    t->nx = g.nx;
+    t->ny = g.ny;
+    t->nz = g.nz;
+    *out = reinterpret_cast<uint64_t>(t);
+    return PB_OK;
+}
+
+PbStatus texture_update(uint64_t h, const float *rlsp, cudaStream_t st)
+{
+    RlspTexture *t = reinterpret_cast<RlspTexture *>(h);
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<float *>(rlsp), sizeof(float) * (size_t)t->nx, t->nx,
+                                   t->ny);
+    p.dstArray = t->arr;
+    p.extent = make_cudaExtent(t->nx, t->ny, t->nz);
+    p.kind = cudaMemcpyDeviceToDevice;
+    return check_cuda(cudaMemcpy3DAsync(&p, st), "cudaMemcpy3DAsync");
+}
+
+bool texture_matches(uint64_t h, const PbGrid &g)
+{
+    const RlspTexture *t = reinterpret_cast<const RlspTexture *>(h);
+    return t && t->nx == g.nx && t->ny == g.ny && t->nz == g.nz;
+}
+
+cudaTextureObject_t texture_object(uint64_t h)
+{
+    return h ? reinterpret_cast<const RlspTexture *>(h)->tex : 0;
+}
+
+void texture_destroy(uint64_t h)
+{
+    RlspTexture *t = reinterpret_cast<RlspTexture *>(h);
+    if (!t) return;
+    cudaDestroyTextureObject(t->tex);
+    cudaFreeArray(t->arr);
+    delete t;
+}
+
+}  // namespace pb

@@ -1,0 +1,173 @@
+"""ctypes binding of libpb_b200.so (declared in include/pb_b200.h).
+
+The shared library is built in-tree by ``make -C dosecuda-jax_b200/csrc``
+(or ``__graft_entry__.build()``).  Importing this module loads it; a missing
+library raises ImportError -- there is no CPU fallback for the dose path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpb_b200.so")
+
+PB_OK = 0
+PB_ERR_INVALID = 1
+PB_ERR_CUDA = 2
+PB_ERR_NOMEM = 3
+PB_ERR_RAY_CAP = 4
+PB_ERR_UNSUPPORTED = 5
+
+PB_MAX_BEAMS = 16
+PB_MAX_LUT_LEN = 1024
+PB_MAX_CURVE = 64
+PB_SPOT_GEO_FLOATS = 8
+
+
+class PbError(RuntimeError):
+    """A non-zero PbStatus from the native library."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class PbGrid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("spacing", ctypes.c_float)]
+
+
+class PbBeamGeom(ctypes.Structure):
+    _fields_ = [("iso", ctypes.c_float * 3), ("src", ctypes.c_float * 3),
+                ("singa", ctypes.c_float), ("cosga", ctypes.c_float),
+                ("sinta", ctypes.c_float), ("costa", ctypes.c_float),
+                ("vsadx", ctypes.c_float), ("vsady", ctypes.c_float)]
+
+
+class PbSpot(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("mu", ctypes.c_float),
+                ("energy_id", ctypes.c_int)]
+
+
+class PbLayer(ctypes.Structure):
+    _fields_ = [("spot_start", ctypes.c_int), ("n_spots", ctypes.c_int),
+                ("energy_id", ctypes.c_int), ("r80", ctypes.c_float),
+                ("energy", ctypes.c_float)]
+
+
+class PbBeam(ctypes.Structure):
+    _fields_ = [("geom", PbBeamGeom),
+                ("layer_start", ctypes.c_int), ("n_layers", ctypes.c_int),
+                ("spot_start", ctypes.c_int), ("n_spots", ctypes.c_int),
+                ("dvp_dev", ctypes.c_void_p), ("depths_dev", ctypes.c_void_p),
+                ("sigmas_dev", ctypes.c_void_p), ("idds_dev", ctypes.c_void_p),
+                ("n_energies", ctypes.c_int), ("lut_len", ctypes.c_int),
+                ("dvp_len", ctypes.c_int)]
+
+
+# numpy views of the structs (same layout) for bulk host arrays
+SPOT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("mu", "<f4"), ("energy_id", "<i4")])
+LAYER_DTYPE = np.dtype([("spot_start", "<i4"), ("n_spots", "<i4"), ("energy_id", "<i4"),
+                        ("r80", "<f4"), ("energy", "<f4")])
+
+# Every entry point the header declares, with its argument types.
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+_D = ctypes.c_double
+_I64 = ctypes.c_int64
+_SIGS = {
+    "pb_last_error": (ctypes.c_char_p, []),
+    "pb_version": (ctypes.c_char_p, []),
+    "pb_beam_setup": (_I, [_D, _D, _D, _D, _VP, _VP, ctypes.POINTER(PbBeamGeom)]),
+    "pb_build_layers": (_I, [_VP, _I, _VP, _I, _I, _VP, _VP, ctypes.POINTER(_I), _VP]),
+    "pb_spot_geometry": (_I, [_VP, _I, _F, _F, _VP]),
+    "pb_rlsp_from_hu": (_I, [_VP, _I64, _VP, _VP, _I, _VP, _VP]),
+    "pb_texture_create": (_I, [_VP, ctypes.POINTER(PbGrid), ctypes.POINTER(ctypes.c_uint64), _VP]),
+    "pb_texture_update": (_I, [ctypes.c_uint64, _VP, _VP]),
+    "pb_texture_destroy": (_I, [ctypes.c_uint64]),
+    "pb_wet": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),
+    "pb_dose": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP, _VP, _VP]),
+    "pb_dose_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP,
+                             _VP]),
+    "pb_objective_work_size": (ctypes.c_size_t, []),
+    "pb_objective": (_I, [_VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP]),
+    "pb_count_pairs": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),
+    "pb_proton_raytrace_host": (_I, [_I, _D, _D, _VP, _VP, _F, _VP, _VP, _D, _D, _VP]),
+    "pb_proton_spot_host": (_I, [_I, _D, _D, _VP, _VP, _VP, _VP, _I, _I, _I, _VP, _VP, _F,
+                                 _VP, _VP, _D, _D, _VP, _I, _VP]),
+}
+
+EXPORTED = tuple(_SIGS)
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make -C dosecuda-jax_b200/csrc` "
+            "(the proton dose path has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    msg = lib.pb_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int, what: str = "") -> None:
+    """Raise PbError for a non-zero PbStatus."""
+    if status != PB_OK:
+        text = last_error()
+        raise PbError(status, f"{what}: {text}" if what else text)
+
+
+def ptr(a) -> ctypes.c_void_p:
+    """Address of a numpy array or torch tensor (None -> NULL)."""
+    if a is None:
+        return ctypes.c_void_p(0)
+    if isinstance(a, np.ndarray):
+        return ctypes.c_void_p(a.ctypes.data)
+    return ctypes.c_void_p(a.data_ptr())
+
+
+def beam_setup(gantry_deg: float, couch_deg: float, vsadx: float, vsady: float,
+               iso, origin) -> PbBeamGeom:
+    iso = np.ascontiguousarray(np.asarray(iso, dtype=np.float32).reshape(3))
+    origin = np.ascontiguousarray(np.asarray(origin, dtype=np.float32).reshape(3))
+    g = PbBeamGeom()
+    check(lib.pb_beam_setup(float(gantry_deg), float(couch_deg), float(vsadx), float(vsady),
+                            ptr(iso), ptr(origin), ctypes.byref(g)), "pb_beam_setup")
+    return g
+
+
+def build_layers(spot_list: np.ndarray, dvp: np.ndarray):
+    """Sorted spots (structured array), layers (structured array), perm."""
+    spot_list = np.ascontiguousarray(spot_list, dtype=np.float32).reshape(-1, 4)
+    dvp = np.ascontiguousarray(dvp, dtype=np.float32)
+    n = spot_list.shape[0]
+    n_e, dvp_len = dvp.shape
+    spots = np.zeros(n, dtype=SPOT_DTYPE)
+    layers = np.zeros(n_e, dtype=LAYER_DTYPE)
+    perm = np.zeros(n, dtype=np.int32)
+    nl = ctypes.c_int(0)
+    check(lib.pb_build_layers(ptr(spot_list), n, ptr(dvp), dvp_len, n_e, ptr(spots),
+                              ptr(layers), ctypes.byref(nl), ptr(perm)), "pb_build_layers")
+    return spots, layers[: nl.value].copy(), perm
+
+
+def spot_geometry(spots: np.ndarray, vsadx: float, vsady: float) -> np.ndarray:
+    geo = np.zeros((len(spots), PB_SPOT_GEO_FLOATS), dtype=np.float32)
+    check(lib.pb_spot_geometry(ptr(spots), len(spots), float(vsadx), float(vsady), ptr(geo)),
+          "pb_spot_geometry")
+    return geo

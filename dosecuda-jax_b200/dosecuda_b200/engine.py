@@ -1,0 +1,312 @@
+"""Device-resident plan state and the calls into libpb_b200.so.
+
+torch provides device memory and the current stream; every computation is a
+C-ABI call (include/pb_b200.h) that launches the package's sm_100a kernels.
+
+A ``DevicePlan`` holds, on one GPU, everything the pencil-beam kernels read
+for one plan: the grid, per-beam geometry and model tables, the layers and
+per-spot geometry in sorted (layer) order, the spot weights and the WET of
+every beam.  It exposes the forward dose, the adjoint (spot-weight
+gradient) and the dense pair count, so that an optimisation loop keeps all
+state on the device (reference host round trips: IMPTClasses.cu:274-340,
+plan_impt.py:185-206).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import PbBeam, PbGrid, check, ptr
+
+
+def _stream(device: torch.device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def require_cuda(device) -> torch.device:
+    dev = torch.device(device)
+    if dev.type != "cuda":
+        raise ValueError("the pencil-beam dose path runs on CUDA devices only")
+    if not torch.cuda.is_available():
+        raise RuntimeError("CUDA error: no CUDA device is available")
+    return dev
+
+
+@dataclass
+class ModelTables:
+    """One beam model's tables on one device (plan_impt.py:63-149)."""
+    dvp: torch.Tensor
+    depths: torch.Tensor
+    sigmas: torch.Tensor
+    idds: torch.Tensor
+    n_energies: int
+    lut_len: int
+    dvp_len: int
+    dvp_host: np.ndarray
+
+
+def model_tables(model, device: torch.device) -> ModelTables:
+    """Upload (once per device) the LUTs of an IMPTBeamModel-like object."""
+    cache = model.__dict__.setdefault("_pb_device_tables", {})
+    key = (device.index, id(model.divergence_params), id(model.lut_depths))
+    hit = cache.get(key)
+    if hit is not None:
+        return hit
+    dvp = np.ascontiguousarray(model.divergence_params, dtype=np.float32)
+    dep = np.ascontiguousarray(model.lut_depths, dtype=np.float32)
+    sig = np.ascontiguousarray(model.lut_sigmas, dtype=np.float32)
+    idd = np.ascontiguousarray(model.lut_idds, dtype=np.float32)
+    if dvp.ndim != 2 or dvp.shape[1] < 5:
+        raise ValueError("divergence_params must be n_energies x 5 (energy, R80, A, B, C)")
+    if dep.ndim != 2 or dep.shape != sig.shape or dep.shape != idd.shape:
+        raise ValueError("lut_depths / lut_sigmas / lut_idds must share one 2-D shape")
+    if dep.shape[0] != dvp.shape[0]:
+        raise ValueError("LUT rows and divergence_params rows differ")
+    if dep.shape[1] > _lib.PB_MAX_LUT_LEN:
+        raise ValueError(f"LUT length {dep.shape[1]} exceeds {_lib.PB_MAX_LUT_LEN}")
+    t = ModelTables(
+        dvp=torch.from_numpy(dvp).to(device), depths=torch.from_numpy(dep).to(device),
+        sigmas=torch.from_numpy(sig).to(device), idds=torch.from_numpy(idd).to(device),
+        n_energies=dvp.shape[0], lut_len=dep.shape[1], dvp_len=dvp.shape[1], dvp_host=dvp)
+    cache[key] = t
+    return t
+
+
+def rlsp_from_hu(hu: torch.Tensor, curve_hu: np.ndarray, curve_rlsp: np.ndarray,
+                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """HU -> RLSP on the GPU with numpy.interp semantics (plan_impt.py:158-168)."""
+    if hu.dtype != torch.float32 or not hu.is_cuda:
+        raise ValueError("hu must be a float32 CUDA tensor")
+    hu = hu.contiguous()
+    if out is None:
+        out = torch.empty_like(hu)
+    xh = np.ascontiguousarray(curve_hu, dtype=np.float64)
+    yh = np.ascontiguousarray(curve_rlsp, dtype=np.float64)
+    check(_lib.lib.pb_rlsp_from_hu(ptr(hu), hu.numel(), ptr(xh), ptr(yh), len(xh), ptr(out),
+                                   _stream(hu.device)), "pb_rlsp_from_hu")
+    return out
+
+
+@dataclass
+class BeamSpec:
+    """What the kernels need from one beam of a plan."""
+    gantry_angle: float
+    couch_angle: float
+    iso: np.ndarray
+    spot_list: np.ndarray      # n x 4 float32 (x, y, mu, energy_id)
+    model: object              # IMPTBeamModel-like
+
+
+def grid_of(volume_shape: Sequence[int], spacing: float) -> PbGrid:
+    nz, ny, nx = (int(v) for v in volume_shape)
+    return PbGrid(nx, ny, nz, float(spacing))
+
+
+class DevicePlan:
+    """A plan prepared on one GPU (see module docstring)."""
+
+    def __init__(self, volume_shape, spacing: float, origin, beams: List[BeamSpec],
+                 device="cuda"):
+        self.device = require_cuda(device)
+        if not beams:
+            raise ValueError("a plan needs at least one beam")
+        if len(beams) > _lib.PB_MAX_BEAMS:
+            raise ValueError(f"at most {_lib.PB_MAX_BEAMS} beams per plan")
+        self.shape = tuple(int(v) for v in volume_shape)
+        self.grid = grid_of(self.shape, spacing)
+        self.n_vox = int(np.prod(self.shape))
+        self.n_beams = len(beams)
+        origin = np.asarray(origin, dtype=np.float32).reshape(3)
+
+        self.geoms = (_lib.PbBeamGeom * self.n_beams)()
+        self.tables: List[ModelTables] = []
+        layer_blocks, geo_blocks, mu_blocks, perm_blocks = [], [], [], []
+        self.spot_offsets = [0]
+        self.layer_offsets = [0]
+        self.n_layers: List[int] = []
+        for b, bs in enumerate(beams):
+            t = model_tables(bs.model, self.device)
+            self.tables.append(t)
+            self.geoms[b] = _lib.beam_setup(bs.gantry_angle, bs.couch_angle, bs.model.VSADX,
+                                            bs.model.VSADY, bs.iso, origin)
+            sl = np.ascontiguousarray(bs.spot_list, dtype=np.float32).reshape(-1, 4)
+            spots, layers, perm = _lib.build_layers(sl, t.dvp_host)
+            geo = _lib.spot_geometry(spots, self.geoms[b].vsadx, self.geoms[b].vsady)
+            layer_blocks.append(layers)
+            geo_blocks.append(geo)
+            mu_blocks.append(spots["mu"].astype(np.float32))
+            perm_blocks.append(perm.astype(np.int64) + self.spot_offsets[-1])
+            self.spot_offsets.append(self.spot_offsets[-1] + len(spots))
+            self.layer_offsets.append(self.layer_offsets[-1] + len(layers))
+            self.n_layers.append(len(layers))
+        self.n_spots = self.spot_offsets[-1]
+        layers_all = np.concatenate(layer_blocks) if self.layer_offsets[-1] else \
+            np.zeros(1, dtype=_lib.LAYER_DTYPE)
+        geo_all = np.concatenate(geo_blocks) if self.n_spots else \
+            np.zeros((1, _lib.PB_SPOT_GEO_FLOATS), np.float32)
+        self.layers_np = layers_all
+        self.layers = torch.from_numpy(layers_all.view(np.uint8).copy()).to(self.device)
+        self.spot_geo = torch.from_numpy(np.ascontiguousarray(geo_all)).to(self.device)
+        # sorted position q holds the spot of plan row perm[q]
+        self.perm = torch.from_numpy(np.concatenate(perm_blocks) if self.n_spots
+                                     else np.zeros(0, np.int64)).to(self.device)
+        mu_sorted = np.concatenate(mu_blocks) if self.n_spots else np.zeros(0, np.float32)
+        self.mu_sorted = torch.from_numpy(mu_sorted).to(self.device)
+        self.beams = (PbBeam * self.n_beams)()
+        for b in range(self.n_beams):
+            t = self.tables[b]
+            B = self.beams[b]
+            B.geom = self.geoms[b]
+            B.layer_start = self.layer_offsets[b]
+            B.n_layers = self.n_layers[b]
+            B.spot_start = self.spot_offsets[b]
+            B.n_spots = self.spot_offsets[b + 1] - self.spot_offsets[b]
+            B.dvp_dev = t.dvp.data_ptr()
+            B.depths_dev = t.depths.data_ptr()
+            B.sigmas_dev = t.sigmas.data_ptr()
+            B.idds_dev = t.idds.data_ptr()
+            B.n_energies = t.n_energies
+            B.lut_len = t.lut_len
+            B.dvp_len = t.dvp_len
+        self.wet: Optional[torch.Tensor] = None
+        self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._tex = ctypes.c_uint64(0)
+
+    def __del__(self):
+        tex = getattr(self, "_tex", None)
+        if tex is not None and tex.value:
+            try:
+                torch.cuda.synchronize(self.device)
+                _lib.lib.pb_texture_destroy(tex)
+            except Exception:
+                pass
+            tex.value = 0
+
+    # -- spot order helpers ---------------------------------------------------
+    def to_sorted(self, mu_plan: torch.Tensor) -> torch.Tensor:
+        """Plan-row-ordered weights -> sorted (layer) order."""
+        return mu_plan.index_select(0, self.perm)
+
+    def to_plan(self, v_sorted: torch.Tensor) -> torch.Tensor:
+        out = torch.empty_like(v_sorted)
+        out.index_copy_(0, self.perm, v_sorted)
+        return out
+
+    def mu_plan(self) -> torch.Tensor:
+        return self.to_plan(self.mu_sorted)
+
+    # -- WET ---------------------------------------------------------------------
+    def _texture(self, rlsp: torch.Tensor) -> int:
+        st = _stream(self.device)
+        if self._tex.value:
+            check(_lib.lib.pb_texture_update(self._tex, ptr(rlsp), st), "pb_texture_update")
+        else:
+            check(_lib.lib.pb_texture_create(ptr(rlsp), ctypes.byref(self.grid),
+                                             ctypes.byref(self._tex), st), "pb_texture_create")
+        return self._tex.value
+
+    def compute_wet(self, rlsp: torch.Tensor, check_status: bool = True,
+                    wet_mode: str = "texture") -> torch.Tensor:
+        """Smoothed WET (cm) of every beam: n_beams x V on the device.
+
+        wet_mode "texture" samples RLSP through the texture unit as the
+        reference does; "exact" uses exact trilinear weights (the FP64
+        oracle's arithmetic)."""
+        if rlsp.dtype != torch.float32 or rlsp.device != self.device or rlsp.numel() != self.n_vox:
+            raise ValueError("rlsp must be a float32 tensor of the grid's size on the plan's device")
+        if wet_mode not in ("texture", "exact"):
+            raise ValueError("wet_mode must be 'texture' or 'exact'")
+        rlsp = rlsp.contiguous()
+        tex = self._texture(rlsp) if wet_mode == "texture" else 0
+        raw = torch.empty((self.n_beams, self.n_vox), dtype=torch.float32, device=self.device)
+        wet = torch.empty_like(raw)
+        self._status.zero_()
+        check(_lib.lib.pb_wet(ptr(rlsp), tex, ctypes.byref(self.grid),
+                              ctypes.cast(self.geoms, ctypes.c_void_p),
+                              self.n_beams, ptr(raw), ptr(wet), ptr(self._status),
+                              _stream(self.device)), "pb_wet")
+        if check_status and int(self._status.item()) & _lib.PB_ERR_RAY_CAP:
+            raise _lib.PbError(_lib.PB_ERR_RAY_CAP, "a WET ray reached its step cap")
+        self.wet = wet
+        self.raw_wet = raw
+        return wet
+
+    def set_wet(self, wet: torch.Tensor) -> None:
+        if wet.numel() != self.n_beams * self.n_vox or wet.dtype != torch.float32:
+            raise ValueError("wet must be float32 with n_beams x V elements")
+        self.wet = wet.to(self.device).reshape(self.n_beams, self.n_vox).contiguous()
+
+    def _need_wet(self):
+        if self.wet is None:
+            raise RuntimeError("WET has not been computed for this plan")
+
+    # -- forward / adjoint -------------------------------------------------------
+    def forward(self, mu_sorted: Optional[torch.Tensor] = None, scale: float = 1.0,
+                beam_doses: bool = False, out: Optional[torch.Tensor] = None):
+        """Dose (V) = scale * sum over beams; optionally n_beams x V per beam."""
+        self._need_wet()
+        mu = self.mu_sorted if mu_sorted is None else mu_sorted
+        if mu.dtype != torch.float32 or mu.numel() != self.n_spots:
+            raise ValueError("mu must be float32 with one entry per spot")
+        mu = mu.contiguous()
+        dose = out if out is not None else torch.empty(self.n_vox, dtype=torch.float32,
+                                                       device=self.device)
+        bd = torch.empty((self.n_beams, self.n_vox), dtype=torch.float32,
+                         device=self.device) if beam_doses else None
+        check(_lib.lib.pb_dose(ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p),
+                               self.n_beams, ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
+                               ptr(mu), float(scale), ptr(dose), ptr(bd),
+                               _stream(self.device)), "pb_dose")
+        return (dose, bd) if beam_doses else dose
+
+    def adjoint(self, dobj_ddose: torch.Tensor, scale: float = 1.0,
+                out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """grad[s] (sorted order) = scale * sum_v dobj_ddose[v] K(v, s)."""
+        self._need_wet()
+        if dobj_ddose.dtype != torch.float32 or dobj_ddose.numel() != self.n_vox:
+            raise ValueError("dobj_ddose must be float32 with one entry per voxel")
+        w = dobj_ddose.contiguous()
+        grad = out if out is not None else torch.empty(max(self.n_spots, 1), dtype=torch.float32,
+                                                       device=self.device)
+        check(_lib.lib.pb_dose_adjoint(ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p),
+                                       self.n_beams, ptr(self.wet), ptr(self.layers),
+                                       ptr(self.spot_geo), ptr(w), float(scale), ptr(grad),
+                                       _stream(self.device)), "pb_dose_adjoint")
+        return grad[: self.n_spots]
+
+    def count_pairs(self) -> int:
+        """Dense spot-voxel pair count E of the reference kernel."""
+        self._need_wet()
+        c = torch.zeros(1, dtype=torch.int64, device=self.device)
+        check(_lib.lib.pb_count_pairs(ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p),
+                                      self.n_beams, ptr(self.wet), ptr(self.layers), ptr(c),
+                                      _stream(self.device)), "pb_count_pairs")
+        return int(c.item())
+
+
+_OBJ_WORK = {}
+
+
+def objective(dose: torch.Tensor, presc: torch.Tensor, weight: torch.Tensor,
+              resid: Optional[torch.Tensor] = None):
+    """FP64 sum_v w (D-P)^2 on the device (1-element float64 tensor) and,
+    if ``resid`` is given, 2 w (D-P) written into it."""
+    dev = dose.device
+    n = dose.numel()
+    for t in (presc, weight):
+        if t.numel() != n or t.dtype != torch.float32 or t.device != dev:
+            raise ValueError("dose, prescription and weights must match")
+    work = _OBJ_WORK.get(dev)
+    if work is None:
+        work = torch.empty(int(_lib.lib.pb_objective_work_size()), dtype=torch.uint8, device=dev)
+        _OBJ_WORK[dev] = work
+    obj = torch.empty(1, dtype=torch.float64, device=dev)
+    check(_lib.lib.pb_objective(ptr(dose.contiguous()), ptr(presc.contiguous()),
+                                ptr(weight.contiguous()), n, ptr(obj), ptr(resid), ptr(work),
+                                _stream(dev)), "pb_objective")
+    return obj

@@ -1,0 +1,300 @@
+"""IMPT plan API (mirror of DoseCUDA/plan_impt.py) on the B200 kernels.
+
+Class names, attributes, method names, arguments and error behaviour follow
+the reference (plan_impt.py:63-342); the dose computation goes through the
+package's CUDA kernels with all beams of a plan in one launch and the CT,
+RLSP, WET and dose kept on the device.
+
+Beyond the reference:
+  IMPTDoseGrid.prepareIMPTPlan      device-resident plan for repeated use
+  IMPTDoseGrid.computeIMPTPlanGradient
+                                    objective + spot-weight gradient
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import pandas as pd
+import torch
+
+from . import engine, nrrd
+from .plan import Beam, DoseGrid, Plan, Prescription, VolumeObject  # noqa: F401
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+
+
+def resource_filename(rel_path: str) -> str:
+    """Path of a package data file (the reference uses pkg_resources)."""
+    return os.path.join(_PKG, rel_path)
+
+
+class IMPTBeamModel():
+    """Lookup-table beam model of one range-shifter setting
+    (plan_impt.py:63-149): VSADX/VSADY from machine_geometry.csv; per energy
+    divergence_params (energy, R80, A, B, C) and the first 400 rows of
+    depth / sigma / IDD from energy_NNN.csv."""
+
+    def __init__(self, dicom_rangeshifter_label, path_to_model, folder_rangeshifter_label):
+
+        self.dicom_rangeshifter_label = dicom_rangeshifter_label
+
+        machine_geometry_path = resource_filename(os.path.join(path_to_model, "machine_geometry.csv"))
+
+        self.VSADX = None
+        self.VSADY = None
+
+        for line in open(machine_geometry_path, "r"):
+            if line.startswith("VSADX"):
+                self.VSADX = float(line.split(',')[1])
+            if line.startswith("VSADY"):
+                self.VSADY = float(line.split(',')[1])
+
+        if self.VSADX is None:
+            raise Exception("VSADX not found in machine_geometry.csv")
+        if self.VSADY is None:
+            raise Exception("VSADY not found in machine_geometry.csv")
+
+        energy_list_path = resource_filename(os.path.join(path_to_model, folder_rangeshifter_label,
+                                                          "energies.csv"))
+        self.energy_table = pd.read_csv(energy_list_path)
+        self.energy_labels = self.energy_table["energy_label"].to_numpy()
+        energy_ids = self.energy_table["index"].to_numpy()
+        self.reference_sigmas = self.energy_table["sigma"].to_numpy()
+
+        dvps, deps, sigs, idds = [], [], [], []
+        for energy_id in energy_ids:
+            lut_path = resource_filename(os.path.join(path_to_model, folder_rangeshifter_label,
+                                                      "energy_%03d.csv" % energy_id))
+            with open(lut_path, "r") as f:
+                f.readline()  # header
+                dvps.append([float(p) for p in f.readline().split(",")])
+                f.readline()  # blank
+                f.readline()  # header
+                d, s, i = [], [], []
+                for k, line in enumerate(f):
+                    if k > 399:
+                        break
+                    parts = line.split(",")
+                    d.append(float(parts[0]))
+                    s.append(float(parts[1]))
+                    i.append(float(parts[2]))
+            deps.append(d)
+            sigs.append(s)
+            idds.append(i)
+
+        self.divergence_params = np.array(dvps, dtype=np.single)
+        self.lut_depths = np.array(deps, dtype=np.single)
+        self.lut_sigmas = np.array(sigs, dtype=np.single)
+        self.lut_idds = np.array(idds, dtype=np.single)
+
+    def energyIDFromLabel(self, energy_label):
+        energy_row = self.energy_table[self.energy_table["energy_label"] == energy_label]
+        if len(energy_row) != 1:
+            raise Exception("Energy ID not found for %.2f" % energy_label)
+        return energy_row.index[0]
+
+
+def _hu_curve(machine_name):
+    df = pd.read_csv(resource_filename(os.path.join("lookuptables", "protons", machine_name,
+                                                    "HU_RLSP.csv")))
+    return df["HU"].to_numpy(dtype=np.float64), df["RLSP"].to_numpy(dtype=np.float64)
+
+
+def _beam_model(plan, beam):
+    try:
+        model_index = list(plan.dicom_rangeshifter_label.astype(str)).index(
+            beam.dicom_rangeshifter_label)
+    except ValueError:
+        print("Beam model not found for rangeshifter ID %s" % beam.dicom_rangeshifter_label)
+        sys.exit(1)
+    return plan.beam_models[model_index]
+
+
+def _spot_array(beam) -> np.ndarray:
+    sl = np.asarray(beam.spot_list, dtype=np.single)
+    if sl.ndim == 1 and sl.size == 4:
+        sl = sl.reshape(1, 4)
+    if sl.ndim != 2 or (sl.size and sl.shape[1] != 4):
+        raise ValueError("'spot_list' must be 2-dimensional and of type float.")
+    return sl.reshape(-1, 4)
+
+
+class IMPTDoseGrid(DoseGrid):
+
+    def __init__(self):
+        super().__init__()
+        self.RLSP = []
+        self._device_rlsp = None
+
+    def _device(self, gpu_id):
+        return engine.require_cuda(torch.device("cuda", int(gpu_id)))
+
+    def _check_isotropic(self):
+        if self.spacing[0] != self.spacing[1] or self.spacing[0] != self.spacing[2]:
+            raise Exception("Spacing must be isotropic for IMPT dose calculation - consider "
+                            "resampling CT")
+
+    def _rlsp_device(self, machine_name, device):
+        hu = torch.from_numpy(np.ascontiguousarray(self.HU, dtype=np.single)).to(device)
+        xh, yh = _hu_curve(machine_name)
+        rlsp = engine.rlsp_from_hu(hu, xh, yh)
+        self._device_rlsp = rlsp
+        return rlsp
+
+    def RLSPFromHU(self, machine_name, gpu_id=0):
+        """numpy.interp of HU over the machine's HU->RLSP curve, float32
+        (plan_impt.py:158-168), evaluated on the GPU."""
+        rlsp = self._rlsp_device(machine_name, self._device(gpu_id))
+        return rlsp.cpu().numpy().reshape(np.shape(self.HU))
+
+    def _specs(self, plan, beams):
+        specs = []
+        for beam in beams:
+            model = _beam_model(plan, beam)
+            specs.append(engine.BeamSpec(beam.gantry_angle, beam.couch_angle,
+                                         np.asarray(beam.iso, dtype=np.single),
+                                         _spot_array(beam), model))
+        return specs
+
+    def prepareIMPTPlan(self, plan, gpu_id=0, beams=None, wet_mode="texture"):
+        """Device-resident plan with its WET computed: the state an
+        optimisation loop reuses (engine.DevicePlan).  wet_mode "texture"
+        reproduces the reference's texture-sampled WET; "exact" uses exact
+        trilinear interpolation."""
+        self._check_isotropic()
+        device = self._device(gpu_id)
+        rlsp = self._rlsp_device(plan.machine_name, device)
+        beams = plan.beam_list if beams is None else beams
+        dp = engine.DevicePlan(np.shape(self.HU), float(self.spacing[0]),
+                               np.asarray(self.origin, dtype=np.single),
+                               self._specs(plan, beams), device)
+        dp.compute_wet(rlsp.reshape(-1), wet_mode=wet_mode)
+        return dp
+
+    def computeIMPTPlan(self, plan, gpu_id=0, wet_mode="texture"):
+        """Dose of every beam and their sum, times n_fractions
+        (plan_impt.py:170-206)."""
+        self.beam_doses = []
+        self.dose = np.zeros(self.size, dtype=np.single)
+        self._check_isotropic()
+        if not plan.beam_list:
+            self.RLSP = self.RLSPFromHU(plan.machine_name, gpu_id)
+            self.dose *= plan.n_fractions
+            return
+        dp = self.prepareIMPTPlan(plan, gpu_id, wet_mode=wet_mode)
+        self.RLSP = self._device_rlsp.cpu().numpy().reshape(np.shape(self.HU))
+        dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
+        shape = np.shape(self.HU)
+        bd_host = bd.cpu().numpy()
+        self.beam_doses = [bd_host[b].reshape(shape) for b in range(dp.n_beams)]
+        self.dose = dose.cpu().numpy().reshape(shape)
+
+    def computeIMPTWET(self, plan, gpu_id=0, wet_mode="texture"):
+        """Per-beam WET volumes as VolumeObjects (plan_impt.py:208-236)."""
+        self._check_isotropic()
+        dp = self.prepareIMPTPlan(plan, gpu_id, wet_mode=wet_mode)
+        self.RLSP = self._device_rlsp.cpu().numpy().reshape(np.shape(self.HU))
+        wet = dp.wet.cpu().numpy()
+        out = []
+        for b in range(dp.n_beams):
+            wet_object = VolumeObject()
+            wet_object.voxel_data = np.array(wet[b].reshape(np.shape(self.HU)), dtype=np.single)
+            wet_object.origin = np.array(self.origin, dtype=np.single)
+            wet_object.spacing = np.array(self.spacing, dtype=np.single)
+            out.append(wet_object)
+        return out
+
+    def computeIMPTPlanFromWET(self, plan, wet_object, beam, gpu_id=0):
+        """One beam's dose from a precomputed WET volume
+        (plan_impt.py:238-257); no n_fractions factor."""
+        self._check_isotropic()
+        device = self._device(gpu_id)
+        wet = np.asarray(wet_object.voxel_data, dtype=np.single)
+        dp = engine.DevicePlan(wet.shape, float(self.spacing[0]),
+                               np.asarray(self.origin, dtype=np.single),
+                               self._specs(plan, [beam]), device)
+        dp.set_wet(torch.from_numpy(np.ascontiguousarray(wet)).to(device))
+        return dp.forward().cpu().numpy().reshape(wet.shape)
+
+    def writeWETNRRD(self, plan, wet_path, gpu_id=0):
+        if not wet_path.endswith(".nrrd"):
+            raise Exception("WET path must have .nrrd extension")
+        for i, w in enumerate(self.computeIMPTWET(plan, gpu_id)):
+            nrrd.write(wet_path.replace(".nrrd", "_beam%02i.nrrd" % (i + 1)), w.voxel_data,
+                       self.origin, self.spacing)
+
+    def computeIMPTPlanGradient(self, plan, target_dose, voxel_weights, gpu_id=0,
+                                wet_mode="texture"):
+        """Quadratic objective sum_v w_v (D_v - P_v)^2 of the plan dose and its
+        gradient with respect to every spot weight, in beam order then each
+        beam's spot_list row order.  Returns (objective: float, gradient:
+        float32 ndarray)."""
+        from .autograd import plan_objective_and_grad
+        dp = self.prepareIMPTPlan(plan, gpu_id, wet_mode=wet_mode)
+        obj, grad = plan_objective_and_grad(dp, target_dose, voxel_weights,
+                                            scale=float(plan.n_fractions))
+        return obj, grad
+
+
+class IMPTBeam(Beam):
+
+    def __init__(self, beam=None):
+        super().__init__()
+
+        self.spot_list = []
+        self.n_spots = 0
+        self.dicom_rangeshifter_label = None
+
+        if beam is not None:
+            self.gantry_angle = beam.gantry_angle
+            self.couch_angle = beam.couch_angle
+            self.iso = beam.iso
+            self.spot_list = beam.spot_list
+            self.n_spots = beam.n_spots
+            self.dicom_rangeshifter_label = beam.dicom_rangeshifter_label
+
+    def addSpotData(self, cp, energy_id):
+        """Spots of one control point (ScanSpotPositionMap, meterset weights)."""
+        spm = np.reshape(np.array(cp.ScanSpotPositionMap), (-1, 2))
+        mus = np.array(cp.ScanSpotMetersetWeights)
+        energy_id_array = np.full(mus.size, energy_id)
+        spot_list = np.array(np.column_stack((spm, mus, energy_id_array)), dtype=np.single)
+        self.spot_list = np.vstack((self.spot_list, spot_list)) if self.n_spots > 0 else spot_list
+        self.n_spots += mus.size
+
+    def changeSpotEnergy(self, energy_id):
+        self.spot_list[:, 3] = energy_id
+
+    def addSingleSpot(self, x, y, mu, energy_id):
+        spot = np.array([x, y, mu, energy_id], dtype=np.single)
+        self.spot_list = np.vstack((self.spot_list, spot)) if self.n_spots > 0 else spot
+        self.n_spots += 1
+
+    def resetSpots(self):
+        self.spot_list = np.empty((0, 4), dtype=np.single)
+        self.n_spots = 0
+
+
+class IMPTPlan(Plan):
+
+    def __init__(self, machine_name="HitachiProbeatJHU"):
+        super().__init__()
+        self.machine_name = machine_name
+
+        rangeshifter_list = pd.read_csv(resource_filename(os.path.join(
+            "lookuptables", "protons", machine_name, "rangeshifter_labels.csv")))
+        self.dicom_rangeshifter_label = rangeshifter_list["dicom_rangeshifter_label"]
+        self.folder_rangeshifter_label = rangeshifter_list["folder_rangeshifter_label"]
+
+        self.beam_models = []
+        for d, f in zip(self.dicom_rangeshifter_label, self.folder_rangeshifter_label):
+            self.beam_models.append(IMPTBeamModel(d, os.path.join("lookuptables", "protons",
+                                                                  machine_name), f))
+
+    def writePlanDicom(self, ct_dir, output_file, rt_struct_file=None):
+        raise NotImplementedError("writePlanDicom writes DICOM through pydicom")
+
+    def readPlanDicom(self, plan_path):
+        raise NotImplementedError("readPlanDicom reads DICOM through pydicom")

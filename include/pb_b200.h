@@ -1,0 +1,222 @@
+/*
+ * pb_b200.h -- C ABI of the B200 proton pencil-beam dose library
+ * (libpb_b200.so).
+ *
+ * Replaces the native half of DoseCUDA's proton path:
+ *   DoseCUDA/dose_kernels/IMPTClasses.cuh:90-91
+ *       void proton_raytrace_cuda(int gpu_id, CudaDose*, CudaBeam*);
+ *       void proton_spot_cuda(int gpu_id, IMPTDose*, IMPTBeam*);
+ *   and the CPython wrappers that feed them,
+ *   DoseCUDA/dose_kernels/dosemodule.cu:104-201 (proton_raytrace) and
+ *   dosemodule.cu:243-374 (proton_spot).
+ *
+ * Conventions
+ *   - Plain C types only.  Every function returns a PbStatus; none throws.
+ *     pb_last_error() gives the text of the last failure on this thread.
+ *   - Volumes are C-ordered (nz, ny, nx) float32, x fastest; the linear
+ *     index of voxel (i, j, k) is i + nx*(j + ny*k)  (CudaClasses.cuh:96-98).
+ *   - Functions whose pointer arguments are named *_dev take device
+ *     pointers on the current CUDA device and are ordered on `stream`
+ *     (a cudaStream_t passed as void*; NULL = legacy default stream).  They
+ *     allocate nothing: buffers, including work space, come from the caller.
+ *   - Functions named *_host take host pointers, select `gpu_id`, and
+ *     return when the result is in host memory (the reference's contract).
+ *     They keep grow-only device buffers per device between calls.
+ *   - WET is in cm, distances in mm, angles in degrees, dose in the IDD
+ *     table's units per mm^2 per MU (IMPTClasses.cu:243-244).
+ */
+#ifndef PB_B200_H
+#define PB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PB_OK = 0,
+    PB_ERR_INVALID = 1,      /* bad argument (null pointer, size, shape)   */
+    PB_ERR_CUDA = 2,         /* a CUDA runtime call or launch failed       */
+    PB_ERR_NOMEM = 3,        /* host or device allocation failed           */
+    PB_ERR_RAY_CAP = 4,      /* a WET ray reached its step cap             */
+    PB_ERR_UNSUPPORTED = 5   /* valid request this build cannot serve      */
+} PbStatus;
+
+#define PB_MAX_BEAMS 16      /* beams per plan in one launch               */
+#define PB_MAX_LUT_LEN 1024  /* LUT rows per energy (reference: 400)       */
+#define PB_MAX_CURVE 64      /* points of an HU -> RLSP curve              */
+
+/* Voxel grid: isotropic spacing only (dosemodule.cu:146, plan_impt.py:177). */
+typedef struct {
+    int nx, ny, nz;
+    float spacing;           /* mm */
+} PbGrid;
+
+/* Beam geometry after the reference's set-up: gantry' = fmod(g+180, 360),
+ * iso' = iso - origin, source at (vsadx+vsady)/2 rotated by gantry' about z
+ * and couch about y (CudaClasses.cu:17-51, dosemodule.cu:148-175). */
+typedef struct {
+    float iso[3];            /* isocentre minus grid origin, mm            */
+    float src[3];            /* source relative to the isocentre, mm       */
+    float singa, cosga;      /* gantry' sine / cosine                      */
+    float sinta, costa;      /* couch sine / cosine                        */
+    float vsadx, vsady;      /* virtual source-axis distances, mm          */
+} PbBeamGeom;
+
+/* A spot as the reference stores it (IMPTClasses.cuh:8-15). */
+typedef struct {
+    float x, y, mu;
+    int energy_id;
+} PbSpot;
+
+/* An energy layer (IMPTClasses.cuh:17-26); spot_start is relative to the
+ * beam's first spot. */
+typedef struct {
+    int spot_start, n_spots, energy_id;
+    float r80, energy;
+} PbLayer;
+
+/* One beam of a plan as the dose kernels see it.  Model tables are device
+ * pointers: dvp is n_energies x dvp_len (energy, R80, A, B, C), the LUTs are
+ * n_energies x lut_len (plan_impt.py:63-149). */
+typedef struct {
+    PbBeamGeom geom;
+    int layer_start, n_layers;   /* into the plan's layer array            */
+    int spot_start, n_spots;     /* into the plan's spot arrays            */
+    const float *dvp_dev;
+    const float *depths_dev, *sigmas_dev, *idds_dev;
+    int n_energies, lut_len, dvp_len;
+} PbBeam;
+
+/* Number of floats of per-spot geometry that pb_spot_geometry writes. */
+#define PB_SPOT_GEO_FLOATS 8
+
+/* ---------------------------------------------------------------- host */
+
+/* Text of the last error on this thread ("" if none). */
+const char *pb_last_error(void);
+
+/* Library version string. */
+const char *pb_version(void);
+
+/* Beam set-up, as dosemodule.cu:148-175 + CudaClasses.cu:17-51 do it. */
+PbStatus pb_beam_setup(double gantry_deg, double couch_deg, double vsadx,
+                       double vsady, const float iso[3], const float origin[3],
+                       PbBeamGeom *out);
+
+/* Sort spots by energy id (ties keep input order) and group them into
+ * layers like importLayers (dosemodule.cu:204-225, IMPTClasses.cu:29-67).
+ * spot_list is n_spots x 4 float (x, y, mu, energy_id); the energy id is
+ * truncated to int.  dvp is host n_energies x dvp_len.  layers_out needs
+ * room for n_energies entries; perm_out (nullable) receives, for each
+ * sorted spot, its row in spot_list. */
+PbStatus pb_build_layers(const float *spot_list, int n_spots, const float *dvp,
+                         int dvp_len, int n_energies, PbSpot *spots_out,
+                         PbLayer *layers_out, int *n_layers_out, int *perm_out);
+
+/* Per-spot geometry for the dose kernels: PB_SPOT_GEO_FLOATS floats per
+ * spot (x, y, x/VSADX, y/VSADY, x*y*(1/VSADX-1/VSADY), 1/|t|^2, 0, 0). */
+PbStatus pb_spot_geometry(const PbSpot *spots, int n_spots, float vsadx,
+                          float vsady, float *geo_out);
+
+/* -------------------------------------------------------------- device */
+
+/* HU -> RLSP with numpy.interp semantics in FP64, rounded to FP32
+ * (plan_impt.py:158-168).  The curve is host data, increasing in HU. */
+PbStatus pb_rlsp_from_hu(const float *hu_dev, int64_t n, const double *curve_hu,
+                         const double *curve_rlsp, int n_curve, float *rlsp_dev,
+                         void *stream);
+
+/* Handle of a 3-D texture holding an RLSP volume with the reference's
+ * sampling state: float channel, linear filter, border 0, unnormalised
+ * coordinates (TextureClasses.cu:14-41, IMPTClasses.cu:292).  The texture
+ * unit's filter weights are fixed point, so samples through it differ
+ * slightly from exact trilinear interpolation; the reference's WET is
+ * defined by them.  Creating one allocates a CUDA array. */
+typedef uint64_t PbTexture;
+
+PbStatus pb_texture_create(const float *rlsp_dev, const PbGrid *grid,
+                           PbTexture *tex_out, void *stream);
+/* Refill an existing texture from a volume of the same grid. */
+PbStatus pb_texture_update(PbTexture tex, const float *rlsp_dev, void *stream);
+PbStatus pb_texture_destroy(PbTexture tex);
+
+/* WET (cm) of every voxel for n_beams beams: the ray trace toward the
+ * source (CudaClasses.cu:180-228, accumulated in FP64) followed by the
+ * lateral smoothing (IMPTClasses.cu:139-202).
+ *   tex != 0: RLSP is sampled through the texture (the reference's
+ *             samples); rlsp_dev is not read and may be NULL.
+ *   tex == 0: RLSP is read from rlsp_dev with exact FP32 trilinear
+ *             weights (border 0).
+ * raw_work_dev and wet_dev hold n_beams x V floats; raw_work_dev receives
+ * the unsmoothed WET.  status_dev (nullable) is one device int that is
+ * OR-ed with PB_ERR_RAY_CAP if a ray reaches its step cap. */
+PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
+                const PbBeamGeom *beams, int n_beams, float *raw_work_dev,
+                float *wet_dev, int *status_dev, void *stream);
+
+/* Forward pencil-beam dose of a plan (IMPTClasses.cu:204-271) for all of
+ * its beams in one launch.  wet_dev: n_beams x V (cm).  layers_dev: all
+ * layers, beam-major.  spot_geo_dev: PB_SPOT_GEO_FLOATS per spot, mu_dev:
+ * one weight per spot, both in sorted (layer) order.  dose_dev (V) receives
+ * scale * sum over beams; beam_dose_dev (nullable, n_beams x V) receives
+ * scale * each beam's dose.  Per-voxel sums are compensated. */
+PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                 const float *wet_dev, const PbLayer *layers_dev,
+                 const float *spot_geo_dev, const float *mu_dev, float scale,
+                 float *dose_dev, float *beam_dose_dev, void *stream);
+
+/* Adjoint of pb_dose: grad_dev[s] = scale * sum_v dobj_dose_dev[v] * K(v,s)
+ * for every spot s, where K(v,s) is the dose per unit weight of spot s at
+ * voxel v.  Matrix-free: footprints are recomputed.  grad_dev is
+ * overwritten. */
+PbStatus pb_dose_adjoint(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                         const float *wet_dev, const PbLayer *layers_dev,
+                         const float *spot_geo_dev, const float *dobj_dose_dev,
+                         float scale, float *grad_dev, void *stream);
+
+/* Quadratic objective sum_v w_v (D_v - P_v)^2, reduced in FP64 into
+ * *obj_dev, and its gradient 2 w_v (D_v - P_v) into resid_dev (nullable).
+ * work_dev holds pb_objective_work_size() bytes. */
+size_t pb_objective_work_size(void);
+PbStatus pb_objective(const float *dose_dev, const float *presc_dev,
+                      const float *weight_dev, int64_t n, double *obj_dev,
+                      float *resid_dev, void *work_dev, void *stream);
+
+/* Dense spot-voxel pair count of a plan: sum over beams and layers of
+ * |{v : 10*WET(v) <= 1.1*R80}| * spots (the reference kernel's work,
+ * IMPTClasses.cu:222-226,255).  count_dev is one uint64, overwritten. */
+PbStatus pb_count_pairs(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                        const float *wet_dev, const PbLayer *layers_dev,
+                        unsigned long long *count_dev, void *stream);
+
+/* ---------------------------------------------------- host drop-in level */
+
+/* proton_raytrace_cuda: smoothed WET of one beam from host RLSP
+ * (IMPTClasses.cu:274-299 via dosemodule.cu:104-201), sampled through a
+ * texture as the reference does.  dims are the numpy shape (nz, ny, nx). */
+PbStatus pb_proton_raytrace_host(int gpu_id, double vsadx, double vsady,
+                                 const float *rlsp, const int64_t dims[3],
+                                 float spacing, const float origin[3],
+                                 const float iso[3], double gantry_deg,
+                                 double couch_deg, float *wet_out);
+
+/* proton_spot_cuda: dose of one beam from host WET and spots
+ * (IMPTClasses.cu:301-340 via dosemodule.cu:243-374). */
+PbStatus pb_proton_spot_host(int gpu_id, double vsadx, double vsady,
+                             const float *dvp, const float *depths,
+                             const float *sigmas, const float *idds,
+                             int n_energies, int lut_len, int dvp_len,
+                             const float *wet, const int64_t dims[3],
+                             float spacing, const float origin[3],
+                             const float iso[3], double gantry_deg,
+                             double couch_deg, const float *spot_list,
+                             int n_spots, float *dose_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PB_B200_H */

@@ -1,0 +1,133 @@
+"""The C-ABI library on the host: it loads, exports every entry point the
+header declares, its host-side plan preparation matches the oracle bit for
+bit, and bad arguments come back as status codes (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "pb_b200.h")
+
+
+def _declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from dosecuda_b200 import _lib
+    names = _declared()
+    assert len(names) >= 16
+    raw = ctypes.CDLL(_lib.LIB_PATH)
+    for n in names:
+        assert hasattr(raw, n), n
+    assert set(names) <= set(_lib.EXPORTED)
+    assert b"sm_100a" in _lib.lib.pb_version()
+
+
+@pytest.mark.parametrize("gantry,couch", [(0, 0), (90, 0), (180, 0), (270, 0), (120, 0),
+                                          (240, 0), (45, 90), (-90, 15), (359.5, 270),
+                                          (33.3, -20)])
+def test_beam_setup_matches_oracle_bitwise(gantry, couch, oracle):
+    from dosecuda_b200 import _lib
+    iso = np.array([12.5, -3.25, 40.0], np.float32)
+    origin = np.array([-150.0, -151.5, -120.25], np.float32)
+    g = _lib.beam_setup(gantry, couch, 1340.0, 1930.0, iso, origin)
+    o = oracle.beam_setup(gantry, couch, 1340.0, 1930.0, iso, origin)
+    assert bytes(g) == bytes(o)
+
+
+def test_beam_setup_semantics():
+    """gantry' = fmod(gantry + 180, 360); source at (VSADX+VSADY)/2 from iso."""
+    from dosecuda_b200 import _lib
+    g = _lib.beam_setup(0.0, 0.0, 1340.0, 1930.0, [0, 0, 0], [0, 0, 0])
+    assert abs(g.src[1] + 1635.0) < 1e-3 and abs(g.src[0]) < 1e-3
+    g = _lib.beam_setup(90.0, 0.0, 1340.0, 1930.0, [1, 2, 3], [0.5, 0.5, 0.5])
+    assert list(g.iso) == [0.5, 1.5, 2.5]
+    assert abs(np.hypot(g.src[0], g.src[1]) - 1635.0) < 1e-2
+
+
+def _random_spots(rng, n, n_e):
+    sl = np.zeros((n, 4), np.float32)
+    sl[:, 0] = rng.uniform(-80, 80, n)
+    sl[:, 1] = rng.uniform(-80, 80, n)
+    sl[:, 2] = rng.uniform(0.1, 2.0, n)
+    sl[:, 3] = rng.integers(0, n_e, n)
+    return sl
+
+
+def test_build_layers_matches_oracle(oracle):
+    from dosecuda_b200 import _lib
+    from dosecuda_b200.plan_impt import IMPTPlan
+    dvp = IMPTPlan().beam_models[0].divergence_params
+    rng = np.random.default_rng(0)
+    for n in (0, 1, 7, 500):
+        sl = _random_spots(rng, n, dvp.shape[0])
+        s1, l1, perm = _lib.build_layers(sl, dvp)
+        s2, l2 = oracle.build_layers(sl, dvp)
+        assert s1.tobytes() == s2.tobytes() and l1.tobytes() == l2.tobytes()
+        # perm maps each sorted spot to its input row
+        if n:
+            assert np.array_equal(sl[perm][:, 0], s1["x"])
+
+
+def test_build_layers_reference_quirks():
+    """importLayers (IMPTClasses.cu:37-67): ids are truncated to int; ids at
+    or above n_energies are dropped; one negative id blocks every layer."""
+    from dosecuda_b200 import _lib
+    dvp = np.zeros((5, 5), np.float32)
+    dvp[:, 1] = [10, 20, 30, 40, 50]
+    sl = np.array([[0, 0, 1, 3.9], [1, 0, 1, 1.0], [2, 0, 1, 7.0], [3, 0, 1, 1.2]], np.float32)
+    spots, layers, perm = _lib.build_layers(sl, dvp)
+    assert [(L["energy_id"], L["n_spots"], L["spot_start"]) for L in layers] == [(1, 2, 0),
+                                                                                 (3, 1, 2)]
+    assert list(perm) == [1, 3, 0, 2]
+    assert layers[1]["r80"] == 40
+    sl[0, 3] = -2.0
+    _, layers, _ = _lib.build_layers(sl, dvp)
+    assert len(layers) == 0
+
+
+def test_spot_geometry_values():
+    from dosecuda_b200 import _lib
+    spots = np.zeros(3, _lib.SPOT_DTYPE)
+    spots["x"] = [10.0, -20.0, 0.0]
+    spots["y"] = [5.0, 7.5, 0.0]
+    geo = _lib.spot_geometry(spots, 1340.0, 1930.0)
+    x, y = spots["x"].astype(np.float64), spots["y"].astype(np.float64)
+    tx, ty = x / 1340.0, y / 1930.0
+    assert np.allclose(geo[:, 2], tx, rtol=1e-7) and np.allclose(geo[:, 3], ty, rtol=1e-7)
+    assert np.allclose(geo[:, 4], x * y * (1 / 1340.0 - 1 / 1930.0), rtol=1e-6)
+    assert np.allclose(geo[:, 5], 1.0 / (1.0 + tx * tx + ty * ty), rtol=1e-7)
+
+
+def test_invalid_arguments_return_status_without_a_gpu():
+    from dosecuda_b200 import _lib
+    L = _lib.lib
+    g = _lib.PbGrid(0, 4, 4, 2.0)
+    assert L.pb_dose(ctypes.byref(g), None, 1, None, None, None, None, 1.0, None, None,
+                     None) == _lib.PB_ERR_INVALID
+    assert "dimensions" in _lib.last_error()
+    g = _lib.PbGrid(4, 4, 4, 2.0)
+    assert L.pb_dose(ctypes.byref(g), None, 0, None, None, None, None, 1.0, None, None,
+                     None) == _lib.PB_ERR_INVALID
+    assert L.pb_wet(None, 0, ctypes.byref(g), None, 1, None, None, None, None) == _lib.PB_ERR_INVALID
+    g = _lib.PbGrid(4, 4, 4, -1.0)
+    assert L.pb_wet(None, 0, ctypes.byref(g), None, 1, None, None, None, None) == _lib.PB_ERR_INVALID
+    xh = np.array([0.0, 0.0], np.float64)
+    yh = np.array([1.0, 2.0], np.float64)
+    assert L.pb_rlsp_from_hu(ctypes.c_void_p(1), 4, _lib.ptr(xh), _lib.ptr(yh), 2,
+                             ctypes.c_void_p(1), None) == _lib.PB_ERR_INVALID
+    assert "increasing" in _lib.last_error()
+    assert L.pb_objective(None, None, None, 4, None, None, None, None) == _lib.PB_ERR_INVALID
+    assert L.pb_objective_work_size() >= 8
+    dims = np.array([0, 4, 4], np.int64)
+    buf = np.zeros(16, np.float32)
+    assert L.pb_proton_raytrace_host(0, 1340.0, 1930.0, _lib.ptr(buf), _lib.ptr(dims),
+                                     ctypes.c_float(2.0), _lib.ptr(buf), _lib.ptr(buf), 0.0, 0.0,
+                                     _lib.ptr(buf)) == _lib.PB_ERR_INVALID

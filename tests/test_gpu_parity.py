@@ -1,0 +1,359 @@
+"""Parity of the CUDA path with the FP64 oracle and with the reference's own
+CUDA module (oracle/_ref), through the package's C-ABI.
+
+Tolerances (fractions of the reference dose maximum Dmax unless stated):
+  * exact-trilinear WET vs FP64 oracle:          |dWET| <= 1e-4 cm
+  * dose vs FP64 oracle (same decisions):         <= 1e-3 Dmax  (0.1 %)
+  * pencil-beam pass alone (same WET):            <= 2e-4 Dmax
+  * texture-mode WET / dose vs reference module:  <= 1e-3 Dmax
+  * spot-weight gradient vs central differences:  <= 1e-3 of max |g|
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import cuda_available, max_rel
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+DEV = torch.device("cuda", 0)
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    import dosecuda_b200
+    from dosecuda_b200 import engine, phantoms, plan_impt
+    return dosecuda_b200, engine, phantoms, plan_impt
+
+
+@pytest.fixture(scope="module")
+def curve(pkg):
+    return pkg[3]._hu_curve("HitachiProbeatJHU")
+
+
+@pytest.fixture(scope="module")
+def small(pkg):
+    return pkg[2].small_heterogeneous()
+
+
+@pytest.fixture(scope="module")
+def cube(pkg):
+    return pkg[2].water_cube()
+
+
+def _vol(data, grid):
+    from dosecuda_b200.plan import VolumeObject
+    v = VolumeObject()
+    v.voxel_data = np.ascontiguousarray(data, np.float32)
+    v.origin = np.array(grid.origin, np.float32)
+    v.spacing = np.array(grid.spacing, np.float32)
+    return v
+
+
+def _model(plan, beam):
+    labels = list(plan.dicom_rangeshifter_label.astype(str))
+    return plan.beam_models[labels.index(beam.dicom_rangeshifter_label)]
+
+
+def _oracle_beam(O, grid, beam, model):
+    m = O.Model(model)
+    ob = O.beam_setup(beam.gantry_angle, beam.couch_angle, m.vsadx, m.vsady, beam.iso,
+                      grid.origin)
+    spots, layers = O.build_layers(np.asarray(beam.spot_list, np.float32).reshape(-1, 4), m.dvp)
+    return m, ob, spots, layers
+
+
+# ----------------------------------------------------------------- HU->RLSP
+
+def test_rlsp_bitwise_numpy_interp(pkg, curve):
+    engine = pkg[1]
+    rng = np.random.default_rng(0)
+    hu = np.concatenate([rng.uniform(-1500, 4000, 200000).astype(np.float32),
+                         curve[0].astype(np.float32),
+                         np.array([-1e6, 1e6, 0.0, -1000.0, 3096.0, 1369.0], np.float32)])
+    got = engine.rlsp_from_hu(torch.from_numpy(hu).to(DEV), *curve).cpu().numpy()
+    want = np.array(np.interp(hu, *curve), dtype=np.single)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+# ------------------------------------------------------- exact mode vs oracle
+
+def test_wet_exact_matches_oracle(pkg, small, curve, oracle):
+    g = small.grid
+    dp = g.prepareIMPTPlan(small.plan, 0, wet_mode="exact")
+    wet = dp.wet.cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
+    rlsp = oracle.rlsp_from_hu(g.HU, *curve)
+    for b, beam in enumerate(small.plan.beam_list):
+        _, ob, _, _ = _oracle_beam(oracle, g, beam, _model(small.plan, beam))
+        raw = oracle.raytrace(rlsp, g.spacing[0], ob).astype(np.float32)
+        sm = oracle.smooth(raw, g.spacing[0], ob)
+        assert np.abs(wet[b] - sm).max() <= 1e-4
+
+
+def test_dose_exact_matches_oracle(pkg, small, cube, curve, oracle):
+    for case in (small, cube):
+        g, plan = case.grid, case.plan
+        dp = g.prepareIMPTPlan(plan, 0, wet_mode="exact")
+        dose, bd = dp.forward(beam_doses=True)
+        bd = bd.cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
+        beams = [(b.gantry_angle, b.couch_angle, b.iso, b.spot_list, _model(plan, b))
+                 for b in plan.beam_list]
+        ref = oracle.plan_forward(g.HU, g.origin, g.spacing[0], beams, curve)
+        assert max_rel(dose.cpu().numpy().reshape(g.HU.shape), ref["dose"]) <= 1e-3
+        for b in range(dp.n_beams):
+            assert max_rel(bd[b], ref["beam_dose"][b]) <= 1e-3
+
+
+def test_pencil_beam_pass_matches_oracle_same_wet(pkg, small, oracle):
+    engine = pkg[1]
+    g, plan = small.grid, small.plan
+    dp = g.prepareIMPTPlan(plan, 0, wet_mode="exact")
+    wet = dp.wet.cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
+    bd = dp.forward(beam_doses=True)[1].cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
+    for b, beam in enumerate(plan.beam_list):
+        m, ob, spots, layers = _oracle_beam(oracle, g, beam, _model(plan, beam))
+        want = oracle.dose(wet[b], g.spacing[0], ob, m, spots, layers)
+        assert max_rel(bd[b], want) <= 2e-4
+    del engine
+
+
+# ------------------------------------------- texture mode vs the reference
+
+def _reference_plan(ref, case, curve):
+    g, plan = case.grid, case.plan
+    rlsp = np.array(np.interp(g.HU, *curve), dtype=np.single)
+    wets, doses = [], []
+    for beam in plan.beam_list:
+        model = _model(plan, beam)
+        w = ref.proton_raytrace_cuda(model, _vol(rlsp, g), beam, 0)
+        beam.spot_list = np.asarray(beam.spot_list, np.float32).reshape(-1, 4)
+        d = ref.proton_spot_cuda(model, _vol(rlsp, g), _vol(w, g), beam, 0)
+        wets.append(w)
+        doses.append(d)
+    return wets, doses
+
+
+def test_texture_mode_matches_reference(pkg, small, cube, curve, reference_module):
+    for case in (small, cube):
+        g = case.grid
+        dp = g.prepareIMPTPlan(case.plan, 0, wet_mode="texture")
+        wet = dp.wet.cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
+        bd = dp.forward(beam_doses=True)[1].cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
+        rw, rd = _reference_plan(reference_module, case, curve)
+        for b in range(dp.n_beams):
+            assert np.quantile(np.abs(wet[b] - rw[b]), 0.999) <= 1e-4
+            assert max_rel(bd[b], rd[b]) <= 1e-3
+
+
+def test_pencil_beam_pass_matches_reference_same_wet(pkg, small, curve, reference_module):
+    engine = pkg[1]
+    g, plan = small.grid, small.plan
+    rw, rd = _reference_plan(reference_module, small, curve)
+    for b, beam in enumerate(plan.beam_list):
+        dp = engine.DevicePlan(g.HU.shape, float(g.spacing[0]), np.asarray(g.origin, np.float32),
+                               [engine.BeamSpec(beam.gantry_angle, beam.couch_angle, beam.iso,
+                                                beam.spot_list, _model(plan, beam))], DEV)
+        dp.set_wet(torch.from_numpy(rw[b]).to(DEV))
+        assert max_rel(dp.forward().cpu().numpy().reshape(g.HU.shape), rd[b]) <= 2e-4
+
+
+def test_dose_kernels_dropin_matches_reference(pkg, small, curve, reference_module):
+    from dosecuda_b200 import dose_kernels as mine
+    g, plan = small.grid, small.plan
+    rlsp = np.array(np.interp(g.HU, *curve), dtype=np.single)
+    for beam in plan.beam_list:
+        model = _model(plan, beam)
+        beam.spot_list = np.asarray(beam.spot_list, np.float32).reshape(-1, 4)
+        w_ref = reference_module.proton_raytrace_cuda(model, _vol(rlsp, g), beam, 0)
+        w_mine = mine.proton_raytrace_cuda(model, _vol(rlsp, g), beam, 0)
+        assert w_mine.dtype == np.float32 and w_mine.shape == w_ref.shape
+        assert np.quantile(np.abs(w_mine - w_ref), 0.999) <= 1e-4
+        d_ref = reference_module.proton_spot_cuda(model, _vol(rlsp, g), _vol(w_ref, g), beam, 0)
+        d_mine = mine.proton_spot_cuda(model, _vol(rlsp, g), _vol(w_ref, g), beam, 0)
+        assert max_rel(d_mine, d_ref) <= 2e-4
+
+
+def test_compute_plan_matches_reference_loop(pkg, small, curve, reference_module):
+    g, plan = small.grid, small.plan
+    plan.n_fractions = 3
+    try:
+        g.computeIMPTPlan(plan, 0)
+        rw, rd = _reference_plan(reference_module, small, curve)
+        want = np.zeros(g.HU.shape, np.float32)
+        for d in rd:
+            want += d
+        want *= plan.n_fractions
+        assert g.dose.shape == g.HU.shape and g.dose.dtype == np.float32
+        assert max_rel(g.dose, want) <= 1e-3
+        for b, d in enumerate(rd):
+            assert max_rel(g.beam_doses[b], d * plan.n_fractions) <= 1e-3
+        assert np.array_equal(g.RLSP, np.array(np.interp(g.HU, *curve), dtype=np.single))
+    finally:
+        plan.n_fractions = 1
+
+
+def test_negative_energy_id_gives_zero_dose_like_reference(pkg, small, curve):
+    """A negative energy id sorts first and blocks every layer in importLayers
+    (IMPTClasses.cu:37-67): the reference returns a zero dose."""
+    from dosecuda_b200 import dose_kernels as mine
+    g, plan = small.grid, small.plan
+    beam = plan.beam_list[0]
+    sl = np.array(beam.spot_list, np.float32).reshape(-1, 4).copy()
+    sl[0, 3] = -1.0
+    from dosecuda_b200.plan_impt import IMPTBeam
+    b2 = IMPTBeam(beam)
+    b2.spot_list = sl
+    rlsp = np.array(np.interp(g.HU, *curve), dtype=np.single)
+    w = np.ones(g.HU.shape, np.float32)
+    d_mine = mine.proton_spot_cuda(_model(plan, beam), _vol(rlsp, g), _vol(w, g), b2, 0)
+    assert not d_mine.any()
+
+
+# -------------------------------------------------------------- gradient
+
+def test_adjoint_matches_oracle(pkg, small, oracle):
+    g, plan = small.grid, small.plan
+    dp = g.prepareIMPTPlan(plan, 0, wet_mode="exact")
+    shape = g.HU.shape
+    w = np.random.default_rng(1).normal(size=shape).astype(np.float32)
+    got = dp.adjoint(torch.from_numpy(w.reshape(-1)).to(DEV)).cpu().numpy()
+    wet = dp.wet.cpu().numpy().reshape(dp.n_beams, *shape)
+    want = []
+    for b, beam in enumerate(plan.beam_list):
+        m, ob, spots, layers = _oracle_beam(oracle, g, beam, _model(plan, beam))
+        want.append(oracle.adjoint(wet[b], g.spacing[0], ob, m, spots, layers,
+                                   w.astype(np.float64)))
+    want = np.concatenate(want)
+    assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max()
+
+
+def test_gradient_central_differences(pkg, small, oracle):
+    """d(objective)/d(mu) from the adjoint kernel vs FP64 central differences
+    of the oracle objective on 200 seeded spots."""
+    g, plan = small.grid, small.plan
+    presc, wts = small.presc, small.weights
+    obj, grad = g.computeIMPTPlanGradient(plan, presc, wts, 0, wet_mode="exact")
+    dp = g.prepareIMPTPlan(plan, 0, wet_mode="exact")
+    shape = g.HU.shape
+    wet = dp.wet.cpu().numpy().reshape(dp.n_beams, *shape)
+    # FP64 oracle dose and single-spot columns (dose is linear in mu)
+    D = np.zeros(shape)
+    cols = []  # (plan row, beam, sorted index)
+    per_beam = []
+    for b, beam in enumerate(plan.beam_list):
+        m, ob, spots, layers = _oracle_beam(oracle, g, beam, _model(plan, beam))
+        D += oracle.dose(wet[b], g.spacing[0], ob, m, spots, layers)
+        per_beam.append((m, ob, np.asarray(beam.spot_list, np.float32).reshape(-1, 4)))
+    nrow = [len(pb[2]) for pb in per_beam]
+    rng = np.random.default_rng(42)
+    picks = rng.choice(sum(nrow), size=min(200, sum(nrow)), replace=False)
+    offs = np.cumsum([0] + nrow)
+    presc64 = presc.astype(np.float64)
+    w64 = wts.astype(np.float64)
+
+    def objective(Dv):
+        return float(np.sum(w64 * (Dv - presc64) ** 2))
+
+    fd = []
+    for p in picks:
+        b = int(np.searchsorted(offs, p, side="right") - 1)
+        row = int(p - offs[b])
+        m, ob, sl = per_beam[b]
+        one = sl[row:row + 1].copy()
+        mu = float(one[0, 2])
+        one[0, 2] = 1.0
+        spots, layers = oracle.build_layers(one, m.dvp)
+        col = oracle.dose(wet[b], g.spacing[0], ob, m, spots, layers)
+        h = 1e-3 * max(abs(mu), 1.0)
+        fd.append((objective(D + h * col) - objective(D - h * col)) / (2 * h))
+    fd = np.array(fd)
+    err = np.abs(grad[picks] - fd)
+    assert err.max() <= 1e-3 * np.abs(fd).max()
+    assert abs(obj - objective(D)) <= 1e-4 * objective(D)
+
+
+def test_autograd_backward_is_adjoint(pkg, small):
+    from dosecuda_b200 import autograd
+    g, plan = small.grid, small.plan
+    dp = g.prepareIMPTPlan(plan, 0)
+    mu = dp.mu_plan().clone().requires_grad_(True)
+    presc = torch.from_numpy(small.presc.reshape(-1)).to(DEV)
+    w = torch.from_numpy(small.weights.reshape(-1)).to(DEV)
+    d = autograd.dose(mu, dp)
+    obj = autograd.quadratic_objective(d, presc, w)
+    obj.backward()
+    o2, g2 = autograd.plan_objective_and_grad(dp, small.presc, small.weights)
+    assert abs(float(obj.detach()) - o2) <= 1e-9 * abs(o2)
+    # the adjoint's cross-tile sums use float atomics: equal up to rounding
+    assert np.allclose(mu.grad.cpu().numpy(), g2, rtol=1e-5, atol=1e-5 * np.abs(g2).max())
+    d64 = d.detach().double()
+    want = float(torch.sum(w.double() * (d64 - presc.double()) ** 2))
+    assert abs(float(obj.detach()) - want) <= 1e-9 * want
+
+
+# ----------------------------------------------- full-size properties
+
+def test_full_size_linearity_additivity_determinism(pkg):
+    phantoms = pkg[2]
+    case = phantoms.config_forward_heterogeneous()
+    dp = case.grid.prepareIMPTPlan(case.plan, 0)
+    d1, bd = dp.forward(beam_doses=True)
+    d1b = dp.forward()
+    assert torch.equal(d1, d1b)                                  # deterministic
+    d2 = dp.forward(dp.mu_sorted * 2.0)
+    assert torch.allclose(d2, 2.0 * d1, rtol=1e-5, atol=1e-6 * float(d1.max()))  # linear in mu
+    assert torch.allclose(bd.sum(0), d1, rtol=1e-5, atol=1e-6 * float(d1.max()))  # beams add up
+    assert float(d1.max()) > 0
+
+
+def test_full_size_sampled_voxels_vs_oracle(pkg, oracle, curve):
+    """Heterogeneous 256x256x160 plan: raw WET, smoothed WET and dose at
+    sampled voxels (the hottest and a random set) against the oracle."""
+    phantoms = pkg[2]
+    case = phantoms.config_forward_heterogeneous()
+    g, plan = case.grid, case.plan
+    dp = g.prepareIMPTPlan(plan, 0, wet_mode="exact")
+    dose = dp.forward().cpu().numpy()
+    wet = dp.wet.cpu().numpy()
+    raw = dp.raw_wet.cpu().numpy()
+    rng = np.random.default_rng(3)
+    idx = np.unique(np.concatenate([np.argsort(dose)[-400:],
+                                    rng.choice(dose.size, 600, replace=False)])).astype(np.int64)
+    rlsp = oracle.rlsp_from_hu(g.HU, *curve)
+    want = np.zeros(len(idx))
+    for b, beam in enumerate(plan.beam_list):
+        m, ob, spots, layers = _oracle_beam(oracle, g, beam, _model(plan, beam))
+        raw_o = oracle.raytrace(rlsp, g.spacing[0], ob, idx)
+        assert np.abs(raw[b][idx] - raw_o).max() <= 1e-4
+        sm_o = oracle.smooth(raw[b].reshape(g.HU.shape), g.spacing[0], ob, idx)
+        assert np.abs(wet[b][idx] - sm_o).max() <= 1e-4
+        want += oracle.dose(wet[b].reshape(g.HU.shape), g.spacing[0], ob, m, spots, layers, idx)
+    assert np.abs(dose[idx] - want).max() <= 2e-4 * dose.max()
+
+
+def test_count_pairs_matches_oracle(pkg, small, oracle):
+    g, plan = small.grid, small.plan
+    dp = g.prepareIMPTPlan(plan, 0)
+    wet = dp.wet.cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
+    want = 0
+    for b, beam in enumerate(plan.beam_list):
+        _, _, _, layers = _oracle_beam(oracle, g, beam, _model(plan, beam))
+        want += oracle.count_pairs(wet[b], layers)
+    assert dp.count_pairs() == want
+
+
+# ------------------------------------------------------------ error paths
+
+def test_invalid_device_raises_runtime_error(pkg, small, curve):
+    from dosecuda_b200 import dose_kernels as mine
+    g, plan = small.grid, small.plan
+    beam = plan.beam_list[0]
+    rlsp = np.array(np.interp(g.HU, *curve), dtype=np.single)
+    with pytest.raises(RuntimeError, match="CUDA error"):
+        mine.proton_raytrace_cuda(_model(plan, beam), _vol(rlsp, g), beam, 97)
+
+
+def test_ray_cap_status_is_zero_on_valid_geometry(pkg, small):
+    dp = small.grid.prepareIMPTPlan(small.plan, 0)
+    assert int(dp._status.item()) == 0

@@ -1,0 +1,97 @@
+"""The oracle pinned against the reference's own outputs (tests/golden/*.npz,
+made by tests/golden/make_golden.py from the reference CUDA module).
+
+Pins, as fractions of the reference beam-dose maximum Dmax:
+  * pencil-beam pass on the reference's WET:  |D_oracle - D_ref| <= 2e-5 Dmax
+    (FP64 oracle vs the FP32 reference kernel: the pass is pinned exactly).
+  * WET: the reference samples RLSP through the texture unit (8-bit filter
+    weights); the oracle uses exact trilinear weights.  Median |dWET| <=
+    5e-4 cm and 99th percentile <= 3e-3 cm; the smoothing step's
+    `dr < 10*WET` test can still flip at shallow voxels, so the maximum is
+    not pinned here.
+  * full pipeline (oracle WET + oracle pass) vs reference: <= 5e-3 Dmax,
+    the texture-filter effect.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+FILES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+@pytest.fixture(scope="module")
+def plan():
+    from dosecuda_b200.plan_impt import IMPTPlan
+    return IMPTPlan()
+
+
+def _beams(z, plan, oracle):
+    labels = list(plan.dicom_rangeshifter_label.astype(str))
+    for b in range(int(z["n_beams"])):
+        model = plan.beam_models[labels.index(str(z[f"b{b}_label"]))]
+        m = oracle.Model(model)
+        ob = oracle.beam_setup(float(z[f"b{b}_gantry"]), float(z[f"b{b}_couch"]), m.vsadx,
+                               m.vsady, z[f"b{b}_iso"], z["origin"])
+        spots, layers = oracle.build_layers(z[f"b{b}_spots"], m.dvp)
+        yield b, m, ob, spots, layers
+
+
+def test_golden_files_present():
+    assert len(FILES) >= 3
+
+
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_oracle_pencil_beam_pass_matches_reference(path, plan, oracle):
+    z = np.load(path)
+    for b, m, ob, spots, layers in _beams(z, plan, oracle):
+        ref = z[f"b{b}_dose"]
+        got = oracle.dose(z[f"b{b}_wet"], z["spacing"][0], ob, m, spots, layers)
+        assert np.abs(got - ref).max() <= 2e-5 * ref.max()
+
+
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_oracle_wet_and_dose_match_reference(path, plan, oracle):
+    z = np.load(path)
+    rlsp = oracle.rlsp_from_hu(z["hu"], z["curve_hu"], z["curve_rlsp"])
+    for b, m, ob, spots, layers in _beams(z, plan, oracle):
+        raw = oracle.raytrace(rlsp, z["spacing"][0], ob).astype(np.float32)
+        wet = oracle.smooth(raw, z["spacing"][0], ob).astype(np.float32)
+        dw = np.abs(wet - z[f"b{b}_wet"])
+        assert np.median(dw) <= 5e-4
+        assert np.quantile(dw, 0.99) <= 3e-3
+        ref = z[f"b{b}_dose"]
+        got = oracle.dose(wet, z["spacing"][0], ob, m, spots, layers)
+        assert np.abs(got - ref).max() <= 5e-3 * ref.max()
+
+
+def test_rlsp_is_numpy_interp_of_the_machine_curve(plan, oracle):
+    z = np.load(FILES[0])
+    from dosecuda_b200.plan_impt import _hu_curve
+    xh, yh = _hu_curve("HitachiProbeatJHU")
+    assert np.array_equal(xh, z["curve_hu"]) and np.array_equal(yh, z["curve_rlsp"])
+    assert np.array_equal(oracle.rlsp_from_hu(z["hu"], xh, yh),
+                          np.array(np.interp(z["hu"], xh, yh), dtype=np.single))
+
+
+def test_oracle_adjoint_equals_central_differences(plan, oracle):
+    """The FP64 adjoint sum_v w_v K(v, s) is the derivative of
+    sum_v w_v D_v(mu) with respect to mu_s (central differences)."""
+    z = np.load(os.path.join(GOLDEN, "hetero_two_beams.npz"))
+    for b, m, ob, spots, layers in _beams(z, plan, oracle):
+        wet = z[f"b{b}_wet"]
+        rng = np.random.default_rng(b)
+        w = rng.normal(size=wet.shape)
+        g = oracle.adjoint(wet, z["spacing"][0], ob, m, spots, layers, w)
+        for s in rng.choice(len(spots), size=min(5, len(spots)), replace=False):
+            h = 2.0 ** -10          # exact in the FP32 weight field
+            sp = spots.copy()
+            sp["mu"][s] += h
+            dp = oracle.dose(wet, z["spacing"][0], ob, m, sp, layers)
+            sp["mu"][s] -= 2 * h
+            dm = oracle.dose(wet, z["spacing"][0], ob, m, sp, layers)
+            fd = float(np.sum(w * (dp - dm)) / (2 * h))
+            assert abs(fd - g[s]) <= 1e-7 * max(1.0, np.abs(g).max())

@@ -1,0 +1,192 @@
+"""The reference-compatible plan API on the host: beam-model parsing, spot
+bookkeeping, phantoms, NRRD I/O, the dose_kernels attribute contract and
+the errors raised before any device work."""
+import glob
+import os
+import types
+
+import numpy as np
+import pytest
+
+from conftest import PKG_DIR
+
+
+@pytest.fixture(scope="module")
+def plan():
+    from dosecuda_b200.plan_impt import IMPTPlan
+    return IMPTPlan()
+
+
+LUT_DIR = os.path.join(PKG_DIR, "dosecuda_b200", "lookuptables", "protons", "HitachiProbeatJHU")
+
+
+def test_machine_models_parse(plan):
+    assert list(plan.dicom_rangeshifter_label.astype(str)) == ["0", "4"]
+    for model, folder in zip(plan.beam_models, ["RS0", "RS4"]):
+        assert model.VSADX == 1340.0 and model.VSADY == 1930.0
+        assert model.divergence_params.shape == (98, 5)
+        assert model.lut_depths.shape == (98, 400) and model.lut_depths.dtype == np.float32
+        files = sorted(glob.glob(os.path.join(LUT_DIR, folder, "energy_*.csv")))
+        assert len(files) == 98
+        for e, f in enumerate(files):
+            rows = np.loadtxt(f, delimiter=",", skiprows=4, max_rows=400, dtype=np.float64)
+            head = np.loadtxt(f, delimiter=",", skiprows=1, max_rows=1, dtype=np.float64)
+            assert np.array_equal(model.lut_depths[e], rows[:, 0].astype(np.float32))
+            assert np.array_equal(model.lut_sigmas[e], rows[:, 1].astype(np.float32))
+            assert np.array_equal(model.lut_idds[e], rows[:, 2].astype(np.float32))
+            assert np.array_equal(model.divergence_params[e], head.astype(np.float32))
+    m = plan.beam_models[0]
+    assert m.energyIDFromLabel(70.2) == 0 and m.energyIDFromLabel(228.7) == 97
+    with pytest.raises(Exception, match="Energy ID not found"):
+        m.energyIDFromLabel(1.0)
+
+
+def test_beam_spot_api():
+    from dosecuda_b200.plan_impt import IMPTBeam
+    b = IMPTBeam()
+    b.addSingleSpot(1.0, 2.0, 0.5, 3)
+    assert b.spot_list.shape == (4,) and b.n_spots == 1      # the reference's 1-D quirk
+    b.addSingleSpot(-1.0, 0.0, 1.5, 4)
+    assert b.spot_list.shape == (2, 4) and b.spot_list.dtype == np.float32
+    cp = types.SimpleNamespace(ScanSpotPositionMap=[0, 0, 5, 5, -5, 5],
+                               ScanSpotMetersetWeights=[0.1, 0.2, 0.3])
+    b.addSpotData(cp, 7)
+    assert b.n_spots == 5 and list(b.spot_list[-1]) == [-5.0, 5.0, 0.3, 7.0]
+    b.changeSpotEnergy(2)
+    assert set(b.spot_list[:, 3]) == {2.0}
+    c = IMPTBeam(b)
+    assert c.n_spots == 5 and c.spot_list is b.spot_list
+    b.resetSpots()
+    assert b.spot_list.shape == (0, 4) and b.n_spots == 0
+
+
+def test_plan_add_beam_names(plan):
+    from dosecuda_b200.plan_impt import IMPTBeam, IMPTPlan
+    p = IMPTPlan()
+    p.addBeam(IMPTBeam())
+    p.addBeam(IMPTBeam())
+    assert [b.BeamName for b in p.beam_list] == ["PBS_Beam1", "PBS_Beam2"]
+    p.addPrescription(60.0, "PTV", 0.02)
+    assert p.Prescriptions[0].ROIName == "PTV"
+
+
+def test_cube_phantom_like_reference():
+    from dosecuda_b200.plan_impt import IMPTDoseGrid
+    g = IMPTDoseGrid()
+    g.createCubePhantom()
+    assert g.HU.shape == (138, 138, 138) and g.HU.dtype == np.float32
+    assert np.allclose(g.origin, -207.0) and np.allclose(g.spacing, 3.0)
+    edge = round(10.0 / 3.0)
+    assert g.HU[0, 0, 0] == -1000.0 and g.HU[edge, edge, edge] == 0.0
+    assert g.HU[edge - 1, 70, 70] == -1000.0
+
+
+def test_couch_model():
+    from dosecuda_b200.plan_impt import IMPTDoseGrid
+    g = IMPTDoseGrid()
+    g.createCubePhantom(size=[20, 30, 20], spacing=5.0)
+    g.applyCouchModel(couch_wet=8.0)
+    n = int(50.0 / 5.0)
+    assert np.allclose(g.HU[:, -n:, :], ((8.0 / (n * 5.0)) - 1.0) * 1000.0)
+
+
+def test_nrrd_roundtrip(tmp_path):
+    from dosecuda_b200 import nrrd
+    from dosecuda_b200.plan_impt import IMPTDoseGrid
+    rng = np.random.default_rng(0)
+    vol = rng.normal(size=(5, 6, 7)).astype(np.float32)
+    for compress in (False, True):
+        p = str(tmp_path / f"v{compress}.nrrd")
+        nrrd.write(p, vol, [-1.0, 2.0, 3.5], [2.0, 2.0, 2.5], compress=compress)
+        v2, o, s = nrrd.read(p)
+        assert np.array_equal(v2, vol) and np.allclose(o, [-1, 2, 3.5]) and np.allclose(s, [2, 2, 2.5])
+    g = IMPTDoseGrid()
+    g.createCubePhantom(size=[8, 9, 10], spacing=4.0)
+    g.dose = np.ones(g.HU.shape, np.float32)
+    g.beam_doses = [g.dose * 2]
+    g.writeDoseNRRD(str(tmp_path / "d.nrrd"), individual_beams=True, dose_type="PHYSICAL")
+    v, _, _ = nrrd.read(str(tmp_path / "d_beam01.nrrd"))
+    assert np.allclose(v, 2.0)
+    g.writeDoseNRRD(str(tmp_path / "e.nrrd"))
+    v, _, _ = nrrd.read(str(tmp_path / "e.nrrd"))
+    assert np.allclose(v, 1.1)
+    g.writeCTNRRD(str(tmp_path / "ct.nrrd"))
+    g2 = IMPTDoseGrid()
+    g2.loadCTNRRD(str(tmp_path / "ct.nrrd"))
+    assert np.array_equal(g2.HU, g.HU) and np.allclose(g2.origin, g.origin)
+    with pytest.raises(Exception, match="extension"):
+        g.writeDoseNRRD(str(tmp_path / "d.txt"))
+    with pytest.raises(Exception, match="Unknown dose type"):
+        g.writeDoseNRRD(str(tmp_path / "d.nrrd"), dose_type="X")
+
+
+class _Obj:
+    pass
+
+
+def _args():
+    from dosecuda_b200.plan_impt import IMPTPlan
+    model = IMPTPlan().beam_models[0]
+    vol = _Obj()
+    vol.voxel_data = np.zeros((4, 4, 4), np.float32)
+    vol.spacing = np.ones(3, np.float32)
+    vol.origin = np.zeros(3, np.float32)
+    beam = _Obj()
+    beam.iso = np.zeros(3, np.float32)
+    beam.gantry_angle = 0.0
+    beam.couch_angle = 0.0
+    beam.spot_list = np.zeros((2, 4), np.float32)
+    return model, vol, beam
+
+
+def test_dose_kernels_attribute_contract():
+    """dosemodule.cu:23-101: rank/dtype -> ValueError with the reference's
+    message, missing attribute -> AttributeError, non-number -> TypeError;
+    all raised before any device work."""
+    from dosecuda_b200 import dose_kernels as dk
+    model, vol, beam = _args()
+    vol.voxel_data = np.zeros((4, 4, 4), np.float64)
+    with pytest.raises(ValueError, match="'voxel_data' must be 3-dimensional and of type float."):
+        dk.proton_raytrace_cuda(model, vol, beam, 0)
+    model, vol, beam = _args()
+    beam.spot_list = np.zeros(4, np.float32)          # 1-spot beams are 1-D: rejected
+    with pytest.raises(ValueError, match="'spot_list' must be 2-dimensional"):
+        dk.proton_spot_cuda(model, vol, vol, beam, 0)
+    model, vol, beam = _args()
+    del beam.iso
+    with pytest.raises(AttributeError):
+        dk.proton_raytrace_cuda(model, vol, beam, 0)
+    model, vol, beam = _args()
+    beam.gantry_angle = "90"
+    with pytest.raises(TypeError):
+        dk.proton_raytrace_cuda(model, vol, beam, 0)
+
+
+def test_plan_errors_before_device_work(plan):
+    from dosecuda_b200.plan_impt import IMPTBeam, IMPTDoseGrid
+    g = IMPTDoseGrid()
+    g.createCubePhantom(size=[8, 8, 8], spacing=3.0)
+    g.spacing = np.array([3.0, 3.0, 2.0])
+    with pytest.raises(Exception, match="isotropic"):
+        g.computeIMPTPlan(plan)
+    g.spacing = np.array([3.0, 3.0, 3.0])
+    b = IMPTBeam()
+    b.dicom_rangeshifter_label = "9"
+    b.addSingleSpot(0, 0, 1, 10)
+    from dosecuda_b200.plan_impt import IMPTPlan
+    p = IMPTPlan()
+    p.addBeam(b)
+    with pytest.raises(SystemExit):
+        g._specs(p, p.beam_list)
+
+
+def test_phantoms_are_seeded():
+    from dosecuda_b200 import phantoms
+    a = phantoms.small_heterogeneous(seed=4)
+    b = phantoms.small_heterogeneous(seed=4)
+    assert np.array_equal(a.grid.HU, b.grid.HU)
+    assert all(np.array_equal(x.spot_list, y.spot_list)
+               for x, y in zip(a.plan.beam_list, b.plan.beam_list))
+    c = phantoms.water_cube()
+    assert c.grid.HU.shape == (120, 120, 120) and c.n_spots == 121 * 10
+    assert (c.grid.HU == 0).sum() == 80 ** 3
