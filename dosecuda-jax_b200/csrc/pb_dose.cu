@@ -14,28 +14,34 @@
 //   t x ray = ( Y - ys(1-Z/VSADY), -(X - xs(1-Z/VSADX)),
 //               (xs/VSADX) Y - (ys/VSADY) X - xs ys (1/VSADX - 1/VSADY) ).
 //
-// Work decomposition: one block of 256 threads per 8x8x8 voxel tile, two
-// voxels per thread; all beams and layers of the plan are looped inside
-// the block, so each voxel's dose is written once, compensated (Neumaier)
-// across layers and beams, with no atomics.  Per (tile, layer) the layer's
-// LUT row is staged in shared memory and the layer's spots are culled
-// against the tile: a spot is skipped when, for every voxel of the tile,
-// its Gaussian factor is below 2^-24 of the voxel's peak factor (bound from
-// the tile's BEV box and the widest halo sigma in the tile).  Surviving
-// spots are compacted into shared memory and streamed by every thread.
+// Forward work decomposition: one block of 128 threads per 8x8x8 voxel
+// tile, four voxels per thread; all beams and layers of the plan are looped
+// inside the block, so each voxel's dose is written once, compensated
+// (Neumaier) across layers and beams, with no atomics.  Per (tile, layer)
+// the layer's LUT row is staged in shared memory and the layer's spots are
+// culled against the tile: a spot is skipped when, for every voxel of the
+// tile, its Gaussian factor is below 2^-24 of the voxel's peak factor (bound
+// from the tile's BEV box and the widest halo sigma in the tile).  Surviving
+// spots are compacted into shared memory (each value stored twice), and
+// every thread evaluates each spot on its four voxels as two packed FP32x2
+// voxel pairs (two spot-voxel pairs per instruction) with the SFU's ex2.
 //
 // The adjoint uses the same tiles and culling; per (tile, layer) the active
 // voxels (dObj/dD != 0, inside the range cut) are compacted into shared
-// memory and each thread takes one surviving spot and reduces over them,
-// then adds its partial to the spot's gradient with one atomic.
+// memory; the surviving spots, taken as packed pairs, are split with the
+// voxels into (spot pair, voxel stripe) work items so that every thread is
+// busy; partial sums meet in shared memory and each spot's sum goes to its
+// gradient with one global atomic per (tile, layer).
 #include "pb_internal.h"
 
 namespace pb {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
-constexpr int kVpt = 2;            // voxels per thread
-constexpr float kCullLog2 = 24.0f; // skip factors below 2^-24
+constexpr int kVpt = 4;             // forward: voxels per thread (z, z+2, z+4, z+6)
+constexpr int kCull = 2;            // forward: spots culled per thread per chunk
+constexpr int kSpt = 4;             // adjoint: spots per thread per chunk
+constexpr float kCullLog2 = 24.0f;  // skip factors below 2^-24
 
 struct PlanArgs {
     PbGrid g;
@@ -45,19 +51,43 @@ struct PlanArgs {
     PbBeam beams[PB_MAX_BEAMS];
 };
 
+// One spot, each value duplicated, for packed FP32x2 evaluation against a
+// pair of voxels.
 struct __align__(16) SpotRec {
-    float4 a;  // (-x, -y, tx, -ty)
-    float4 b;  // (-cs, it2, mu, 0)
+    float4 a;  // (-x, -x, -y, -y)
+    float4 b;  // (tx, tx, -ty, -ty)
+    float4 c;  // (-cs, -cs, it2, it2)
+    float4 d;  // (mu, mu, 0, 0)
 };
 
+// One voxel's layer record, each value duplicated for FP32x2 use.
 struct __align__(16) VoxRec {
-    float4 a;  // (X, Y, gx, gy)
-    float4 b;  // (ps2, hs2, w*Pf, w*Hf)
+    float4 xy;   // (X, X, Y, Y)
+    float4 g;    // (gx, gx, gy, gy)
+    float4 s;    // (ps2, ps2, hs2, hs2)
+    float4 f;    // (w*Pf, w*Pf, w*Hf, w*Hf)
 };
 
 struct TileBounds {
     float x0, x1, y0, y1, gx0, gx1, gy0, gy1;
 };
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 lo2(const float4 &v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4 &v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 ex2x2(float2 a) { return make_float2(ex2(a.x), ex2(a.y)); }
+
+// Squared axis distance of two spots at one voxel, times 1/|t|^2.
+__device__ __forceinline__ float2 axis_r2(float2 nx, float2 ny, float2 tx, float2 nty,
+                                          float2 ncs, float2 it2, float2 X, float2 Y,
+                                          float2 GX, float2 GY)
+{
+    const float2 ax = __ffma2_rn(nx, GX, X);
+    const float2 ay = __ffma2_rn(ny, GY, Y);
+    const float2 cz = __ffma2_rn(tx, Y, __ffma2_rn(nty, X, ncs));
+    const float2 S = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(cz, cz)));
+    return __fmul2_rn(S, it2);
+}
 
 // Per-(voxel, layer) Gaussian parameters.  wet_mm is 10*WET (cm), dist the
 // distance to the source (mm).  Exponent scales are pre-multiplied by
@@ -129,15 +159,15 @@ __device__ __forceinline__ void neumaier(float &s, float &c, float x)
 }
 
 // Block-wide min/max of the tile's BEV box over valid voxels.
+template <int NV>
 __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y,
                                                   const float *GX, const float *GY,
-                                                  const bool *valid,
-                                                  float (*s_red)[9])
+                                                  const bool *valid, float (*s_red)[9])
 {
     float v[8] = {INFINITY, -INFINITY, INFINITY, -INFINITY,
                   INFINITY, -INFINITY, INFINITY, -INFINITY};
 #pragma unroll
-    for (int q = 0; q < kVpt; ++q) {
+    for (int q = 0; q < NV; ++q) {
         if (!valid[q]) continue;
         v[0] = fminf(v[0], X[q]);  v[1] = fmaxf(v[1], X[q]);
         v[2] = fminf(v[2], Y[q]);  v[3] = fmaxf(v[3], Y[q]);
@@ -152,14 +182,15 @@ __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y
         for (int m = 0; m < 8; ++m) s_red[warp][m] = v[m];
     }
     __syncthreads();
-    TileBounds tb;
     float r[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) r[m] = s_red[0][m];
     for (int w = 1; w < kWarps; ++w) {
 #pragma unroll
-        for (int m = 0; m < 8; ++m) r[m] = (m & 1) ? fmaxf(r[m], s_red[w][m]) : fminf(r[m], s_red[w][m]);
+        for (int m = 0; m < 8; ++m)
+            r[m] = (m & 1) ? fmaxf(r[m], s_red[w][m]) : fminf(r[m], s_red[w][m]);
     }
+    TileBounds tb;
     tb.x0 = r[0]; tb.x1 = r[1]; tb.y0 = r[2]; tb.y1 = r[3];
     tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
     return tb;
@@ -176,56 +207,46 @@ __device__ __forceinline__ float block_max_slot8(float v, float (*s_red)[9])
     return r;
 }
 
-struct VoxelGeom {
-    float X[kVpt], Y[kVpt], GX[kVpt], GY[kVpt], DIST[kVpt], WMM[kVpt];
-};
-
-__device__ __forceinline__ void beam_voxel_geom(const PbGrid &g, const PbBeam &B,
-                                                const float *__restrict__ wetb,
-                                                const int *vi, const int *vj,
-                                                const int *vk, const bool *valid,
-                                                const int64_t *vidx, VoxelGeom &o)
-{
-#pragma unroll
-    for (int q = 0; q < kVpt; ++q) {
-        if (valid[q]) {
-            float px, py, pz, hx, hy, hz;
-            vox_mm(B.geom, g.spacing, vi[q], vj[q], vk[q], px, py, pz);
-            image_to_head(B.geom, px, py, pz, hx, hy, hz);
-            o.X[q] = hx;
-            o.Y[q] = hy;
-            o.GX[q] = 1.0f - hz / B.geom.vsadx;
-            o.GY[q] = 1.0f - hz / B.geom.vsady;
-            const float dx = B.geom.src[0] - px, dy = B.geom.src[1] - py,
-                        dz = B.geom.src[2] - pz;
-            o.DIST[q] = sqrtf(dx * dx + dy * dy + dz * dz);
-            o.WMM[q] = __fmul_rn(__ldg(wetb + vidx[q]), 10.0f);
-        } else {
-            o.X[q] = o.Y[q] = 0.0f;
-            o.GX[q] = o.GY[q] = 1.0f;
-            o.DIST[q] = 0.0f;
-            o.WMM[q] = INFINITY;
-        }
-    }
-}
-
-__device__ __forceinline__ void tile_voxels(const PlanArgs &A, int *vi, int *vj,
-                                            int *vk, bool *valid, int64_t *vidx)
+// Voxels of this block's tile owned by this thread: (li, lj, lk + step*q).
+template <int NV>
+__device__ __forceinline__ void tile_voxels(const PlanArgs &A, int *vi, int *vj, int *vk,
+                                            bool *valid, int64_t *vidx)
 {
     int t = blockIdx.x;
     const int tx = t % A.tiles_x;
     t /= A.tiles_x;
     const int ty = t % A.tiles_y;
     const int tz = t / A.tiles_y;
+    constexpr int step = 8 / NV;
     const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
 #pragma unroll
-    for (int q = 0; q < kVpt; ++q) {
+    for (int q = 0; q < NV; ++q) {
         vi[q] = tx * 8 + li;
         vj[q] = ty * 8 + lj;
-        vk[q] = tz * 8 + lk + 4 * q;
+        vk[q] = tz * 8 + lk + step * q;
         valid[q] = vi[q] < A.g.nx && vj[q] < A.g.ny && vk[q] < A.g.nz;
         vidx[q] = valid[q] ? vi[q] + (int64_t)A.g.nx * (vj[q] + (int64_t)A.g.ny * vk[q]) : 0;
     }
+}
+
+// Head-frame position of a voxel and its divergence factors.
+__device__ __forceinline__ void voxel_head(const PbGrid &g, const PbBeam &B, int i, int j,
+                                           int k, float &X, float &Y, float &Z, float &gx,
+                                           float &gy)
+{
+    float px, py, pz;
+    vox_mm(B.geom, g.spacing, i, j, k, px, py, pz);
+    image_to_head(B.geom, px, py, pz, X, Y, Z);
+    gx = 1.0f - Z / B.geom.vsadx;
+    gy = 1.0f - Z / B.geom.vsady;
+}
+
+// Distance to the source, which sits at (0, 0, (VSADX+VSADY)/2) in the head
+// frame (CudaClasses.cu:17-51 rotated into the nozzle frame).
+__device__ __forceinline__ float source_distance(const PbBeam &B, float X, float Y, float Z)
+{
+    const float dz = 0.5f * (B.geom.vsadx + B.geom.vsady) - Z;
+    return sqrtf(fmaf(X, X, fmaf(Y, Y, dz * dz)));
 }
 
 __device__ __forceinline__ void stage_lut(const PbBeam &B, int e, float *s_dep,
@@ -241,22 +262,23 @@ __device__ __forceinline__ void stage_lut(const PbBeam &B, int e, float *s_dep,
 
 // ------------------------------------------------------------------ forward
 
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 4)
 k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
        const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
        const float *__restrict__ mu, float *__restrict__ dose,
        float *__restrict__ beam_dose)
 {
+    constexpr int NP = kVpt / 2;  // voxel pairs per thread
     __shared__ float s_dep[PB_MAX_LUT_LEN], s_sig[PB_MAX_LUT_LEN], s_idd[PB_MAX_LUT_LEN];
-    __shared__ SpotRec s_spot[kThreads];
+    __shared__ SpotRec s_spot[kThreads * kCull];
     __shared__ float s_red[kWarps][9];
-    __shared__ int s_wcount[kWarps];
+    __shared__ int s_wcount[kCull][kWarps];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int vi[kVpt], vj[kVpt], vk[kVpt];
     bool valid[kVpt];
     int64_t vidx[kVpt];
-    tile_voxels(A, vi, vj, vk, valid, vidx);
+    tile_voxels<kVpt>(A, vi, vj, vk, valid, vidx);
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
 
     float tot_s[kVpt], tot_c[kVpt];
@@ -265,9 +287,19 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
-        VoxelGeom vg;
-        beam_voxel_geom(A.g, B, wet + b * V, vi, vj, vk, valid, vidx, vg);
-        const TileBounds tb = tile_bounds(vg.X, vg.Y, vg.GX, vg.GY, valid, s_red);
+        float X[kVpt], Y[kVpt], Z[kVpt], GX[kVpt], GY[kVpt], WMM[kVpt];
+#pragma unroll
+        for (int q = 0; q < kVpt; ++q) {
+            if (valid[q]) {
+                voxel_head(A.g, B, vi[q], vj[q], vk[q], X[q], Y[q], Z[q], GX[q], GY[q]);
+                WMM[q] = __fmul_rn(__ldg(wet + b * V + vidx[q]), 10.0f);
+            } else {
+                X[q] = Y[q] = Z[q] = 0.0f;
+                GX[q] = GY[q] = 1.0f;
+                WMM[q] = INFINITY;
+            }
+        }
+        const TileBounds tb = tile_bounds<kVpt>(X, Y, GX, GY, valid, s_red);
         float bs_s[kVpt], bs_c[kVpt];
 #pragma unroll
         for (int q = 0; q < kVpt; ++q) bs_s[q] = bs_c[q] = 0.0f;
@@ -279,7 +311,7 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
             bool any = false;
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
-                act[q] = valid[q] && !(vg.WMM[q] > cut);
+                act[q] = valid[q] && !(WMM[q] > cut);
                 any |= act[q];
             }
             if (!__syncthreads_or(any)) continue;
@@ -291,58 +323,74 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
             float hmax = -INFINITY;
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
+                ps2[q] = hs2[q] = pf[q] = hf[q] = 0.0f;
                 if (act[q]) {
-                    layer_params(vg.WMM[q], vg.DIST[q], L.r80, s_dep, s_sig, s_idd,
-                                 B.lut_len, ca, cb, cc, pf[q], hf[q], ps2[q], hs2[q]);
+                    layer_params(WMM[q], source_distance(B, X[q], Y[q], Z[q]), L.r80, s_dep,
+                                 s_sig, s_idd, B.lut_len, ca, cb, cc, pf[q], hf[q], ps2[q],
+                                 hs2[q]);
                     hmax = fmaxf(hmax, hs2[q]);
-                } else {
-                    pf[q] = hf[q] = ps2[q] = hs2[q] = 0.0f;
                 }
             }
             const float nhs = -block_max_slot8(hmax, s_red);
+            float2 X2[NP], Y2[NP], GX2[NP], GY2[NP], PS2[NP], HS2[NP], AP[NP], AH[NP];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                X2[p] = make_float2(X[2 * p], X[2 * p + 1]);
+                Y2[p] = make_float2(Y[2 * p], Y[2 * p + 1]);
+                GX2[p] = make_float2(GX[2 * p], GX[2 * p + 1]);
+                GY2[p] = make_float2(GY[2 * p], GY[2 * p + 1]);
+                PS2[p] = make_float2(ps2[2 * p], ps2[2 * p + 1]);
+                HS2[p] = make_float2(hs2[2 * p], hs2[2 * p + 1]);
+                AP[p] = AH[p] = make_float2(0.0f, 0.0f);
+            }
 
-            float accp[kVpt], acch[kVpt];
-#pragma unroll
-            for (int q = 0; q < kVpt; ++q) accp[q] = acch[q] = 0.0f;
             const int s0 = B.spot_start + L.spot_start;
-            for (int base = 0; base < L.n_spots; base += kThreads) {
-                const int si = base + threadIdx.x;
-                bool keep = false;
-                float4 ga = make_float4(0.f, 0.f, 0.f, 0.f), gb = ga;
-                if (si < L.n_spots) {
-                    ga = __ldg(geo + 2 * (int64_t)(s0 + si));
-                    gb = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                    keep = cull_keep(ga.x, ga.y, gb.y, tb, nhs);
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (lane == 0) s_wcount[warp] = __popc(m);
-                __syncthreads();
-                int off = 0, total = 0;
+            for (int base = 0; base < L.n_spots; base += kThreads * kCull) {
+                bool keep[kCull];
+                float4 ga[kCull], gb[kCull];
+                unsigned m[kCull];
 #pragma unroll
-                for (int w = 0; w < kWarps; ++w) {
-                    const int c = s_wcount[w];
-                    off += (w < warp) ? c : 0;
-                    total += c;
+                for (int c = 0; c < kCull; ++c) {
+                    const int si = base + c * kThreads + threadIdx.x;
+                    keep[c] = false;
+                    if (si < L.n_spots) {
+                        ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
+                        gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
+                        keep[c] = cull_keep(ga[c].x, ga[c].y, gb[c].y, tb, nhs);
+                    }
+                    m[c] = __ballot_sync(0xffffffffu, keep[c]);
+                    if (lane == 0) s_wcount[c][warp] = __popc(m[c]);
                 }
-                if (keep) {
-                    const int pos = off + __popc(m & ((1u << lane) - 1u));
-                    SpotRec r;
-                    r.a = make_float4(-ga.x, -ga.y, ga.z, -ga.w);
-                    r.b = make_float4(-gb.x, gb.y, __ldg(mu + s0 + si), 0.0f);
-                    s_spot[pos] = r;
+                __syncthreads();
+                int total = 0;
+#pragma unroll
+                for (int c = 0; c < kCull; ++c) {
+                    int pos = 0;
+                    for (int w = 0; w < kWarps; ++w) {
+                        if (w == warp) pos = total + __popc(m[c] & ((1u << lane) - 1u));
+                        total += s_wcount[c][w];
+                    }
+                    if (keep[c]) {
+                        const float w = __ldg(mu + s0 + base + c * kThreads + threadIdx.x);
+                        SpotRec r;
+                        r.a = make_float4(-ga[c].x, -ga[c].x, -ga[c].y, -ga[c].y);
+                        r.b = make_float4(ga[c].z, ga[c].z, -ga[c].w, -ga[c].w);
+                        r.c = make_float4(-gb[c].x, -gb[c].x, gb[c].y, gb[c].y);
+                        r.d = make_float4(w, w, 0.0f, 0.0f);
+                        s_spot[pos] = r;
+                    }
                 }
                 __syncthreads();
                 for (int c = 0; c < total; ++c) {
                     const SpotRec r = s_spot[c];
+                    const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
+                                 ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
 #pragma unroll
-                    for (int q = 0; q < kVpt; ++q) {
-                        const float ax = fmaf(r.a.x, vg.GX[q], vg.X[q]);
-                        const float ay = fmaf(r.a.y, vg.GY[q], vg.Y[q]);
-                        const float cz = fmaf(r.a.z, vg.Y[q], fmaf(r.a.w, vg.X[q], r.b.x));
-                        const float S = fmaf(ax, ax, fmaf(ay, ay, cz * cz));
-                        const float qq = S * r.b.y;
-                        accp[q] = fmaf(r.b.z, ex2(ps2[q] * qq), accp[q]);
-                        acch[q] = fmaf(r.b.z, ex2(hs2[q] * qq), acch[q]);
+                    for (int p = 0; p < NP; ++p) {
+                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, X2[p], Y2[p],
+                                                  GX2[p], GY2[p]);
+                        AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS2[p], qq)), AP[p]);
+                        AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS2[p], qq)), AH[p]);
                     }
                 }
                 __syncthreads();
@@ -350,7 +398,9 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
                 if (act[q]) {
-                    const float ld = fmaf(pf[q], accp[q], hf[q] * acch[q]);
+                    const float ap = (q & 1) ? AP[q >> 1].y : AP[q >> 1].x;
+                    const float ah = (q & 1) ? AH[q >> 1].y : AH[q >> 1].x;
+                    const float ld = fmaf(pf[q], ap, hf[q] * ah);
                     neumaier(bs_s[q], bs_c[q], ld);
                     neumaier(tot_s[q], tot_c[q], ld);
                 }
@@ -370,126 +420,173 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 
 // ------------------------------------------------------------------ adjoint
 
-__global__ void __launch_bounds__(kThreads, 2)
+constexpr int kAdjVpt = 4;  // adjoint: voxels per thread (same tile shape)
+
+__global__ void __launch_bounds__(kThreads, 4)
 k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
           const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
           const float *__restrict__ wfield, float *__restrict__ grad)
 {
     __shared__ float s_dep[PB_MAX_LUT_LEN], s_sig[PB_MAX_LUT_LEN], s_idd[PB_MAX_LUT_LEN];
-    __shared__ VoxRec s_vox[kThreads * kVpt];
-    __shared__ SpotRec s_spot[kThreads];
+    __shared__ VoxRec s_vox[kThreads * kAdjVpt];
+    __shared__ int s_cand[kThreads * kSpt];
+    __shared__ float s_gsum[kThreads * kSpt];
     __shared__ float s_red[kWarps][9];
-    __shared__ int s_wcount[kWarps * kVpt];
-    __shared__ int s_scount[kWarps];
+    __shared__ int s_wcount[kAdjVpt > kSpt ? kAdjVpt : kSpt][kWarps];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int vi[kVpt], vj[kVpt], vk[kVpt];
-    bool valid[kVpt];
-    int64_t vidx[kVpt];
-    tile_voxels(A, vi, vj, vk, valid, vidx);
+    int vi[kAdjVpt], vj[kAdjVpt], vk[kAdjVpt];
+    bool valid[kAdjVpt];
+    int64_t vidx[kAdjVpt];
+    tile_voxels<kAdjVpt>(A, vi, vj, vk, valid, vidx);
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
-    float wv[kVpt];
+    float wv[kAdjVpt];
     bool anyw = false;
 #pragma unroll
-    for (int q = 0; q < kVpt; ++q) {
+    for (int q = 0; q < kAdjVpt; ++q) {
         wv[q] = valid[q] ? __ldg(wfield + vidx[q]) * A.scale : 0.0f;
         anyw |= (wv[q] != 0.0f);
     }
     if (!__syncthreads_or(anyw)) return;
+    for (int c = threadIdx.x; c < kThreads * kSpt; c += kThreads) s_gsum[c] = 0.0f;
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
-        VoxelGeom vg;
-        beam_voxel_geom(A.g, B, wet + b * V, vi, vj, vk, valid, vidx, vg);
-        const TileBounds tb = tile_bounds(vg.X, vg.Y, vg.GX, vg.GY, valid, s_red);
+        float X[kAdjVpt], Y[kAdjVpt], Z[kAdjVpt], GX[kAdjVpt], GY[kAdjVpt], WMM[kAdjVpt];
+#pragma unroll
+        for (int q = 0; q < kAdjVpt; ++q) {
+            if (valid[q]) {
+                voxel_head(A.g, B, vi[q], vj[q], vk[q], X[q], Y[q], Z[q], GX[q], GY[q]);
+                WMM[q] = __fmul_rn(__ldg(wet + b * V + vidx[q]), 10.0f);
+            } else {
+                X[q] = Y[q] = Z[q] = 0.0f;
+                GX[q] = GY[q] = 1.0f;
+                WMM[q] = INFINITY;
+            }
+        }
+        const TileBounds tb = tile_bounds<kAdjVpt>(X, Y, GX, GY, valid, s_red);
 
         for (int l = 0; l < B.n_layers; ++l) {
             const PbLayer L = layers[B.layer_start + l];
             const float cut = __fmul_rn(1.1f, L.r80);
-            bool act[kVpt];
+            bool act[kAdjVpt];
             bool any = false;
 #pragma unroll
-            for (int q = 0; q < kVpt; ++q) {
-                act[q] = valid[q] && wv[q] != 0.0f && !(vg.WMM[q] > cut);
+            for (int q = 0; q < kAdjVpt; ++q) {
+                act[q] = valid[q] && wv[q] != 0.0f && !(WMM[q] > cut);
                 any |= act[q];
             }
             if (!__syncthreads_or(any)) continue;
+            // Compaction slots of the active voxels (order q, warp, lane).
+            unsigned mq[kAdjVpt];
+#pragma unroll
+            for (int q = 0; q < kAdjVpt; ++q) {
+                mq[q] = __ballot_sync(0xffffffffu, act[q]);
+                if (lane == 0) s_wcount[q][warp] = __popc(mq[q]);
+            }
             stage_lut(B, L.energy_id, s_dep, s_sig, s_idd);
             __syncthreads();
+            int nact = 0, pos[kAdjVpt];
+#pragma unroll
+            for (int q = 0; q < kAdjVpt; ++q) {
+                pos[q] = 0;
+                for (int w = 0; w < kWarps; ++w) {
+                    if (w == warp) pos[q] = nact + __popc(mq[q] & ((1u << lane) - 1u));
+                    nact += s_wcount[q][w];
+                }
+            }
             const float *cabc = B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2;
             const float ca = __ldg(cabc), cb = __ldg(cabc + 1), cc = __ldg(cabc + 2);
             float hmax = -INFINITY;
-            unsigned mq[kVpt];
-            VoxRec rec[kVpt];
 #pragma unroll
-            for (int q = 0; q < kVpt; ++q) {
+            for (int q = 0; q < kAdjVpt; ++q) {
                 if (act[q]) {
                     float pf, hf, ps2, hs2;
-                    layer_params(vg.WMM[q], vg.DIST[q], L.r80, s_dep, s_sig, s_idd,
-                                 B.lut_len, ca, cb, cc, pf, hf, ps2, hs2);
+                    layer_params(WMM[q], source_distance(B, X[q], Y[q], Z[q]), L.r80, s_dep,
+                                 s_sig, s_idd, B.lut_len, ca, cb, cc, pf, hf, ps2, hs2);
                     hmax = fmaxf(hmax, hs2);
-                    rec[q].a = make_float4(vg.X[q], vg.Y[q], vg.GX[q], vg.GY[q]);
-                    rec[q].b = make_float4(ps2, hs2, wv[q] * pf, wv[q] * hf);
+                    VoxRec r;
+                    r.xy = make_float4(X[q], X[q], Y[q], Y[q]);
+                    r.g = make_float4(GX[q], GX[q], GY[q], GY[q]);
+                    r.s = make_float4(ps2, ps2, hs2, hs2);
+                    const float a = wv[q] * pf, h = wv[q] * hf;
+                    r.f = make_float4(a, a, h, h);
+                    s_vox[pos[q]] = r;
                 }
-                mq[q] = __ballot_sync(0xffffffffu, act[q]);
-                if (lane == 0) s_wcount[q * kWarps + warp] = __popc(mq[q]);
             }
-            const float nhs = -block_max_slot8(hmax, s_red);  // includes a barrier
-            // Compact the active voxels' records: order q, warp, lane.
-            int nact = 0;
-#pragma unroll
-            for (int q = 0; q < kVpt; ++q) {
-                int pos = 0;
-                for (int w = 0; w < kWarps; ++w) {
-                    const int c = s_wcount[q * kWarps + w];
-                    if (w == warp) pos = nact + __popc(mq[q] & ((1u << lane) - 1u));
-                    nact += c;
-                }
-                if (act[q]) s_vox[pos] = rec[q];
-            }
+            // includes the barrier that publishes s_vox and frees s_wcount
+            const float nhs = -block_max_slot8(hmax, s_red);
 
             const int s0 = B.spot_start + L.spot_start;
-            for (int base = 0; base < L.n_spots; base += kThreads) {
-                const int si = base + threadIdx.x;
-                bool keep = false;
-                float4 ga = make_float4(0.f, 0.f, 0.f, 0.f), gb = ga;
-                if (si < L.n_spots) {
-                    ga = __ldg(geo + 2 * (int64_t)(s0 + si));
-                    gb = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                    keep = cull_keep(ga.x, ga.y, gb.y, tb, nhs);
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (lane == 0) s_scount[warp] = __popc(m);
-                __syncthreads();
-                int off = 0, total = 0;
+            for (int base = 0; base < L.n_spots; base += kThreads * kSpt) {
+                bool keep[kSpt];
+                unsigned m[kSpt];
 #pragma unroll
-                for (int w = 0; w < kWarps; ++w) {
-                    const int c = s_scount[w];
-                    off += (w < warp) ? c : 0;
-                    total += c;
-                }
-                if (keep) {
-                    const int p = off + __popc(m & ((1u << lane) - 1u));
-                    SpotRec r;
-                    r.a = make_float4(-ga.x, -ga.y, ga.z, -ga.w);
-                    r.b = make_float4(-gb.x, gb.y, __int_as_float(s0 + si), 0.0f);
-                    s_spot[p] = r;
+                for (int c = 0; c < kSpt; ++c) {
+                    const int si = base + c * kThreads + threadIdx.x;
+                    keep[c] = false;
+                    if (si < L.n_spots) {
+                        const float4 ga = __ldg(geo + 2 * (int64_t)(s0 + si));
+                        const float4 gb = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
+                        keep[c] = cull_keep(ga.x, ga.y, gb.y, tb, nhs);
+                    }
+                    m[c] = __ballot_sync(0xffffffffu, keep[c]);
+                    if (lane == 0) s_wcount[c][warp] = __popc(m[c]);
                 }
                 __syncthreads();
-                if ((int)threadIdx.x < total) {
-                    const SpotRec r = s_spot[threadIdx.x];
-                    float acc = 0.0f;
-                    for (int c = 0; c < nact; ++c) {
-                        const VoxRec v = s_vox[c];
-                        const float ax = fmaf(r.a.x, v.a.z, v.a.x);
-                        const float ay = fmaf(r.a.y, v.a.w, v.a.y);
-                        const float cz = fmaf(r.a.z, v.a.y, fmaf(r.a.w, v.a.x, r.b.x));
-                        const float S = fmaf(ax, ax, fmaf(ay, ay, cz * cz));
-                        const float qq = S * r.b.y;
-                        acc = fmaf(v.b.z, ex2(v.b.x * qq), acc);
-                        acc = fmaf(v.b.w, ex2(v.b.y * qq), acc);
+                int total = 0;
+#pragma unroll
+                for (int c = 0; c < kSpt; ++c) {
+                    int pos = 0;
+                    for (int w = 0; w < kWarps; ++w) {
+                        if (w == warp) pos = total + __popc(m[c] & ((1u << lane) - 1u));
+                        total += s_wcount[c][w];
                     }
-                    if (acc != 0.0f) atomicAdd(grad + __float_as_int(r.b.z), acc);
+                    if (keep[c]) s_cand[pos] = s0 + base + c * kThreads + threadIdx.x;
+                }
+                __syncthreads();
+                // Work items (spot pair, voxel stripe): every thread busy even
+                // when few spots survive the culling.  Partial sums meet in
+                // shared memory, then one atomic per spot goes to global.
+                const int npair = (total + 1) >> 1;
+                const int stripes = npair >= kThreads ? 1 : kThreads / npair;
+                const int items = npair * stripes;
+                for (int it = threadIdx.x; it < items; it += kThreads) {
+                    const int sp = it % npair, vs = it / npair;
+                    float2 nx, ny, tx, nty, ncs, it2;
+                    float4 ga[2], gb[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = 2 * sp + h;
+                        ga[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        gb[h] = make_float4(0.f, 1.f, 0.f, 0.f);
+                        if (c < total) {
+                            ga[h] = __ldg(geo + 2 * (int64_t)s_cand[c]);
+                            gb[h] = __ldg(geo + 2 * (int64_t)s_cand[c] + 1);
+                        }
+                    }
+                    nx = make_float2(-ga[0].x, -ga[1].x);
+                    ny = make_float2(-ga[0].y, -ga[1].y);
+                    tx = make_float2(ga[0].z, ga[1].z);
+                    nty = make_float2(-ga[0].w, -ga[1].w);
+                    ncs = make_float2(-gb[0].x, -gb[1].x);
+                    it2 = make_float2(gb[0].y, gb[1].y);
+                    float2 acc = make_float2(0.0f, 0.0f);
+                    for (int c = vs; c < nact; c += stripes) {
+                        const VoxRec v = s_vox[c];
+                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
+                                                  hi2(v.xy), lo2(v.g), hi2(v.g));
+                        acc = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qq)), acc);
+                        acc = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qq)), acc);
+                    }
+                    if (acc.x != 0.0f) atomicAdd(&s_gsum[2 * sp], acc.x);
+                    if (acc.y != 0.0f && 2 * sp + 1 < total) atomicAdd(&s_gsum[2 * sp + 1], acc.y);
+                }
+                __syncthreads();
+                for (int c = threadIdx.x; c < total; c += kThreads) {
+                    const float a = s_gsum[c];
+                    if (a != 0.0f) atomicAdd(grad + s_cand[c], a);
+                    s_gsum[c] = 0.0f;
                 }
                 __syncthreads();
             }
@@ -510,10 +607,10 @@ k_objective(const float *__restrict__ dose, const float *__restrict__ presc,
     double acc = 0.0;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
          q += (int64_t)gridDim.x * blockDim.x) {
-        const float d = dose[q] - presc[q];
-        const float w = weight[q];
-        acc += (double)w * (double)d * (double)d;
-        if (resid) resid[q] = 2.0f * w * d;
+        const double d = (double)dose[q] - (double)presc[q];
+        const double w = (double)weight[q];
+        acc += w * d * d;
+        if (resid) resid[q] = (float)(2.0 * w * d);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);

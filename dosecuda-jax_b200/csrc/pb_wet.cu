@@ -134,6 +134,57 @@ __device__ __forceinline__ float trilinear(const float *__restrict__ rho,
 // reference's own.  TEX = false interpolates with exact FP32 trilinear
 // weights from global memory and forms the direction in FP64, the CPU
 // oracle's arithmetic.
+// Number of leading samples t = 0, 1, ... whose texture coordinates are
+// certainly inside [0, n) on every axis, so the in-grid test can be skipped
+// for them.  The bound is taken on the exact (real-number) coordinates
+// A + B t of the FP32 formula with a margin of 4e-3 texel; the FP32
+// evaluation differs from them by less than 1e-3 texel for any grid this
+// library accepts, so the skipped tests would all have passed.
+__device__ __forceinline__ int safe_steps(const PbGrid &g, const PbBeamGeom &B, float inv_s,
+                                          float px, float py, float pz, float ux, float uy,
+                                          float uz, int cap)
+{
+    const double margin = 4e-3;
+    const float pv[3] = {px, py, pz}, uv[3] = {ux, uy, uz};
+    const int nv[3] = {g.nx, g.ny, g.nz};
+    double T = (double)cap;
+    for (int a = 0; a < 3; ++a) {
+        const double A = (double)inv_s * ((double)pv[a] + (double)B.iso[a]) + 0.5;
+        const double Bt = (double)inv_s * (double)uv[a];
+        const double lo = margin, hi = (double)nv[a] - margin;
+        if (A < lo || A > hi) return 0;
+        if (Bt > 0.0) T = fmin(T, (hi - A) / Bt);
+        else if (Bt < 0.0) T = fmin(T, (lo - A) / Bt);
+    }
+    if (!(T >= 0.0)) return 0;
+    const double n = floor(T) + 1.0;
+    return n < (double)cap ? (int)n : cap;
+}
+
+template <bool TEX>
+__device__ __forceinline__ float ray_sample(const float *__restrict__ rho,
+                                            cudaTextureObject_t tex, const PbGrid &g,
+                                            float x, float y, float z)
+{
+    if (TEX) return tex3D<float>(tex, x, y, z);
+    return trilinear(rho, g.nx, g.ny, g.nz, __fsub_rn(x, 0.5f), __fsub_rn(y, 0.5f),
+                     __fsub_rn(z, 0.5f));
+}
+
+// Raw WET (cm) per voxel: samples every 1 mm from the voxel toward the
+// source while the texture coordinate stays inside [0, n); WET = -0.05 +
+// 0.1 * sum(max(RLSP, 0)).  The sum is carried in FP64 (FP32 partials of 8
+// samples).  A ray that exceeds the grid-diagonal step cap stops and raises
+// PB_ERR_RAY_CAP in *status.  The leading samples that are certainly inside
+// the grid (safe_steps) are taken 8 at a time without the in-grid test, so
+// that several texture fetches are in flight per thread.
+//
+// TEX = true samples RLSP through a border-0, linearly filtered 3-D texture
+// and forms the ray direction with rnorm3df, as the reference does
+// (CudaClasses.cuh:41-52, TextureClasses.cu:14-41), so the samples are the
+// reference's own.  TEX = false interpolates with exact FP32 trilinear
+// weights from global memory and forms the direction in FP64, the CPU
+// oracle's arithmetic.
 template <bool TEX>
 __global__ void __launch_bounds__(128)
 k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
@@ -161,36 +212,39 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
     }
     const float inv_s = __fdiv_rn(1.0f, g.spacing);
     const float fnx = (float)g.nx, fny = (float)g.ny, fnz = (float)g.nz;
+    const float ix = B.iso[0], iy = B.iso[1], iz = B.iso[2];
+    const int nsafe = safe_steps(g, B, inv_s, px, py, pz, ux, uy, uz, cap);
     double acc = 0.0;
+    int n = 0;
+    for (; n + 8 <= nsafe; n += 8) {
+        float r[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const float t = (float)(n + m);
+            const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
+            const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
+            const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
+            r[m] = ray_sample<TEX>(rho, tex, g, x, y, z);
+        }
+        float part = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) part += fmaxf(r[m], 0.0f);
+        acc += (double)part;
+    }
     float part = 0.0f;
-    int inpart = 0;
-    float t = 0.0f;
-    for (int n = 0;; ++n) {
-        const float qx = __fmaf_rn(ux, t, px);
-        const float qy = __fmaf_rn(uy, t, py);
-        const float qz = __fmaf_rn(uz, t, pz);
-        const float x = __fmaf_rn(inv_s, __fadd_rn(qx, B.iso[0]), 0.5f);
-        const float y = __fmaf_rn(inv_s, __fadd_rn(qy, B.iso[1]), 0.5f);
-        const float z = __fmaf_rn(inv_s, __fadd_rn(qz, B.iso[2]), 0.5f);
-        if (!(x >= 0.0f && x < fnx && y >= 0.0f && y < fny && z >= 0.0f && z < fnz))
+    for (;; ++n) {
+        const float t = (float)n;
+        const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
+        const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
+        const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
+        if (n >= nsafe &&
+            !(x >= 0.0f && x < fnx && y >= 0.0f && y < fny && z >= 0.0f && z < fnz))
             break;
         if (n >= cap) {
             if (status) atomicOr(status, (int)PB_ERR_RAY_CAP);
             break;
         }
-        float r;
-        if (TEX)
-            r = tex3D<float>(tex, x, y, z);
-        else
-            r = trilinear(rho, g.nx, g.ny, g.nz, __fsub_rn(x, 0.5f), __fsub_rn(y, 0.5f),
-                          __fsub_rn(z, 0.5f));
-        part += fmaxf(r, 0.0f);
-        if (++inpart == 16) {
-            acc += (double)part;
-            part = 0.0f;
-            inpart = 0;
-        }
-        t = __fadd_rn(t, 1.0f);
+        part += fmaxf(ray_sample<TEX>(rho, tex, g, x, y, z), 0.0f);
     }
     acc += (double)part;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
@@ -198,13 +252,99 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
     raw[b * V + v] = __double2float_rn(fma(0.1, acc, -0.05));
 }
 
+// Linear map of the smoothing samples in index space, per beam: head ->
+// image rotation (rot, row-major, FP64 from the FP32 sines and cosines the
+// kernels use) and, per direction, the index step of 1 mm (dm).
+struct SmoothSteps {
+    double rot[PB_MAX_BEAMS][9];
+    float dm[PB_MAX_BEAMS][6][3];
+    double inv_s;
+    float tie;   // half-width of the band around half-integers sent to the exact path
+};
+
+static void smooth_steps(const PbGrid &g, const PbBeamGeom *beams, int n_beams,
+                         const SmoothDirs &d, SmoothSteps &o)
+{
+    o.inv_s = 1.0 / (double)g.spacing;
+    // Bound on |FP32 reference-order index - real index|: about 8 roundings
+    // of a coordinate no larger than `ext` mm, divided by the spacing, plus
+    // the fast path's own rounding; the band is twice that, at least 2e-3.
+    double ext = g.spacing * (double)(g.nx > g.ny ? (g.nx > g.nz ? g.nx : g.nz)
+                                                  : (g.ny > g.nz ? g.ny : g.nz));
+    for (int b = 0; b < n_beams; ++b)
+        for (int a = 0; a < 3; ++a) ext = fmax(ext, fabs((double)beams[b].iso[a]) + ext);
+    const double err = 8.0 * ldexp(ext + 16.0, -24) * o.inv_s + 2e-4;
+    o.tie = (float)fmax(2e-3, 2.0 * err);
+    for (int b = 0; b < n_beams; ++b) {
+        const PbBeamGeom &B = beams[b];
+        const double sg = B.singa, cg = B.cosga, st = B.sinta, ct = B.costa;
+        // head (hx, hy, hz) -> (xz, yz, zz) = (-hx, hz, hy); gantry; couch
+        // x = (xz cg - yz sg) ct + zz st ; y = xz sg + yz cg ;
+        // z = -(xz cg - yz sg) st + zz ct
+        double *M = o.rot[b];
+        M[0] = -cg * ct; M[1] = st;  M[2] = -sg * ct;
+        M[3] = -sg;      M[4] = 0.0; M[5] = cg;
+        M[6] = cg * st;  M[7] = ct;  M[8] = sg * st;
+        for (int dd = 0; dd < 6; ++dd) {
+            const double c = d.c[dd], s = d.s[dd];
+            for (int a = 0; a < 3; ++a)
+                o.dm[b][dd][a] = (float)((M[3 * a] * c + M[3 * a + 1] * s) * o.inv_s);
+        }
+    }
+}
+
+// roundf(q / s) as an int (CudaClasses.cuh:112-116).  q * (1/s) differs
+// from the correctly rounded quotient by a few ulp, which can change the
+// rounding only next to a half-integer; there the exact division is taken.
+__device__ __forceinline__ int nearest_index(float q, float s, float inv_s)
+{
+    float m = __fmul_rn(q, inv_s);
+    const float tie = fabsf(fabsf(m - floorf(m)) - 0.5f);
+    if (tie < fmaf(fabsf(m), 1e-6f, 1e-6f)) m = __fdiv_rn(q, s);
+    return (int)roundf(m);
+}
+
 // Smoothed WET: mean of the voxel's raw WET and the in-grid nearest-voxel
 // samples at 1..9 mm along six BEV-lateral directions, taking radius dr
 // while dr < 10*WET(cm) (IMPTClasses.cu:166-198).
+//
+// The sample's voxel index along an axis is roundf of
+//   m(dr) = (head_to_image(h + dr*(c, s, 0)) + iso) / spacing,
+// evaluated in the reference's FP32 operation order (exact_sample below).
+// That value is close to the real-number m(dr) = m0 + dr*dm (the map is
+// linear): within about 8 roundings of the largest coordinate, divided by
+// the spacing (SmoothSteps::tie holds twice that bound, at least 2e-3).  The
+// kernel evaluates m0 + dr*dm with one FMA per axis and rounds it with an
+// FADD round-to-nearest, and only where some axis lies within `tie` of a
+// half-integer -- where the two could round differently -- does it take the
+// reference-order path.  The chosen voxels are the same.
+__device__ __forceinline__ void exact_sample(const PbBeamGeom &B, float s, float inv_s,
+                                             float hx, float hy, float hz, float dr, float c,
+                                             float sn, int &ii, int &jj, int &kk)
+{
+    float qx, qy, qz;
+    head_to_image(B, __fadd_rn(hx, __fmul_rn(dr, c)), __fadd_rn(hy, __fmul_rn(dr, sn)), hz,
+                  qx, qy, qz);
+    ii = nearest_index(__fadd_rn(qx, B.iso[0]), s, inv_s);
+    jj = nearest_index(__fadd_rn(qy, B.iso[1]), s, inv_s);
+    kk = nearest_index(__fadd_rn(qz, B.iso[2]), s, inv_s);
+}
+
+// Round to nearest (ties to even) for |m| < 2^22 with FP32 adds; reports
+// whether m lies within `tie` of a half-integer.
+__device__ __forceinline__ int round_fadd(float m, float tie, bool &near)
+{
+    const float magic = 12582912.0f;  // 1.5 * 2^23
+    const float t = __fadd_rn(m, magic);
+    const float r = __fsub_rn(t, magic);
+    near |= fabsf(__fsub_rn(m, r)) > 0.5f - tie;
+    return __float_as_int(t) - 0x4B400000;
+}
+
 __global__ void __launch_bounds__(128)
 k_smooth(const float *__restrict__ raw, PbGrid g,
-         const __grid_constant__ BeamGeomSet bs, SmoothDirs d, int zbricks,
-         float *__restrict__ wet)
+         const __grid_constant__ BeamGeomSet bs, SmoothDirs d,
+         const __grid_constant__ SmoothSteps st, int zbricks, float *__restrict__ wet)
 {
     const int b = blockIdx.z / zbricks;
     const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
@@ -223,15 +363,29 @@ k_smooth(const float *__restrict__ raw, PbGrid g,
     image_to_head(B, px, py, pz, hx, hy, hz);
     const float lim = __fmul_rn(center, 10.0f);
     const float s = g.spacing;
+    const float inv_s = __fdiv_rn(1.0f, s);
+    if (!(1.0f < lim)) {
+        wet[b * V + v] = center;
+        return;
+    }
+    // m0: real-number index coordinates of the voxel itself
+    const double *M = st.rot[b];
+    const double dhx = hx, dhy = hy, dhz = hz;
+    const float m0x = (float)((M[0] * dhx + M[1] * dhy + M[2] * dhz + (double)B.iso[0]) *
+                              st.inv_s);
+    const float m0y = (float)((M[3] * dhx + M[4] * dhy + M[5] * dhz + (double)B.iso[1]) *
+                              st.inv_s);
+    const float m0z = (float)((M[6] * dhx + M[7] * dhy + M[8] * dhz + (double)B.iso[2]) *
+                              st.inv_s);
+    const float tie = st.tie;
     for (int dd = 0; dd < 6; ++dd) {
-        const float c = d.c[dd], sn = d.s[dd];
+        const float dmx = st.dm[b][dd][0], dmy = st.dm[b][dd][1], dmz = st.dm[b][dd][2];
         for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f)) {
-            float qx, qy, qz;
-            head_to_image(B, __fadd_rn(hx, __fmul_rn(dr, c)),
-                          __fadd_rn(hy, __fmul_rn(dr, sn)), hz, qx, qy, qz);
-            const int ii = (int)roundf(__fdiv_rn(__fadd_rn(qx, B.iso[0]), s));
-            const int jj = (int)roundf(__fdiv_rn(__fadd_rn(qy, B.iso[1]), s));
-            const int kk = (int)roundf(__fdiv_rn(__fadd_rn(qz, B.iso[2]), s));
+            bool near = false;
+            int ii = round_fadd(fmaf(dr, dmx, m0x), tie, near);
+            int jj = round_fadd(fmaf(dr, dmy, m0y), tie, near);
+            int kk = round_fadd(fmaf(dr, dmz, m0z), tie, near);
+            if (near) exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], ii, jj, kk);
             if (ii >= 0 && ii < g.nx && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz) {
                 sum += __ldg(R + ii + (int64_t)g.nx * (jj + (int64_t)g.ny * kk));
                 n += 1;
@@ -256,6 +410,8 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
     for (int b = 0; b < n_beams; ++b) bs.b[b] = beams[b];
     SmoothDirs d;
     smooth_dirs(d.c, d.s);
+    SmoothSteps ss;
+    smooth_steps(g, beams, n_beams, d, ss);
     const int zb = (g.nz + 3) / 4;
     dim3 block(8, 4, 4);
     dim3 grid((g.nx + 7) / 8, (g.ny + 3) / 4, zb * n_beams);
@@ -267,7 +423,7 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
                                                   status);
     PbStatus s = check_launch("k_raytrace");
     if (s != PB_OK) return s;
-    k_smooth<<<grid, block, 0, st>>>(raw, g, bs, d, zb, wet);
+    k_smooth<<<grid, block, 0, st>>>(raw, g, bs, d, ss, zb, wet);
     return check_launch("k_smooth");
 }
 

@@ -22,7 +22,7 @@ PB_ERR_RAY_CAP = 4
 PB_ERR_UNSUPPORTED = 5
 
 PB_MAX_BEAMS = 16
-PB_MAX_LUT_LEN = 1024
+PB_MAX_LUT_LEN = 512
 PB_MAX_CURVE = 64
 PB_SPOT_GEO_FLOATS = 8
 

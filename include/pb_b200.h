@@ -45,7 +45,7 @@ typedef enum {
 } PbStatus;
 
 #define PB_MAX_BEAMS 16      /* beams per plan in one launch               */
-#define PB_MAX_LUT_LEN 1024  /* LUT rows per energy (reference: 400)       */
+#define PB_MAX_LUT_LEN 512   /* LUT rows per energy (reference: 400)       */
 #define PB_MAX_CURVE 64      /* points of an HU -> RLSP curve              */
 
 /* Voxel grid: isotropic spacing only (dosemodule.cu:146, plan_impt.py:177). */
