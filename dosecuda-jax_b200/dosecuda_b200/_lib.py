@@ -25,6 +25,7 @@ PB_MAX_BEAMS = 16
 PB_MAX_LUT_LEN = 512
 PB_MAX_CURVE = 64
 PB_SPOT_GEO_FLOATS = 8
+PB_NOALLOC_MAX_WET_FLOATS = 8 * 1024 * 1024
 
 
 class PbError(RuntimeError):
@@ -90,6 +91,7 @@ _SIGS = {
     "pb_texture_update": (_I, [ctypes.c_uint64, _VP, _VP]),
     "pb_texture_destroy": (_I, [ctypes.c_uint64]),
     "pb_wet": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),
+    "pb_wet_noalloc": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP]),
     "pb_dose": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP, _VP, _VP]),
     "pb_dose_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP,
                              _VP]),

@@ -157,6 +157,23 @@ PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
                 const PbBeamGeom *beams, int n_beams, float *raw_work_dev,
                 float *wet_dev, int *status_dev, void *stream);
 
+/* pb_wet for callers that cannot allocate device memory (code inside a
+ * framework that owns the device pool, such as an XLA/JAX custom call, or a
+ * plug-in handed only its input and output buffers).  No counterpart in the
+ * reference.  Same arguments and result as pb_wet, without raw_work_dev:
+ * the unsmoothed WET goes to a fixed work array inside this library of
+ * PB_NOALLOC_MAX_WET_FLOATS floats (32 MiB per GPU, held until exit);
+ * n_beams x V above that is rejected with PB_ERR_INVALID.  The call
+ * allocates nothing (tex, if non-zero, comes from pb_texture_create made
+ * earlier; tex = 0 needs nothing else).  Its first call on a device looks
+ * up the array's device address; make it before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+#define PB_NOALLOC_MAX_WET_FLOATS (8u * 1024u * 1024u)
+PbStatus pb_wet_noalloc(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
+                        const PbBeamGeom *beams, int n_beams, float *wet_dev,
+                        int *status_dev, void *stream);
+
 /* Forward pencil-beam dose of a plan (IMPTClasses.cu:204-271) for all of
  * its beams in one launch.  wet_dev: n_beams x V (cm).  layers_dev: all
  * layers, beam-major.  spot_geo_dev: PB_SPOT_GEO_FLOATS per spot, mu_dev:
