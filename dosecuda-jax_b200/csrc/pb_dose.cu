@@ -36,11 +36,12 @@
 
 namespace pb {
 
-constexpr int kThreads = 128;
-constexpr int kWarps = kThreads / 32;
+constexpr int kThreads = 128;       // forward block
 constexpr int kVpt = 4;             // forward: voxels per thread (z, z+2, z+4, z+6)
 constexpr int kCull = 2;            // forward: spots culled per thread per chunk
-constexpr int kSpt = 4;             // adjoint: spots per thread per chunk
+constexpr int kAdjThreads = 256;    // adjoint block
+constexpr int kAdjVpt = 2;          // adjoint: voxels per thread (z, z+4)
+constexpr int kSpt = 2;             // adjoint: spots culled per thread per chunk
 constexpr float kCullLog2 = 24.0f;  // skip factors below 2^-24
 
 struct PlanArgs {
@@ -159,11 +160,12 @@ __device__ __forceinline__ void neumaier(float &s, float &c, float x)
 }
 
 // Block-wide min/max of the tile's BEV box over valid voxels.
-template <int NV>
+template <int NV, int NT>
 __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y,
                                                   const float *GX, const float *GY,
                                                   const bool *valid, float (*s_red)[9])
 {
+    constexpr int kWarps = NT / 32;
     float v[8] = {INFINITY, -INFINITY, INFINITY, -INFINITY,
                   INFINITY, -INFINITY, INFINITY, -INFINITY};
 #pragma unroll
@@ -196,8 +198,10 @@ __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y
     return tb;
 }
 
+template <int NT>
 __device__ __forceinline__ float block_max_slot8(float v, float (*s_red)[9])
 {
+    constexpr int kWarps = NT / 32;
     v = warp_max(v);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) s_red[warp][8] = v;
@@ -207,10 +211,11 @@ __device__ __forceinline__ float block_max_slot8(float v, float (*s_red)[9])
     return r;
 }
 
-// Voxels of this block's tile owned by this thread: (li, lj, lk + step*q).
+// Voxels of this block's tile owned by this thread: (li, lj, lk + step*q),
+// with 64 * 8/NV threads per 8x8x8 tile.
 template <int NV>
 __device__ __forceinline__ void tile_voxels(const PlanArgs &A, int *vi, int *vj, int *vk,
-                                            bool *valid, int64_t *vidx)
+                                            bool *valid, int *vidx)
 {
     int t = blockIdx.x;
     const int tx = t % A.tiles_x;
@@ -225,7 +230,7 @@ __device__ __forceinline__ void tile_voxels(const PlanArgs &A, int *vi, int *vj,
         vj[q] = ty * 8 + lj;
         vk[q] = tz * 8 + lk + step * q;
         valid[q] = vi[q] < A.g.nx && vj[q] < A.g.ny && vk[q] < A.g.nz;
-        vidx[q] = valid[q] ? vi[q] + (int64_t)A.g.nx * (vj[q] + (int64_t)A.g.ny * vk[q]) : 0;
+        vidx[q] = valid[q] ? vi[q] + A.g.nx * (vj[q] + A.g.ny * vk[q]) : 0;
     }
 }
 
@@ -249,11 +254,12 @@ __device__ __forceinline__ float source_distance(const PbBeam &B, float X, float
     return sqrtf(fmaf(X, X, fmaf(Y, Y, dz * dz)));
 }
 
+template <int NT>
 __device__ __forceinline__ void stage_lut(const PbBeam &B, int e, float *s_dep,
                                           float *s_sig, float *s_idd)
 {
     const size_t o = (size_t)e * B.lut_len;
-    for (int x = threadIdx.x; x < B.lut_len; x += kThreads) {
+    for (int x = threadIdx.x; x < B.lut_len; x += NT) {
         s_dep[x] = __ldg(B.depths_dev + o + x);
         s_sig[x] = __ldg(B.sigmas_dev + o + x);
         s_idd[x] = __ldg(B.idds_dev + o + x);
@@ -262,23 +268,35 @@ __device__ __forceinline__ void stage_lut(const PbBeam &B, int e, float *s_dep,
 
 // ------------------------------------------------------------------ forward
 
-__global__ void __launch_bounds__(kThreads, 4)
+// BEAM_OUT: also write each beam's dose (beam_dose != nullptr).
+#ifndef PB_DOSE_MIN_BLOCKS
+#define PB_DOSE_MIN_BLOCKS 5
+#endif
+#ifndef PB_ADJ_MIN_BLOCKS
+#define PB_ADJ_MIN_BLOCKS 3
+#endif
+
+template <bool BEAM_OUT>
+__global__ void __launch_bounds__(kThreads, PB_DOSE_MIN_BLOCKS)
 k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
        const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
        const float *__restrict__ mu, float *__restrict__ dose,
        float *__restrict__ beam_dose)
 {
     constexpr int NP = kVpt / 2;  // voxel pairs per thread
+    constexpr int kWarps = kThreads / 32;
     __shared__ float s_dep[PB_MAX_LUT_LEN], s_sig[PB_MAX_LUT_LEN], s_idd[PB_MAX_LUT_LEN];
     __shared__ SpotRec s_spot[kThreads * kCull];
     __shared__ float s_red[kWarps][9];
     __shared__ int s_wcount[kCull][kWarps];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int vi[kVpt], vj[kVpt], vk[kVpt];
+    int vidx[kVpt];
     bool valid[kVpt];
-    int64_t vidx[kVpt];
-    tile_voxels<kVpt>(A, vi, vj, vk, valid, vidx);
+    {
+        int vi[kVpt], vj[kVpt], vk[kVpt];
+        tile_voxels<kVpt>(A, vi, vj, vk, valid, vidx);
+    }
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
 
     float tot_s[kVpt], tot_c[kVpt];
@@ -287,19 +305,34 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
-        float X[kVpt], Y[kVpt], Z[kVpt], GX[kVpt], GY[kVpt], WMM[kVpt];
+        // voxel geometry of this beam, kept only as packed voxel pairs
+        float2 XP[NP], YP[NP], GXP[NP], GYP[NP], WP[NP];
+        TileBounds tb;
+        {
+            float X[kVpt], Y[kVpt], GX[kVpt], GY[kVpt], W[kVpt];
 #pragma unroll
-        for (int q = 0; q < kVpt; ++q) {
-            if (valid[q]) {
-                voxel_head(A.g, B, vi[q], vj[q], vk[q], X[q], Y[q], Z[q], GX[q], GY[q]);
-                WMM[q] = __fmul_rn(__ldg(wet + b * V + vidx[q]), 10.0f);
-            } else {
-                X[q] = Y[q] = Z[q] = 0.0f;
-                GX[q] = GY[q] = 1.0f;
-                WMM[q] = INFINITY;
+            for (int q = 0; q < kVpt; ++q) {
+                if (valid[q]) {
+                    const int i = vidx[q] % A.g.nx, jk = vidx[q] / A.g.nx;
+                    float Z;
+                    voxel_head(A.g, B, i, jk % A.g.ny, jk / A.g.ny, X[q], Y[q], Z, GX[q], GY[q]);
+                    W[q] = __fmul_rn(__ldg(wet + b * V + vidx[q]), 10.0f);
+                } else {
+                    X[q] = Y[q] = 0.0f;
+                    GX[q] = GY[q] = 1.0f;
+                    W[q] = INFINITY;
+                }
+            }
+            tb = tile_bounds<kVpt, kThreads>(X, Y, GX, GY, valid, s_red);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                XP[p] = make_float2(X[2 * p], X[2 * p + 1]);
+                YP[p] = make_float2(Y[2 * p], Y[2 * p + 1]);
+                GXP[p] = make_float2(GX[2 * p], GX[2 * p + 1]);
+                GYP[p] = make_float2(GY[2 * p], GY[2 * p + 1]);
+                WP[p] = make_float2(W[2 * p], W[2 * p + 1]);
             }
         }
-        const TileBounds tb = tile_bounds<kVpt>(X, Y, GX, GY, valid, s_red);
         float bs_s[kVpt], bs_c[kVpt];
 #pragma unroll
         for (int q = 0; q < kVpt; ++q) bs_s[q] = bs_c[q] = 0.0f;
@@ -311,38 +344,45 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
             bool any = false;
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
-                act[q] = valid[q] && !(WMM[q] > cut);
+                const float w = (q & 1) ? WP[q >> 1].y : WP[q >> 1].x;
+                act[q] = valid[q] && !(w > cut);
                 any |= act[q];
             }
             if (!__syncthreads_or(any)) continue;
-            stage_lut(B, L.energy_id, s_dep, s_sig, s_idd);
+            stage_lut<kThreads>(B, L.energy_id, s_dep, s_sig, s_idd);
             __syncthreads();
             const float *cabc = B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2;
             const float ca = __ldg(cabc), cb = __ldg(cabc + 1), cc = __ldg(cabc + 2);
-            float pf[kVpt], hf[kVpt], ps2[kVpt], hs2[kVpt];
+            float pf[kVpt], hf[kVpt];
+            float2 PS[NP], HS[NP];
             float hmax = -INFINITY;
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
-                ps2[q] = hs2[q] = pf[q] = hf[q] = 0.0f;
+                float ps2 = 0.0f, hs2 = 0.0f;
+                pf[q] = hf[q] = 0.0f;
                 if (act[q]) {
-                    layer_params(WMM[q], source_distance(B, X[q], Y[q], Z[q]), L.r80, s_dep,
-                                 s_sig, s_idd, B.lut_len, ca, cb, cc, pf[q], hf[q], ps2[q],
-                                 hs2[q]);
-                    hmax = fmaxf(hmax, hs2[q]);
+                    const int p = q >> 1;
+                    const float X = (q & 1) ? XP[p].y : XP[p].x;
+                    const float Y = (q & 1) ? YP[p].y : YP[p].x;
+                    const float gx = (q & 1) ? GXP[p].y : GXP[p].x;
+                    const float w = (q & 1) ? WP[p].y : WP[p].x;
+                    const float Z = B.geom.vsadx * (1.0f - gx);
+                    layer_params(w, source_distance(B, X, Y, Z), L.r80, s_dep, s_sig, s_idd,
+                                 B.lut_len, ca, cb, cc, pf[q], hf[q], ps2, hs2);
+                    hmax = fmaxf(hmax, hs2);
+                }
+                if (q & 1) {
+                    PS[q >> 1].y = ps2;
+                    HS[q >> 1].y = hs2;
+                } else {
+                    PS[q >> 1].x = ps2;
+                    HS[q >> 1].x = hs2;
                 }
             }
-            const float nhs = -block_max_slot8(hmax, s_red);
-            float2 X2[NP], Y2[NP], GX2[NP], GY2[NP], PS2[NP], HS2[NP], AP[NP], AH[NP];
+            const float nhs = -block_max_slot8<kThreads>(hmax, s_red);
+            float2 AP[NP], AH[NP];
 #pragma unroll
-            for (int p = 0; p < NP; ++p) {
-                X2[p] = make_float2(X[2 * p], X[2 * p + 1]);
-                Y2[p] = make_float2(Y[2 * p], Y[2 * p + 1]);
-                GX2[p] = make_float2(GX[2 * p], GX[2 * p + 1]);
-                GY2[p] = make_float2(GY[2 * p], GY[2 * p + 1]);
-                PS2[p] = make_float2(ps2[2 * p], ps2[2 * p + 1]);
-                HS2[p] = make_float2(hs2[2 * p], hs2[2 * p + 1]);
-                AP[p] = AH[p] = make_float2(0.0f, 0.0f);
-            }
+            for (int p = 0; p < NP; ++p) AP[p] = AH[p] = make_float2(0.0f, 0.0f);
 
             const int s0 = B.spot_start + L.spot_start;
             for (int base = 0; base < L.n_spots; base += kThreads * kCull) {
@@ -381,16 +421,17 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                     }
                 }
                 __syncthreads();
+#pragma unroll 2
                 for (int c = 0; c < total; ++c) {
                     const SpotRec r = s_spot[c];
                     const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
                                  ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
-                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, X2[p], Y2[p],
-                                                  GX2[p], GY2[p]);
-                        AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS2[p], qq)), AP[p]);
-                        AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS2[p], qq)), AH[p]);
+                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
+                                                  GXP[p], GYP[p]);
+                        AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS[p], qq)), AP[p]);
+                        AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
                     }
                 }
                 __syncthreads();
@@ -401,12 +442,12 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                     const float ap = (q & 1) ? AP[q >> 1].y : AP[q >> 1].x;
                     const float ah = (q & 1) ? AH[q >> 1].y : AH[q >> 1].x;
                     const float ld = fmaf(pf[q], ap, hf[q] * ah);
-                    neumaier(bs_s[q], bs_c[q], ld);
+                    if (BEAM_OUT) neumaier(bs_s[q], bs_c[q], ld);
                     neumaier(tot_s[q], tot_c[q], ld);
                 }
             }
         }
-        if (beam_dose) {
+        if (BEAM_OUT) {
 #pragma unroll
             for (int q = 0; q < kVpt; ++q)
                 if (valid[q]) beam_dose[b * V + vidx[q]] = (bs_s[q] + bs_c[q]) * A.scale;
@@ -420,24 +461,23 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 
 // ------------------------------------------------------------------ adjoint
 
-constexpr int kAdjVpt = 4;  // adjoint: voxels per thread (same tile shape)
-
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kAdjThreads, PB_ADJ_MIN_BLOCKS)
 k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
           const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
           const float *__restrict__ wfield, float *__restrict__ grad)
 {
     __shared__ float s_dep[PB_MAX_LUT_LEN], s_sig[PB_MAX_LUT_LEN], s_idd[PB_MAX_LUT_LEN];
-    __shared__ VoxRec s_vox[kThreads * kAdjVpt];
-    __shared__ int s_cand[kThreads * kSpt];
-    __shared__ float s_gsum[kThreads * kSpt];
+    constexpr int kWarps = kAdjThreads / 32;
+    __shared__ VoxRec s_vox[kAdjThreads * kAdjVpt];
+    __shared__ int s_cand[kAdjThreads * kSpt];
+    __shared__ float s_gsum[kAdjThreads * kSpt];
     __shared__ float s_red[kWarps][9];
     __shared__ int s_wcount[kAdjVpt > kSpt ? kAdjVpt : kSpt][kWarps];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int vi[kAdjVpt], vj[kAdjVpt], vk[kAdjVpt];
     bool valid[kAdjVpt];
-    int64_t vidx[kAdjVpt];
+    int vidx[kAdjVpt];
     tile_voxels<kAdjVpt>(A, vi, vj, vk, valid, vidx);
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
     float wv[kAdjVpt];
@@ -448,7 +488,7 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
         anyw |= (wv[q] != 0.0f);
     }
     if (!__syncthreads_or(anyw)) return;
-    for (int c = threadIdx.x; c < kThreads * kSpt; c += kThreads) s_gsum[c] = 0.0f;
+    for (int c = threadIdx.x; c < kAdjThreads * kSpt; c += kAdjThreads) s_gsum[c] = 0.0f;
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
@@ -464,7 +504,7 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                 WMM[q] = INFINITY;
             }
         }
-        const TileBounds tb = tile_bounds<kAdjVpt>(X, Y, GX, GY, valid, s_red);
+        const TileBounds tb = tile_bounds<kAdjVpt, kAdjThreads>(X, Y, GX, GY, valid, s_red);
 
         for (int l = 0; l < B.n_layers; ++l) {
             const PbLayer L = layers[B.layer_start + l];
@@ -484,7 +524,7 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                 mq[q] = __ballot_sync(0xffffffffu, act[q]);
                 if (lane == 0) s_wcount[q][warp] = __popc(mq[q]);
             }
-            stage_lut(B, L.energy_id, s_dep, s_sig, s_idd);
+            stage_lut<kAdjThreads>(B, L.energy_id, s_dep, s_sig, s_idd);
             __syncthreads();
             int nact = 0, pos[kAdjVpt];
 #pragma unroll
@@ -515,15 +555,15 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                 }
             }
             // includes the barrier that publishes s_vox and frees s_wcount
-            const float nhs = -block_max_slot8(hmax, s_red);
+            const float nhs = -block_max_slot8<kAdjThreads>(hmax, s_red);
 
             const int s0 = B.spot_start + L.spot_start;
-            for (int base = 0; base < L.n_spots; base += kThreads * kSpt) {
+            for (int base = 0; base < L.n_spots; base += kAdjThreads * kSpt) {
                 bool keep[kSpt];
                 unsigned m[kSpt];
 #pragma unroll
                 for (int c = 0; c < kSpt; ++c) {
-                    const int si = base + c * kThreads + threadIdx.x;
+                    const int si = base + c * kAdjThreads + threadIdx.x;
                     keep[c] = false;
                     if (si < L.n_spots) {
                         const float4 ga = __ldg(geo + 2 * (int64_t)(s0 + si));
@@ -542,16 +582,16 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                         if (w == warp) pos = total + __popc(m[c] & ((1u << lane) - 1u));
                         total += s_wcount[c][w];
                     }
-                    if (keep[c]) s_cand[pos] = s0 + base + c * kThreads + threadIdx.x;
+                    if (keep[c]) s_cand[pos] = s0 + base + c * kAdjThreads + threadIdx.x;
                 }
                 __syncthreads();
                 // Work items (spot pair, voxel stripe): every thread busy even
                 // when few spots survive the culling.  Partial sums meet in
                 // shared memory, then one atomic per spot goes to global.
                 const int npair = (total + 1) >> 1;
-                const int stripes = npair >= kThreads ? 1 : kThreads / npair;
+                const int stripes = npair >= kAdjThreads ? 1 : kAdjThreads / npair;
                 const int items = npair * stripes;
-                for (int it = threadIdx.x; it < items; it += kThreads) {
+                for (int it = threadIdx.x; it < items; it += kAdjThreads) {
                     const int sp = it % npair, vs = it / npair;
                     float2 nx, ny, tx, nty, ncs, it2;
                     float4 ga[2], gb[2];
@@ -583,7 +623,7 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                     if (acc.y != 0.0f && 2 * sp + 1 < total) atomicAdd(&s_gsum[2 * sp + 1], acc.y);
                 }
                 __syncthreads();
-                for (int c = threadIdx.x; c < total; c += kThreads) {
+                for (int c = threadIdx.x; c < total; c += kAdjThreads) {
                     const float a = s_gsum[c];
                     if (a != 0.0f) atomicAdd(grad + s_cand[c], a);
                     s_gsum[c] = 0.0f;
@@ -684,9 +724,12 @@ PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
     PlanArgs A;
     fill_args(A, g, beams, n_beams, scale);
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
-    k_dose<<<(unsigned)tiles, kThreads, 0, st>>>(A, wet, layers,
-                                                 reinterpret_cast<const float4 *>(geo), mu,
-                                                 dose, beam_dose);
+    if (beam_dose)
+        k_dose<true><<<(unsigned)tiles, kThreads, 0, st>>>(
+            A, wet, layers, reinterpret_cast<const float4 *>(geo), mu, dose, beam_dose);
+    else
+        k_dose<false><<<(unsigned)tiles, kThreads, 0, st>>>(
+            A, wet, layers, reinterpret_cast<const float4 *>(geo), mu, dose, nullptr);
     return check_launch("k_dose");
 }
 
@@ -705,7 +748,7 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                             "cudaMemsetAsync(grad)");
     if (s != PB_OK) return s;
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
-    k_adjoint<<<(unsigned)tiles, kThreads, 0, st>>>(A, wet, layers,
+    k_adjoint<<<(unsigned)tiles, kAdjThreads, 0, st>>>(A, wet, layers,
                                                     reinterpret_cast<const float4 *>(geo), w,
                                                     grad);
     return check_launch("k_adjoint");
