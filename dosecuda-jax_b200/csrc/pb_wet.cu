@@ -122,18 +122,6 @@ __device__ __forceinline__ float trilinear(const float *__restrict__ rho,
     return fmaf(az, c1 - c0, c0);
 }
 
-// Raw WET (cm) per voxel: samples every 1 mm from the voxel toward the
-// source while the texture coordinate stays inside [0, n); WET = -0.05 +
-// 0.1 * sum(max(RLSP, 0)).  The sum is carried in FP64 (FP32 partials of 16
-// samples).  A ray that exceeds the grid-diagonal step cap stops and raises
-// PB_ERR_RAY_CAP in *status.
-//
-// TEX = true samples RLSP through a border-0, linearly filtered 3-D texture
-// and forms the ray direction with rnorm3df, as the reference does
-// (CudaClasses.cuh:41-52, TextureClasses.cu:14-41), so the samples are the
-// reference's own.  TEX = false interpolates with exact FP32 trilinear
-// weights from global memory and forms the direction in FP64, the CPU
-// oracle's arithmetic.
 // Number of leading samples t = 0, 1, ... whose texture coordinates are
 // certainly inside [0, n) on every axis, so the in-grid test can be skipped
 // for them.  The bound is taken on the exact (real-number) coordinates
