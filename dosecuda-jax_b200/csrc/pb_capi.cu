@@ -512,3 +512,142 @@ PbStatus pb_proton_spot_host(int gpu_id, double vsadx, double vsady, const float
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ variants, batch
+
+namespace pb {
+
+// work_dev layout: [queue counter | padding to 256 B][WET records][dose records]
+static size_t batch_wet_offset() { return 256; }
+static size_t batch_dose_offset(int n_plans)
+{
+    const size_t w = batch_wet_offset() + batch_wet_size() * (size_t)n_plans * PB_MAX_BEAMS;
+    return (w + 255) & ~(size_t)255;
+}
+
+}  // namespace pb
+
+extern "C" {
+
+int pb_dose_variant_count(void) { return dose_variant_count(); }
+
+const char *pb_dose_variant_name(int variant) { return dose_variant_name(variant); }
+
+PbStatus pb_dose_variant(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                         const float *wet_dev, const PbLayer *layers_dev,
+                         const float *spot_geo_dev, const float *mu_dev, float scale,
+                         float *dose_dev, int variant, void *stream)
+{
+    if (variant < 0 || variant >= dose_variant_count())
+        return set_error(PB_ERR_INVALID, "variant must be in [0, %d)", dose_variant_count());
+    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev);
+    if (s != PB_OK) return s;
+    if (!dose_dev || !mu_dev) return set_error(PB_ERR_INVALID, "NULL argument");
+    return launch_dose(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev, mu_dev, scale,
+                       dose_dev, nullptr, static_cast<cudaStream_t>(stream), variant);
+}
+
+size_t pb_batch_work_size(int n_plans)
+{
+    if (n_plans <= 0) return 0;
+    return batch_dose_offset(n_plans) + batch_dose_size() * (size_t)n_plans;
+}
+
+PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
+                        PbBatchInfo *info, void *stream)
+{
+    if (!plans || n_plans <= 0 || !work_dev || !info)
+        return set_error(PB_ERR_INVALID, "NULL argument or empty batch");
+    for (int p = 0; p < n_plans; ++p) {
+        const PbBatchPlan &P = plans[p];
+        PbStatus s = check_beams(&P.grid, P.beams, P.n_beams, P.wet_dev, P.layers_dev,
+                                 P.spot_geo_dev);
+        if (s != PB_OK)
+            return set_error(s, "plan %d: %s", p, pb_last_error());
+        if ((!P.rlsp_dev && !P.tex) || !P.raw_work_dev || !P.dose_dev || !P.mu_dev)
+            return set_error(PB_ERR_INVALID, "plan %d: NULL buffer", p);
+        if (P.tex && !texture_matches(P.tex, P.grid))
+            return set_error(PB_ERR_INVALID, "plan %d: texture extent differs from the grid", p);
+    }
+    // WET records in plan order
+    std::vector<unsigned char> wet_items(batch_wet_size() * (size_t)n_plans * PB_MAX_BEAMS);
+    long long bricks = 0;
+    int n_wet = 0;
+    for (int p = 0; p < n_plans; ++p) {
+        const PbBatchPlan &P = plans[p];
+        PbBeamGeom geoms[PB_MAX_BEAMS];
+        for (int b = 0; b < P.n_beams; ++b) geoms[b] = P.beams[b].geom;
+        bricks += fill_batch_wet(wet_items.data(), n_wet, P.grid, geoms, P.n_beams, P.rlsp_dev,
+                                 texture_object(P.tex), P.raw_work_dev, P.wet_dev, bricks);
+        n_wet += P.n_beams;
+    }
+    // dose records, most expensive tiles first (spots over all beams)
+    std::vector<int> order((size_t)n_plans);
+    std::vector<long long> cost((size_t)n_plans);
+    for (int p = 0; p < n_plans; ++p) {
+        order[p] = p;
+        long long c = 0;
+        for (int b = 0; b < plans[p].n_beams; ++b) c += plans[p].beams[b].n_spots;
+        cost[p] = c;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<unsigned char> dose_items(batch_dose_size() * (size_t)n_plans);
+    long long tiles = 0;
+    for (int q = 0; q < n_plans; ++q) {
+        const PbBatchPlan &P = plans[order[q]];
+        BatchDose &D = *reinterpret_cast<BatchDose *>(dose_items.data() + batch_dose_size() * q);
+        fill_batch_dose(D, P.grid, P.beams, P.n_beams, P.scale, P.wet_dev, P.layers_dev,
+                        P.spot_geo_dev, P.mu_dev, P.dose_dev, tiles);
+        tiles += plan_tiles(P.grid);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char *w = static_cast<unsigned char *>(work_dev);
+    PbStatus s = check_cuda(cudaMemcpyAsync(w + batch_wet_offset(), wet_items.data(),
+                                            batch_wet_size() * (size_t)n_wet,
+                                            cudaMemcpyHostToDevice, st), "H2D batch WET records");
+    if (s != PB_OK) return s;
+    s = check_cuda(cudaMemcpyAsync(w + batch_dose_offset(n_plans), dose_items.data(),
+                                   dose_items.size(), cudaMemcpyHostToDevice, st),
+                   "H2D batch dose records");
+    if (s != PB_OK) return s;
+    s = check_cuda(cudaStreamSynchronize(st), "synchronize");
+    if (s != PB_OK) return s;
+    info->n_bricks = bricks;
+    info->n_tiles = tiles;
+    info->n_wet_items = n_wet;
+    info->n_plans = n_plans;
+    return PB_OK;
+}
+
+PbStatus pb_batch_run(const PbBatchInfo *info, void *work_dev, int flags, int variant,
+                      int blocks_per_sm, int *status_dev, void *stream)
+{
+    if (!info || !work_dev || info->n_plans <= 0)
+        return set_error(PB_ERR_INVALID, "NULL argument or empty batch");
+    if (variant < 0 || variant >= dose_variant_count())
+        return set_error(PB_ERR_INVALID, "variant must be in [0, %d)", dose_variant_count());
+    if (blocks_per_sm <= 0 || blocks_per_sm > 32)
+        return set_error(PB_ERR_INVALID, "blocks_per_sm must be in [1, 32]");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char *w = static_cast<unsigned char *>(work_dev);
+    if (flags & PB_BATCH_WET) {
+        PbStatus s = launch_wet_batch(w + batch_wet_offset(), info->n_wet_items, info->n_bricks,
+                                      status_dev, st);
+        if (s != PB_OK) return s;
+    }
+    if (flags & PB_BATCH_DOSE) {
+        int dev = 0, sms = 0;
+        PbStatus s = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        if (s != PB_OK) return s;
+        s = check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+                       "cudaDeviceGetAttribute");
+        if (s != PB_OK) return s;
+        return launch_dose_batch(w + batch_dose_offset(info->n_plans), info->n_plans,
+                                 info->n_tiles, reinterpret_cast<unsigned long long *>(w), variant,
+                                 blocks_per_sm * sms, st);
+    }
+    return PB_OK;
+}
+
+}  // extern "C"

@@ -36,9 +36,6 @@
 
 namespace pb {
 
-constexpr int kThreads = 128;       // forward block
-constexpr int kVpt = 4;             // forward: voxels per thread (z, z+2, z+4, z+6)
-constexpr int kCull = 2;            // forward: spots culled per thread per chunk
 constexpr int kAdjThreads = 256;    // adjoint block
 constexpr int kAdjVpt = 2;          // adjoint: voxels per thread (z, z+4)
 constexpr int kSpt = 2;             // adjoint: spots culled per thread per chunk
@@ -214,10 +211,10 @@ __device__ __forceinline__ float block_max_slot8(float v, float (*s_red)[9])
 // Voxels of this block's tile owned by this thread: (li, lj, lk + step*q),
 // with 64 * 8/NV threads per 8x8x8 tile.
 template <int NV>
-__device__ __forceinline__ void tile_voxels(const PlanArgs &A, int *vi, int *vj, int *vk,
-                                            bool *valid, int *vidx)
+__device__ __forceinline__ void tile_voxels(const PlanArgs &A, int tile, int *vi, int *vj,
+                                            int *vk, bool *valid, int *vidx)
 {
-    int t = blockIdx.x;
+    int t = tile;
     const int tx = t % A.tiles_x;
     t /= A.tiles_x;
     const int ty = t % A.tiles_y;
@@ -268,34 +265,48 @@ __device__ __forceinline__ void stage_lut(const PbBeam &B, int e, float *s_dep,
 
 // ------------------------------------------------------------------ forward
 
-// BEAM_OUT: also write each beam's dose (beam_dose != nullptr).
-#ifndef PB_DOSE_MIN_BLOCKS
-#define PB_DOSE_MIN_BLOCKS 5
-#endif
 #ifndef PB_ADJ_MIN_BLOCKS
 #define PB_ADJ_MIN_BLOCKS 3
 #endif
 
-template <bool BEAM_OUT>
-__global__ void __launch_bounds__(kThreads, PB_DOSE_MIN_BLOCKS)
-k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
-       const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
-       const float *__restrict__ mu, float *__restrict__ dose,
-       float *__restrict__ beam_dose)
+// Shared memory of one forward tile.
+template <int NT, int KCULL>
+struct DoseShared {
+    float dep[PB_MAX_LUT_LEN], sig[PB_MAX_LUT_LEN], idd[PB_MAX_LUT_LEN];
+    SpotRec spot[NT * KCULL];
+    float red[NT / 32][9];
+    int wcount[KCULL][NT / 32];
+};
+
+// Forward dose of one 8x8x8 tile of one plan by one block of NT threads,
+// VPT = 512 / NT voxels per thread; spots are culled KCULL per thread per
+// compaction round.  BEAM_OUT: also write each beam's dose.
+template <int NT, int VPT, int KCULL, bool BEAM_OUT>
+__device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
+                                          const float *__restrict__ wet,
+                                          const PbLayer *__restrict__ layers,
+                                          const float4 *__restrict__ geo,
+                                          const float *__restrict__ mu, float *__restrict__ dose,
+                                          float *__restrict__ beam_dose,
+                                          DoseShared<NT, KCULL> &sh)
 {
+    static_assert(NT * VPT == 512, "a block covers one 8x8x8 tile");
+    constexpr int kVpt = VPT;
+    constexpr int kThreads = NT;
+    constexpr int kCull = KCULL;
     constexpr int NP = kVpt / 2;  // voxel pairs per thread
     constexpr int kWarps = kThreads / 32;
-    __shared__ float s_dep[PB_MAX_LUT_LEN], s_sig[PB_MAX_LUT_LEN], s_idd[PB_MAX_LUT_LEN];
-    __shared__ SpotRec s_spot[kThreads * kCull];
-    __shared__ float s_red[kWarps][9];
-    __shared__ int s_wcount[kCull][kWarps];
+    float *s_dep = sh.dep, *s_sig = sh.sig, *s_idd = sh.idd;
+    SpotRec *s_spot = sh.spot;
+    float (*s_red)[9] = sh.red;
+    int (*s_wcount)[kWarps] = sh.wcount;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int vidx[kVpt];
     bool valid[kVpt];
     {
         int vi[kVpt], vj[kVpt], vk[kVpt];
-        tile_voxels<kVpt>(A, vi, vj, vk, valid, vidx);
+        tile_voxels<kVpt>(A, tile, vi, vj, vk, valid, vidx);
     }
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
 
@@ -459,6 +470,62 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
         if (valid[q]) dose[vidx[q]] = (tot_s[q] + tot_c[q]) * A.scale;
 }
 
+#ifndef PB_DOSE_MIN_BLOCKS
+#define PB_DOSE_MIN_BLOCKS 5
+#endif
+// Resident blocks per SM the forward kernels are compiled for.
+template <int NT> constexpr int dose_min_blocks() { return NT == 128 ? PB_DOSE_MIN_BLOCKS : 3; }
+
+template <int NT, int VPT, int KCULL, bool BEAM_OUT>
+__global__ void __launch_bounds__(NT, dose_min_blocks<NT>())
+k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+       const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
+       const float *__restrict__ mu, float *__restrict__ dose,
+       float *__restrict__ beam_dose)
+{
+    __shared__ DoseShared<NT, KCULL> sh;
+    dose_tile<NT, VPT, KCULL, BEAM_OUT>(A, blockIdx.x, wet, layers, geo, mu, dose, beam_dose, sh);
+}
+
+// One plan of a batch as the persistent kernel reads it.
+struct BatchDose {
+    PlanArgs A;
+    const float *wet;
+    const PbLayer *layers;
+    const float4 *geo;
+    const float *mu;
+    float *dose;
+    long long tile_start;   // first work item of the plan (queue order)
+};
+
+// Persistent forward over many plans: blocks take (plan, tile) items from
+// one queue until it is empty.  Plans are stored in decreasing order of
+// estimated cost per tile so that the expensive tiles start first.
+template <int NT, int VPT, int KCULL>
+__global__ void __launch_bounds__(NT, dose_min_blocks<NT>())
+k_dose_batch(const BatchDose *__restrict__ plans, int n_plans, long long n_items,
+             unsigned long long *counter)
+{
+    __shared__ DoseShared<NT, KCULL> sh;
+    __shared__ long long s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(counter, 1ULL);
+        __syncthreads();
+        const long long it = s_item;
+        __syncthreads();
+        if (it >= n_items) break;
+        int lo = 0, hi = n_plans - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (plans[mid].tile_start <= it) lo = mid; else hi = mid - 1;
+        }
+        const BatchDose &D = plans[lo];
+        dose_tile<NT, VPT, KCULL, false>(D.A, (int)(it - D.tile_start), D.wet, D.layers, D.geo,
+                                         D.mu, D.dose, nullptr, sh);
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ adjoint
 
 __global__ void __launch_bounds__(kAdjThreads, PB_ADJ_MIN_BLOCKS)
@@ -478,7 +545,7 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
     int vi[kAdjVpt], vj[kAdjVpt], vk[kAdjVpt];
     bool valid[kAdjVpt];
     int vidx[kAdjVpt];
-    tile_voxels<kAdjVpt>(A, vi, vj, vk, valid, vidx);
+    tile_voxels<kAdjVpt>(A, blockIdx.x, vi, vj, vk, valid, vidx);
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
     float wv[kAdjVpt];
     bool anyw = false;
@@ -716,21 +783,97 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
     for (int b = 0; b < n_beams; ++b) A.beams[b] = beams[b];
 }
 
+// Forward kernel variants the autotuner chooses from: block threads x voxels
+// per thread over the 8x8x8 tile, and spots culled per thread per round.
+struct DoseVariant {
+    int nt, vpt, kcull;
+    const char *name;
+};
+static const DoseVariant kDoseVariants[] = {
+    {128, 4, 2, "t128_v4_c2"}, {128, 4, 1, "t128_v4_c1"}, {128, 4, 4, "t128_v4_c4"},
+    {256, 2, 1, "t256_v2_c1"}, {256, 2, 2, "t256_v2_c2"},
+};
+constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
+
+int dose_variant_count() { return kNumDoseVariants; }
+const char *dose_variant_name(int v)
+{
+    return (v >= 0 && v < kNumDoseVariants) ? kDoseVariants[v].name : "";
+}
+
+template <int NT, int VPT, int KCULL>
+static void launch_dose_t(const PlanArgs &A, unsigned tiles, const float *wet,
+                          const PbLayer *layers, const float4 *geo, const float *mu,
+                          float *dose, cudaStream_t st)
+{
+    k_dose<NT, VPT, KCULL, false><<<tiles, NT, 0, st>>>(A, wet, layers, geo, mu, dose, nullptr);
+}
+
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers, const float *geo,
                      const float *mu, float scale, float *dose, float *beam_dose,
-                     cudaStream_t st)
+                     cudaStream_t st, int variant)
 {
     PlanArgs A;
     fill_args(A, g, beams, n_beams, scale);
-    const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
-    if (beam_dose)
-        k_dose<true><<<(unsigned)tiles, kThreads, 0, st>>>(
-            A, wet, layers, reinterpret_cast<const float4 *>(geo), mu, dose, beam_dose);
-    else
-        k_dose<false><<<(unsigned)tiles, kThreads, 0, st>>>(
-            A, wet, layers, reinterpret_cast<const float4 *>(geo), mu, dose, nullptr);
+    const unsigned tiles = (unsigned)((int64_t)A.tiles_x * A.tiles_y * A.tiles_z);
+    const float4 *g4 = reinterpret_cast<const float4 *>(geo);
+    if (beam_dose) {
+        // per-beam output: the default shape only
+        k_dose<128, 4, 2, true><<<tiles, 128, 0, st>>>(A, wet, layers, g4, mu, dose, beam_dose);
+        return check_launch("k_dose");
+    }
+    switch (variant) {
+    case 1: launch_dose_t<128, 4, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 2: launch_dose_t<128, 4, 4>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 3: launch_dose_t<256, 2, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 4: launch_dose_t<256, 2, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    default: launch_dose_t<128, 4, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    }
     return check_launch("k_dose");
+}
+
+void fill_batch_dose(BatchDose &D, const PbGrid &g, const PbBeam *beams, int n_beams,
+                     float scale, const float *wet, const PbLayer *layers, const float *geo,
+                     const float *mu, float *dose, long long tile_start)
+{
+    fill_args(D.A, g, beams, n_beams, scale);
+    D.wet = wet;
+    D.layers = layers;
+    D.geo = reinterpret_cast<const float4 *>(geo);
+    D.mu = mu;
+    D.dose = dose;
+    D.tile_start = tile_start;
+}
+
+size_t batch_dose_size() { return sizeof(BatchDose); }
+
+long long plan_tiles(const PbGrid &g)
+{
+    return (long long)((g.nx + 7) / 8) * ((g.ny + 7) / 8) * ((g.nz + 7) / 8);
+}
+
+PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items,
+                           unsigned long long *counter, int variant, int blocks,
+                           cudaStream_t st)
+{
+    PbStatus s = check_cuda(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st),
+                            "cudaMemsetAsync(queue)");
+    if (s != PB_OK) return s;
+    const BatchDose *P = static_cast<const BatchDose *>(plans_dev);
+    switch (variant) {
+    case 1: k_dose_batch<128, 4, 1><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 2: k_dose_batch<128, 4, 4><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 3: k_dose_batch<256, 2, 1><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 4: k_dose_batch<256, 2, 2><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
+    default: k_dose_batch<128, 4, 2><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    }
+    return check_launch("k_dose_batch");
+}
+
+int dose_variant_threads(int variant)
+{
+    return (variant >= 0 && variant < kNumDoseVariants) ? kDoseVariants[variant].nt : 128;
 }
 
 PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,

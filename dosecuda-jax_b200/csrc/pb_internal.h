@@ -29,6 +29,14 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
                     const PbBeamGeom *beams, int n_beams, float *raw, float *wet, int *status,
                     cudaStream_t st);
 
+// Batched WET pass (pb_wet.cu): one record per (plan, beam).
+size_t batch_wet_size();
+long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbBeamGeom *beams,
+                         int n_beams, const float *rlsp, cudaTextureObject_t tex, float *raw,
+                         float *wet, long long brick_start);
+PbStatus launch_wet_batch(const void *items_dev, int n_items, long long n_bricks, int *status,
+                          cudaStream_t st);
+
 PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st);
 PbStatus texture_update(uint64_t h, const float *rlsp, cudaStream_t st);
 bool texture_matches(uint64_t h, const PbGrid &g);
@@ -38,7 +46,22 @@ void texture_destroy(uint64_t h);
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers,
                      const float *geo, const float *mu, float scale,
-                     float *dose, float *beam_dose, cudaStream_t st);
+                     float *dose, float *beam_dose, cudaStream_t st, int variant = 0);
+
+int dose_variant_count();
+const char *dose_variant_name(int v);
+int dose_variant_threads(int variant);
+
+// Batched forward (pb_dose.cu): device records of the plans of a batch.
+struct BatchDose;
+size_t batch_dose_size();
+long long plan_tiles(const PbGrid &g);
+void fill_batch_dose(BatchDose &D, const PbGrid &g, const PbBeam *beams, int n_beams,
+                     float scale, const float *wet, const PbLayer *layers, const float *geo,
+                     const float *mu, float *dose, long long tile_start);
+PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items,
+                           unsigned long long *counter, int variant, int blocks,
+                           cudaStream_t st);
 
 PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                         const float *wet, const PbLayer *layers,

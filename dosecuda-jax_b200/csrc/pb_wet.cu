@@ -174,17 +174,11 @@ __device__ __forceinline__ float ray_sample(const float *__restrict__ rho,
 // weights from global memory and forms the direction in FP64, the CPU
 // oracle's arithmetic.
 template <bool TEX>
-__global__ void __launch_bounds__(128)
-k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
-           const __grid_constant__ BeamGeomSet bs, int zbricks, int cap,
-           float *__restrict__ raw, int *status)
+__device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
+                                                cudaTextureObject_t tex, const PbGrid &g,
+                                                const PbBeamGeom &B, int i, int j, int k,
+                                                int cap, int *status)
 {
-    const int b = blockIdx.z / zbricks;
-    const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
-    const int j = blockIdx.y * 4 + threadIdx.y;
-    const int i = blockIdx.x * 8 + threadIdx.x;
-    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
-    const PbBeamGeom &B = bs.b[b];
     float px, py, pz, ux, uy, uz;
     vox_mm(B, g.spacing, i, j, k, px, py, pz);
     if (TEX) {
@@ -235,9 +229,23 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
         part += fmaxf(ray_sample<TEX>(rho, tex, g, x, y, z), 0.0f);
     }
     acc += (double)part;
+    return __double2float_rn(fma(0.1, acc, -0.05));
+}
+
+template <bool TEX>
+__global__ void __launch_bounds__(128)
+k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
+           const __grid_constant__ BeamGeomSet bs, int zbricks, int cap,
+           float *__restrict__ raw, int *status)
+{
+    const int b = blockIdx.z / zbricks;
+    const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
+    const int j = blockIdx.y * 4 + threadIdx.y;
+    const int i = blockIdx.x * 8 + threadIdx.x;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
-    raw[b * V + v] = __double2float_rn(fma(0.1, acc, -0.05));
+    raw[b * V + v] = raytrace_voxel<TEX>(rho, tex, g, bs.b[b], i, j, k, cap, status);
 }
 
 // Linear map of the smoothing samples in index space, per beam: head ->
@@ -329,19 +337,11 @@ __device__ __forceinline__ int round_fadd(float m, float tie, bool &near)
     return __float_as_int(t) - 0x4B400000;
 }
 
-__global__ void __launch_bounds__(128)
-k_smooth(const float *__restrict__ raw, PbGrid g,
-         const __grid_constant__ BeamGeomSet bs, SmoothDirs d,
-         const __grid_constant__ SmoothSteps st, int zbricks, float *__restrict__ wet)
+__device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const PbGrid &g,
+                                              const PbBeamGeom &B, const SmoothDirs &d,
+                                              const double *M, const float (*dm)[3],
+                                              double inv_s_d, float tie, int i, int j, int k)
 {
-    const int b = blockIdx.z / zbricks;
-    const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
-    const int j = blockIdx.y * 4 + threadIdx.y;
-    const int i = blockIdx.x * 8 + threadIdx.x;
-    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
-    const PbBeamGeom &B = bs.b[b];
-    const int64_t V = (int64_t)g.nx * g.ny * g.nz;
-    const float *R = raw + b * V;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
     const float center = R[v];
     float sum = center;
@@ -352,22 +352,17 @@ k_smooth(const float *__restrict__ raw, PbGrid g,
     const float lim = __fmul_rn(center, 10.0f);
     const float s = g.spacing;
     const float inv_s = __fdiv_rn(1.0f, s);
-    if (!(1.0f < lim)) {
-        wet[b * V + v] = center;
-        return;
-    }
+    if (!(1.0f < lim)) return center;
     // m0: real-number index coordinates of the voxel itself
-    const double *M = st.rot[b];
     const double dhx = hx, dhy = hy, dhz = hz;
-    const float m0x = (float)((M[0] * dhx + M[1] * dhy + M[2] * dhz + (double)B.iso[0]) *
-                              st.inv_s);
-    const float m0y = (float)((M[3] * dhx + M[4] * dhy + M[5] * dhz + (double)B.iso[1]) *
-                              st.inv_s);
-    const float m0z = (float)((M[6] * dhx + M[7] * dhy + M[8] * dhz + (double)B.iso[2]) *
-                              st.inv_s);
-    const float tie = st.tie;
+    const float m0x =
+        (float)((M[0] * dhx + M[1] * dhy + M[2] * dhz + (double)B.iso[0]) * inv_s_d);
+    const float m0y =
+        (float)((M[3] * dhx + M[4] * dhy + M[5] * dhz + (double)B.iso[1]) * inv_s_d);
+    const float m0z =
+        (float)((M[6] * dhx + M[7] * dhy + M[8] * dhz + (double)B.iso[2]) * inv_s_d);
     for (int dd = 0; dd < 6; ++dd) {
-        const float dmx = st.dm[b][dd][0], dmy = st.dm[b][dd][1], dmz = st.dm[b][dd][2];
+        const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
         for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f)) {
             bool near = false;
             int ii = round_fadd(fmaf(dr, dmx, m0x), tie, near);
@@ -380,7 +375,88 @@ k_smooth(const float *__restrict__ raw, PbGrid g,
             }
         }
     }
-    wet[b * V + v] = __fdiv_rn(sum, (float)n);
+    return __fdiv_rn(sum, (float)n);
+}
+
+__global__ void __launch_bounds__(128)
+k_smooth(const float *__restrict__ raw, PbGrid g,
+         const __grid_constant__ BeamGeomSet bs, SmoothDirs d,
+         const __grid_constant__ SmoothSteps st, int zbricks, float *__restrict__ wet)
+{
+    const int b = blockIdx.z / zbricks;
+    const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
+    const int j = blockIdx.y * 4 + threadIdx.y;
+    const int i = blockIdx.x * 8 + threadIdx.x;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const int64_t V = (int64_t)g.nx * g.ny * g.nz;
+    const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
+    wet[b * V + v] = smooth_voxel(raw + b * V, g, bs.b[b], d, st.rot[b], st.dm[b], st.inv_s,
+                                  st.tie, i, j, k);
+}
+
+// One (plan, beam) of a batched WET pass.
+struct BatchWet {
+    PbGrid g;
+    PbBeamGeom geom;
+    const float *rlsp;
+    cudaTextureObject_t tex;
+    float *raw;                 // this beam's unsmoothed WET (V)
+    float *wet;                 // this beam's smoothed WET (V)
+    double rot[9];
+    float dm[6][3];
+    double inv_s;
+    float tie;
+    int cap;
+    int bx, by, bz;             // 8x4x4 bricks per axis
+    long long brick_start;      // first brick of this item in the launch
+};
+
+__device__ __forceinline__ int find_wet_item(const BatchWet *__restrict__ items, int n,
+                                             long long brick)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].brick_start <= brick) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Brick of 8x4x4 voxels of one (plan, beam) per block of 128 threads.
+__device__ __forceinline__ bool brick_voxel(const BatchWet &W, long long brick, int &i, int &j,
+                                            int &k)
+{
+    long long lb = brick - W.brick_start;
+    const int bx = (int)(lb % W.bx);
+    lb /= W.bx;
+    const int by = (int)(lb % W.by);
+    const int bz = (int)(lb / W.by);
+    i = bx * 8 + (threadIdx.x & 7);
+    j = by * 4 + ((threadIdx.x >> 3) & 3);
+    k = bz * 4 + (threadIdx.x >> 5);
+    return i < W.g.nx && j < W.g.ny && k < W.g.nz;
+}
+
+__global__ void __launch_bounds__(128)
+k_raytrace_batch(const BatchWet *__restrict__ items, int n_items, int *status)
+{
+    const BatchWet &W = items[find_wet_item(items, n_items, blockIdx.x)];
+    int i, j, k;
+    if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
+    const float r = W.tex
+                        ? raytrace_voxel<true>(W.rlsp, W.tex, W.g, W.geom, i, j, k, W.cap, status)
+                        : raytrace_voxel<false>(W.rlsp, 0, W.g, W.geom, i, j, k, W.cap, status);
+    W.raw[i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k)] = r;
+}
+
+__global__ void __launch_bounds__(128)
+k_smooth_batch(const BatchWet *__restrict__ items, int n_items, SmoothDirs d)
+{
+    const BatchWet &W = items[find_wet_item(items, n_items, blockIdx.x)];
+    int i, j, k;
+    if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
+    W.wet[i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k)] =
+        smooth_voxel(W.raw, W.g, W.geom, d, W.rot, W.dm, W.inv_s, W.tie, i, j, k);
 }
 
 int ray_step_cap(const PbGrid &g)
@@ -413,6 +489,58 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
     if (s != PB_OK) return s;
     k_smooth<<<grid, block, 0, st>>>(raw, g, bs, d, ss, zb, wet);
     return check_launch("k_smooth");
+}
+
+size_t batch_wet_size() { return sizeof(BatchWet); }
+
+// Fills the batch records of one plan's beams; returns the bricks they use.
+long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbBeamGeom *beams,
+                         int n_beams, const float *rlsp, cudaTextureObject_t tex, float *raw,
+                         float *wet, long long brick_start)
+{
+    BatchWet *W = static_cast<BatchWet *>(items_host) + first;
+    SmoothDirs d;
+    smooth_dirs(d.c, d.s);
+    SmoothSteps ss;
+    smooth_steps(g, beams, n_beams, d, ss);
+    const int64_t V = (int64_t)g.nx * g.ny * g.nz;
+    const int bx = (g.nx + 7) / 8, by = (g.ny + 3) / 4, bz = (g.nz + 3) / 4;
+    const long long per = (long long)bx * by * bz;
+    for (int b = 0; b < n_beams; ++b) {
+        BatchWet &w = W[b];
+        w.g = g;
+        w.geom = beams[b];
+        w.rlsp = rlsp;
+        w.tex = tex;
+        w.raw = raw + b * V;
+        w.wet = wet + b * V;
+        for (int m = 0; m < 9; ++m) w.rot[m] = ss.rot[b][m];
+        for (int dd = 0; dd < 6; ++dd)
+            for (int a = 0; a < 3; ++a) w.dm[dd][a] = ss.dm[b][dd][a];
+        w.inv_s = ss.inv_s;
+        w.tie = ss.tie;
+        w.cap = ray_step_cap(g);
+        w.bx = bx;
+        w.by = by;
+        w.bz = bz;
+        w.brick_start = brick_start + per * b;
+    }
+    return per * n_beams;
+}
+
+PbStatus launch_wet_batch(const void *items_dev, int n_items, long long n_bricks, int *status,
+                          cudaStream_t st)
+{
+    if (n_bricks <= 0) return PB_OK;
+    if (n_bricks > 0x7fffffffLL) return set_error(PB_ERR_INVALID, "batch too large");
+    SmoothDirs d;
+    smooth_dirs(d.c, d.s);
+    const BatchWet *I = static_cast<const BatchWet *>(items_dev);
+    k_raytrace_batch<<<(unsigned)n_bricks, 128, 0, st>>>(I, n_items, status);
+    PbStatus s = check_launch("k_raytrace_batch");
+    if (s != PB_OK) return s;
+    k_smooth_batch<<<(unsigned)n_bricks, 128, 0, st>>>(I, n_items, d);
+    return check_launch("k_smooth_batch");
 }
 
 // 3-D texture over an RLSP volume: float channel, linear filter, border 0,

@@ -69,6 +69,24 @@ class PbBeam(ctypes.Structure):
                 ("dvp_len", ctypes.c_int)]
 
 
+class PbBatchPlan(ctypes.Structure):
+    _fields_ = [("grid", PbGrid), ("n_beams", ctypes.c_int),
+                ("beams", PbBeam * PB_MAX_BEAMS),
+                ("rlsp_dev", ctypes.c_void_p), ("tex", ctypes.c_uint64),
+                ("raw_work_dev", ctypes.c_void_p), ("wet_dev", ctypes.c_void_p),
+                ("layers_dev", ctypes.c_void_p), ("spot_geo_dev", ctypes.c_void_p),
+                ("mu_dev", ctypes.c_void_p), ("scale", ctypes.c_float),
+                ("dose_dev", ctypes.c_void_p)]
+
+
+class PbBatchInfo(ctypes.Structure):
+    _fields_ = [("n_bricks", ctypes.c_longlong), ("n_tiles", ctypes.c_longlong),
+                ("n_wet_items", ctypes.c_int), ("n_plans", ctypes.c_int)]
+
+
+PB_BATCH_WET = 1
+PB_BATCH_DOSE = 2
+
 # numpy views of the structs (same layout) for bulk host arrays
 SPOT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("mu", "<f4"), ("energy_id", "<i4")])
 LAYER_DTYPE = np.dtype([("spot_start", "<i4"), ("n_spots", "<i4"), ("energy_id", "<i4"),
@@ -95,6 +113,13 @@ _SIGS = {
     "pb_dose": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP, _VP, _VP]),
     "pb_dose_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP,
                              _VP]),
+    "pb_dose_variant_count": (_I, []),
+    "pb_dose_variant_name": (ctypes.c_char_p, [_I]),
+    "pb_dose_variant": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP, _I,
+                             _VP]),
+    "pb_batch_work_size": (ctypes.c_size_t, [_I]),
+    "pb_batch_setup": (_I, [_VP, _I, _VP, ctypes.POINTER(PbBatchInfo), _VP]),
+    "pb_batch_run": (_I, [ctypes.POINTER(PbBatchInfo), _VP, _I, _I, _I, _VP, _VP]),
     "pb_objective_work_size": (ctypes.c_size_t, []),
     "pb_objective": (_I, [_VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP]),
     "pb_count_pairs": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),

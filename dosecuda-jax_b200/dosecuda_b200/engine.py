@@ -264,6 +264,20 @@ class DevicePlan:
                                _stream(self.device)), "pb_dose")
         return (dose, bd) if beam_doses else dose
 
+    def forward_variant(self, variant: int, mu_sorted: Optional[torch.Tensor] = None,
+                        scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Forward dose with one of the kernel shapes of pb_dose_variant."""
+        self._need_wet()
+        mu = (self.mu_sorted if mu_sorted is None else mu_sorted).contiguous()
+        dose = out if out is not None else torch.empty(self.n_vox, dtype=torch.float32,
+                                                       device=self.device)
+        check(_lib.lib.pb_dose_variant(ctypes.byref(self.grid),
+                                       ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                                       ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
+                                       ptr(mu), float(scale), ptr(dose), int(variant),
+                                       _stream(self.device)), "pb_dose_variant")
+        return dose
+
     def adjoint(self, dobj_ddose: torch.Tensor, scale: float = 1.0,
                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
         """grad[s] (sorted order) = scale * sum_v dobj_ddose[v] K(v, s)."""

@@ -274,3 +274,28 @@ def small_heterogeneous(seed: int = 7, angles=(0.0, 135.0), n_spots=300,
     return heterogeneous(seed, angles, n_spots, shape=shape, spacing=spacing, n_slabs=1,
                          n_spheres=2, semi_range=(10.0, 16.0), centre_jitter=5.0,
                          body_inset=15.0)
+
+
+def batch_cases(seed: int = 4, n_plans: int = 32, min_shape=(64, 64, 64),
+                max_shape=(160, 200, 200), spacings=(2.0, 2.5, 3.0), beams=(1, 4),
+                spots=(500, 20000)):
+    """Independent plans of uneven size for the batched mode: grid (nz, ny, nx)
+    drawn per plan between min_shape and max_shape, spacing from `spacings`,
+    1-4 beams at seeded gantry angles, 500-20,000 spots, heterogeneity as in
+    `heterogeneous`, target size scaled to the grid."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for p in range(n_plans):
+        shape = tuple(int(rng.integers(lo, hi + 1)) for lo, hi in zip(min_shape, max_shape))
+        s = float(rng.choice(spacings))
+        nb = int(rng.integers(beams[0], beams[1] + 1))
+        angles = tuple(float(a) for a in np.sort(rng.uniform(0.0, 360.0, nb)))
+        ext = min(shape) * s
+        semi = (0.10 * ext, 0.16 * ext)
+        case = heterogeneous(seed=int(rng.integers(1 << 30)), angles=angles,
+                             n_spots=int(rng.integers(spots[0], spots[1] + 1)), shape=shape,
+                             spacing=s, n_slabs=2, n_spheres=3, semi_range=semi,
+                             centre_jitter=0.05 * ext, body_inset=0.1 * ext)
+        case.name = f"batch{p}_{shape[2]}x{shape[1]}x{shape[0]}_{s:g}mm_{nb}beams"
+        out.append(case)
+    return out

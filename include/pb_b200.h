@@ -185,6 +185,65 @@ PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams,
                  const float *spot_geo_dev, const float *mu_dev, float scale,
                  float *dose_dev, float *beam_dose_dev, void *stream);
 
+/* Forward kernel shapes (block threads x voxels per thread over an 8x8x8
+ * tile, spots culled per thread per round) the autotuner chooses from.
+ * pb_dose uses variant 0. */
+int pb_dose_variant_count(void);
+const char *pb_dose_variant_name(int variant);
+PbStatus pb_dose_variant(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                         const float *wet_dev, const PbLayer *layers_dev,
+                         const float *spot_geo_dev, const float *mu_dev, float scale,
+                         float *dose_dev, int variant, void *stream);
+
+/* ------------------------------------------------------------ batch */
+
+/* One plan of a batch, as its caller holds it on the device.  beams[]
+ * index into the plan's own layers_dev / spot_geo_dev / mu_dev; wet_dev and
+ * raw_work_dev hold n_beams x V floats; tex (or rlsp_dev when tex == 0)
+ * is the plan's RLSP. */
+typedef struct {
+    PbGrid grid;
+    int n_beams;
+    PbBeam beams[PB_MAX_BEAMS];
+    const float *rlsp_dev;
+    PbTexture tex;
+    float *raw_work_dev;
+    float *wet_dev;
+    const PbLayer *layers_dev;
+    const float *spot_geo_dev;
+    const float *mu_dev;
+    float scale;
+    float *dose_dev;
+} PbBatchPlan;
+
+/* Sizes of a prepared batch, filled by pb_batch_setup. */
+typedef struct {
+    long long n_bricks;     /* WET work: 8x4x4-voxel bricks over all (plan, beam) */
+    long long n_tiles;      /* dose work: 8x8x8 tiles over all plans              */
+    int n_wet_items;        /* (plan, beam) records                              */
+    int n_plans;
+} PbBatchInfo;
+
+#define PB_BATCH_WET  1     /* recompute every plan's WET                       */
+#define PB_BATCH_DOSE 2     /* recompute every plan's dose                      */
+
+/* Device work space for a batch of n_plans: plan records and the queue. */
+size_t pb_batch_work_size(int n_plans);
+
+/* Writes the batch's records into work_dev (synchronous; not for use
+ * inside a stream capture).  Plans are ordered by estimated cost per tile,
+ * most expensive first. */
+PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
+                        PbBatchInfo *info, void *stream);
+
+/* Runs a prepared batch: the WET pass of every (plan, beam) in one launch
+ * of 8x4x4 bricks, then one persistent forward launch of blocks_per_sm
+ * blocks per SM that take (plan, tile) items from a queue in work_dev.
+ * No allocation and no host synchronisation: it can be captured in a CUDA
+ * graph once and replayed.  Concurrent runs on one work_dev race. */
+PbStatus pb_batch_run(const PbBatchInfo *info, void *work_dev, int flags, int variant,
+                      int blocks_per_sm, int *status_dev, void *stream);
+
 /* Adjoint of pb_dose: grad_dev[s] = scale * sum_v dobj_dose_dev[v] * K(v,s)
  * for every spot s, where K(v,s) is the dose per unit weight of spot s at
  * voxel v.  Matrix-free: footprints are recomputed.  grad_dev is

@@ -1,0 +1,31 @@
+"""Host-side logic of the autotuner (no GPU): size classes, candidate
+lists and the JSON cache."""
+import json
+
+
+def test_size_class_buckets():
+    from dosecuda_b200 import autotune
+    assert autotune.size_class(10485760, 15000, 4) == "V2^23_S2^14_B4"
+    assert autotune.size_class(1, 1, 1) == "V2^0_S2^0_B1"
+
+
+def test_variants_and_batch_candidates():
+    from dosecuda_b200 import autotune
+    names = autotune.variants()
+    assert len(names) >= 2 and names[0].startswith("t128")
+    cands = autotune.batch_candidates()
+    for v, bps in cands:
+        assert 0 <= v < len(names)
+        assert 2 <= bps <= (5 if autotune.threads_of(names[v]) == 128 else 3)
+
+
+def test_cache_roundtrip(tmp_path, monkeypatch):
+    from dosecuda_b200 import autotune
+    path = tmp_path / "c" / "tune.json"
+    monkeypatch.setenv("DOSECUDA_B200_TUNE_CACHE", str(path))
+    assert autotune.cache_path() == str(path)
+    autotune._store(str(path), "k1", [2, {"0": 1.5}])
+    autotune._store(str(path), "k2", [0, 3])
+    data = json.loads(path.read_text())
+    assert data["k1"][0] == 2 and data["k2"] == [0, 3]
+    assert autotune._load(str(tmp_path / "missing.json")) == {}
