@@ -307,9 +307,9 @@ _OBJ_WORK = {}
 
 
 def objective(dose: torch.Tensor, presc: torch.Tensor, weight: torch.Tensor,
-              resid: Optional[torch.Tensor] = None):
-    """FP64 sum_v w (D-P)^2 on the device (1-element float64 tensor) and,
-    if ``resid`` is given, 2 w (D-P) written into it."""
+              resid: Optional[torch.Tensor] = None, out: Optional[torch.Tensor] = None):
+    """FP64 sum_v w (D-P)^2 on the device (1-element float64 tensor, `out`
+    if given) and, if ``resid`` is given, 2 w (D-P) written into it."""
     dev = dose.device
     n = dose.numel()
     for t in (presc, weight):
@@ -319,7 +319,7 @@ def objective(dose: torch.Tensor, presc: torch.Tensor, weight: torch.Tensor,
     if work is None:
         work = torch.empty(int(_lib.lib.pb_objective_work_size()), dtype=torch.uint8, device=dev)
         _OBJ_WORK[dev] = work
-    obj = torch.empty(1, dtype=torch.float64, device=dev)
+    obj = out if out is not None else torch.empty(1, dtype=torch.float64, device=dev)
     check(_lib.lib.pb_objective(ptr(dose.contiguous()), ptr(presc.contiguous()),
                                 ptr(weight.contiguous()), n, ptr(obj), ptr(resid), ptr(work),
                                 _stream(dev)), "pb_objective")

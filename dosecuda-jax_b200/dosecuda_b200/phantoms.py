@@ -172,7 +172,7 @@ def heterogeneous(seed: int = 2, angles: Sequence[float] = (0.0, 120.0, 240.0),
                   n_spots: int = 8000, shape=(160, 256, 256), spacing: float = 2.0,
                   machine="HitachiProbeatJHU", n_slabs: int = 3, n_spheres: int = 6,
                   semi_range=(30.0, 45.0), centre_jitter: float = 20.0,
-                  body_inset: float = 30.0) -> SynthCase:
+                  body_inset: float = 30.0, pitch: float = 5.0) -> SynthCase:
     rng = np.random.default_rng(seed)
     nz, ny, nx = shape
     s = float(spacing)
@@ -216,9 +216,9 @@ def heterogeneous(seed: int = 2, angles: Sequence[float] = (0.0, 120.0, 240.0),
     # target ellipsoid, centre off the voxel lattice
     semi = rng.uniform(semi_range[0], semi_range[1], size=3)
     tc = rng.uniform(-centre_jitter, centre_jitter, size=3) + rng.uniform(0.1, 0.9, size=3) * s
-    Z, Y, X = np.meshgrid(cz, cy, cx, indexing="ij")
-    target = (((X - tc[0]) / semi[0]) ** 2 + ((Y - tc[1]) / semi[1]) ** 2 +
-              ((Z - tc[2]) / semi[2]) ** 2) <= 1.0
+    target = ((((cx - tc[0]) / semi[0]) ** 2)[None, None, :] +
+              (((cy - tc[1]) / semi[1]) ** 2)[None, :, None] +
+              (((cz - tc[2]) / semi[2]) ** 2)[:, None, None]) <= 1.0
     g.HU = hu
     rlsp = hu_to_rlsp_np(hu, machine)
 
@@ -235,7 +235,7 @@ def heterogeneous(seed: int = 2, angles: Sequence[float] = (0.0, 120.0, 240.0),
         h = to_head(tpts)
         proj = np.stack([h[:, 0] / (1.0 - h[:, 2] / model.VSADX),
                          h[:, 1] / (1.0 - h[:, 2] / model.VSADY)], axis=1)
-        lat = _lattice_over(proj[:: max(1, len(proj) // 20000)])
+        lat = _lattice_over(proj[:: max(1, len(proj) // 20000)], pitch=pitch)
         wet = _wet_samples(rlsp, g.origin, s, tc, src, sub)
         n_layers = max(1, int(round(per_beam / max(len(lat), 1))))
         ids = _pick_energies(model, wet.min() - 2.0, wet.max() + 3.0, n_layers)
@@ -264,8 +264,9 @@ def config_forward_heterogeneous(seed: int = 2) -> SynthCase:
 
 
 def config_gradient(seed: int = 3) -> SynthCase:
-    """4 beams, ~20,000 spots, with the quadratic objective's fields."""
-    return heterogeneous(seed, (0.0, 90.0, 180.0, 270.0), 20000)
+    """4 beams, ~20,000 spots (5 mm lattice over a target of 7-10 cm axes),
+    with the quadratic objective's fields."""
+    return heterogeneous(seed, (0.0, 90.0, 180.0, 270.0), 20000, semi_range=(35.0, 50.0))
 
 
 def small_heterogeneous(seed: int = 7, angles=(0.0, 135.0), n_spots=300,
@@ -299,3 +300,11 @@ def batch_cases(seed: int = 4, n_plans: int = 32, min_shape=(64, 64, 64),
         case.name = f"batch{p}_{shape[2]}x{shape[1]}x{shape[0]}_{s:g}mm_{nb}beams"
         out.append(case)
     return out
+
+
+def config_optimisation(seed: int = 5) -> SynthCase:
+    """512x512x200 at 1 mm, 4 beams, ~60,000 spots (3 mm lattice), with the objective's
+    fields: the large optimisation loop."""
+    return heterogeneous(seed, (0.0, 90.0, 180.0, 270.0), 75000, shape=(200, 512, 512),
+                         spacing=1.0, semi_range=(40.0, 60.0), centre_jitter=15.0,
+                         body_inset=40.0, pitch=3.0)
