@@ -103,43 +103,23 @@ class Clocks:
 
 
 def _dist():
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    from dosecuda_b200 import replicas
+    return replicas.init("nccl", timeout_s=120.0)
 
 
 def _barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from dosecuda_b200 import replicas
+    replicas.barrier(world)
 
 
 def _max_over_ranks(x: float, world: int, device) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from dosecuda_b200 import replicas
+    return replicas.max_over_ranks(x, world, device)
 
 
 def _sum_over_ranks(x: float, world: int, device) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from dosecuda_b200 import replicas
+    return replicas.sum_over_ranks(x, world, device)
 
 
 # ------------------------------------------------------------------ mine
@@ -590,10 +570,8 @@ def main():
         else:
             run_mine(args, world, rank, local)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-            dist.destroy_process_group()
+        from dosecuda_b200 import replicas
+        replicas.finish(world)
 
 
 if __name__ == "__main__":
