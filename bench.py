@@ -262,7 +262,9 @@ def run_mine(args, world, rank, local):
         "kernel_ms": kms,
         "e2e": {"value": E_all / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": 7 * args.steps,
+        # per step: HU->RLSP, [texture mode: five cell-record passes], ray trace,
+        # smoothing, pencil-beam sum, objective (two), adjoint
+        "gpu_launches": (12 if args.wet_mode == "texture" else 7) * args.steps,
         "roofline": {"kernel": "k_dose (forward pencil-beam sum)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": f"of {peak_kind}",

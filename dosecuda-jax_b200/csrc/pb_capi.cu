@@ -253,7 +253,7 @@ PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
     if (n_beams <= 0 || n_beams > PB_MAX_BEAMS)
         return set_error(PB_ERR_INVALID, "n_beams must be in [1, %d] (got %d)", PB_MAX_BEAMS,
                          n_beams);
-    return launch_wet(rlsp_dev, texture_object(tex), *grid, beams, n_beams, raw_work_dev, wet_dev,
+    return launch_wet(rlsp_dev, texture_object(tex), texture_cells(tex), *grid, beams, n_beams, raw_work_dev, wet_dev,
                       status_dev, static_cast<cudaStream_t>(stream));
 }
 
@@ -414,7 +414,7 @@ PbStatus pb_proton_raytrace_host(int gpu_id, double vsadx, double vsady, const f
         PB_TRY(texture_update(D.tex, d_rlsp, st));
     else
         PB_TRY(texture_create(d_rlsp, g, &D.tex, st));
-    PB_TRY(launch_wet(d_rlsp, texture_object(D.tex), g, &bg, 1, d_raw, d_wet, d_status, st));
+    PB_TRY(launch_wet(d_rlsp, texture_object(D.tex), texture_cells(D.tex), g, &bg, 1, d_raw, d_wet, d_status, st));
     int status = 0;
     PB_TRY(check_cuda(cudaMemcpyAsync(wet_out, d_wet, vb, cudaMemcpyDeviceToHost, st), "D2H wet"));
     PB_TRY(check_cuda(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st),
@@ -578,7 +578,8 @@ PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
         PbBeamGeom geoms[PB_MAX_BEAMS];
         for (int b = 0; b < P.n_beams; ++b) geoms[b] = P.beams[b].geom;
         bricks += fill_batch_wet(wet_items.data(), n_wet, P.grid, geoms, P.n_beams, P.rlsp_dev,
-                                 texture_object(P.tex), P.raw_work_dev, P.wet_dev, bricks);
+                                 texture_object(P.tex), texture_cells(P.tex), P.raw_work_dev,
+                                 P.wet_dev, bricks);
         n_wet += P.n_beams;
     }
     // dose records, most expensive tiles first (spots over all beams)

@@ -25,15 +25,15 @@ int ray_step_cap(const PbGrid &g);
 PbStatus launch_rlsp(const float *hu, int64_t n, const double *xh,
                      const double *yh, int m, float *out, cudaStream_t st);
 
-PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
-                    const PbBeamGeom *beams, int n_beams, float *raw, float *wet, int *status,
-                    cudaStream_t st);
+PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *rec,
+                    const PbGrid &g, const PbBeamGeom *beams, int n_beams, float *raw,
+                    float *wet, int *status, cudaStream_t st);
 
 // Batched WET pass (pb_wet.cu): one record per (plan, beam).
 size_t batch_wet_size();
 long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbBeamGeom *beams,
-                         int n_beams, const float *rlsp, cudaTextureObject_t tex, float *raw,
-                         float *wet, long long brick_start);
+                         int n_beams, const float *rlsp, cudaTextureObject_t tex,
+                         const float2 *rec, float *raw, float *wet, long long brick_start);
 PbStatus launch_wet_batch(const void *items_dev, int n_items, long long n_bricks, int *status,
                           cudaStream_t st);
 
@@ -41,6 +41,7 @@ PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaS
 PbStatus texture_update(uint64_t h, const float *rlsp, cudaStream_t st);
 bool texture_matches(uint64_t h, const PbGrid &g);
 cudaTextureObject_t texture_object(uint64_t h);
+const float2 *texture_cells(uint64_t h);
 void texture_destroy(uint64_t h);
 
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,

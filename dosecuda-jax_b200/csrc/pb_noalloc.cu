@@ -84,6 +84,6 @@ extern "C" PbStatus pb_wet_noalloc(const float *rlsp_dev, PbTexture tex, const P
     float *raw = nullptr;
     PbStatus s = noalloc_scratch(&raw);
     if (s != PB_OK) return s;
-    return launch_wet(rlsp_dev, texture_object(tex), *grid, beams, n_beams, raw, wet_dev,
-                      status_dev, static_cast<cudaStream_t>(stream));
+    return launch_wet(rlsp_dev, texture_object(tex), texture_cells(tex), *grid, beams, n_beams,
+                      raw, wet_dev, status_dev, static_cast<cudaStream_t>(stream));
 }

@@ -173,9 +173,33 @@ __device__ __forceinline__ float ray_sample(const float *__restrict__ rho,
 // reference's own.  TEX = false interpolates with exact FP32 trilinear
 // weights from global memory and forms the direction in FP64, the CPU
 // oracle's arithmetic.
+// Run of samples, starting with the one at (x, y, z), whose texture values
+// are certainly the flat value v of the current cell.  Every cell within
+// L-infinity distance r-1 of a flat cell with distance r is flat, with the
+// same value (face-adjacent flat cells share four texels).  Sample m of the
+// run lies within m*dmax texels of sample 0 on each axis, so its computed
+// cell (floor(x-0.5)+1) is within floor(m*dmax)+1 cells of the current one,
+// and the texture unit, which quantises the coordinate before taking the
+// floor, may read the cell next to that one: one more.  Hence samples with
+// m*dmax <= r-3 read only cells of value v, and a flat 2x2x2 neighbourhood
+// filters to exactly v.  Returns 0 where no run is certain.
+__device__ __forceinline__ int flat_run(const float2 *__restrict__ rec, const PbGrid &g,
+                                        float x, float y, float z, float dmax, float &v)
+{
+    const int i = __float2int_rd(x - 0.5f) + 1, j = __float2int_rd(y - 0.5f) + 1,
+              k = __float2int_rd(z - 0.5f) + 1;
+    const float2 r = __ldg(rec + i + (int64_t)(g.nx + 1) * (j + (int64_t)(g.ny + 1) * k));
+    v = r.x;
+    if (r.y < 3.0f) return 0;
+    return __float2int_rd((r.y - 3.0f) / dmax) + 1;
+}
+
+constexpr int kTexBurst = 4;   // texture samples taken per look at a non-flat record
+
 template <bool TEX>
 __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
-                                                cudaTextureObject_t tex, const PbGrid &g,
+                                                cudaTextureObject_t tex,
+                                                const float2 *__restrict__ rec, const PbGrid &g,
                                                 const PbBeamGeom &B, int i, int j, int k,
                                                 int cap, int *status)
 {
@@ -198,20 +222,52 @@ __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
     const int nsafe = safe_steps(g, B, inv_s, px, py, pz, ux, uy, uz, cap);
     double acc = 0.0;
     int n = 0;
-    for (; n + 8 <= nsafe; n += 8) {
-        float r[8];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const float t = (float)(n + m);
+    if (TEX && rec) {
+        // runs through flat regions, the texture unit elsewhere
+        const float dmax = fmaxf(fabsf(inv_s * ux), fmaxf(fabsf(inv_s * uy), fabsf(inv_s * uz))) +
+                           1e-6f;
+        while (n < nsafe) {
+            const float t = (float)n;
             const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
             const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
             const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
-            r[m] = ray_sample<TEX>(rho, tex, g, x, y, z);
+            float v;
+            int run = flat_run(rec, g, x, y, z, dmax, v);
+            if (run > 0) {
+                run = min(run, nsafe - n);
+                acc += (double)run * (double)fmaxf(v, 0.0f);
+                n += run;
+            } else {
+                // not flat here: the texture unit for the next few samples
+                // before looking at the records again
+                float part = fmaxf(tex3D<float>(tex, x, y, z), 0.0f);
+                const int e = min(n + kTexBurst, nsafe);
+                for (++n; n < e; ++n) {
+                    const float t = (float)n;
+                    const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
+                    const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
+                    const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
+                    part += fmaxf(tex3D<float>(tex, x, y, z), 0.0f);
+                }
+                acc += (double)part;
+            }
         }
-        float part = 0.0f;
+    } else {
+        for (; n + 8 <= nsafe; n += 8) {
+            float r[8];
 #pragma unroll
-        for (int m = 0; m < 8; ++m) part += fmaxf(r[m], 0.0f);
-        acc += (double)part;
+            for (int m = 0; m < 8; ++m) {
+                const float t = (float)(n + m);
+                const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
+                const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
+                const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
+                r[m] = ray_sample<TEX>(rho, tex, g, x, y, z);
+            }
+            float part = 0.0f;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) part += fmaxf(r[m], 0.0f);
+            acc += (double)part;
+        }
     }
     float part = 0.0f;
     for (;; ++n) {
@@ -234,9 +290,9 @@ __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
 
 template <bool TEX>
 __global__ void __launch_bounds__(128)
-k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
-           const __grid_constant__ BeamGeomSet bs, int zbricks, int cap,
-           float *__restrict__ raw, int *status)
+k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex,
+           const float2 *__restrict__ rec, PbGrid g, const __grid_constant__ BeamGeomSet bs,
+           int zbricks, int cap, float *__restrict__ raw, int *status)
 {
     const int b = blockIdx.z / zbricks;
     const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
@@ -245,7 +301,7 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex, PbGrid g,
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
-    raw[b * V + v] = raytrace_voxel<TEX>(rho, tex, g, bs.b[b], i, j, k, cap, status);
+    raw[b * V + v] = raytrace_voxel<TEX>(rho, tex, rec, g, bs.b[b], i, j, k, cap, status);
 }
 
 // Linear map of the smoothing samples in index space, per beam: head ->
@@ -400,6 +456,7 @@ struct BatchWet {
     PbBeamGeom geom;
     const float *rlsp;
     cudaTextureObject_t tex;
+    const float2 *rec;          // the texture's cell records (or null)
     float *raw;                 // this beam's unsmoothed WET (V)
     float *wet;                 // this beam's smoothed WET (V)
     double rot[9];
@@ -443,9 +500,9 @@ k_raytrace_batch(const BatchWet *__restrict__ items, int n_items, int *status)
     const BatchWet &W = items[find_wet_item(items, n_items, blockIdx.x)];
     int i, j, k;
     if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
-    const float r = W.tex
-                        ? raytrace_voxel<true>(W.rlsp, W.tex, W.g, W.geom, i, j, k, W.cap, status)
-                        : raytrace_voxel<false>(W.rlsp, 0, W.g, W.geom, i, j, k, W.cap, status);
+    const float r =
+        W.tex ? raytrace_voxel<true>(W.rlsp, W.tex, W.rec, W.g, W.geom, i, j, k, W.cap, status)
+              : raytrace_voxel<false>(W.rlsp, 0, nullptr, W.g, W.geom, i, j, k, W.cap, status);
     W.raw[i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k)] = r;
 }
 
@@ -466,9 +523,9 @@ int ray_step_cap(const PbGrid &g)
     return (int)ceil(diag) + 2;
 }
 
-PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
-                    const PbBeamGeom *beams, int n_beams, float *raw, float *wet, int *status,
-                    cudaStream_t st)
+PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *rec,
+                    const PbGrid &g, const PbBeamGeom *beams, int n_beams, float *raw,
+                    float *wet, int *status, cudaStream_t st)
 {
     BeamGeomSet bs;
     for (int b = 0; b < n_beams; ++b) bs.b[b] = beams[b];
@@ -480,11 +537,11 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const PbGrid &g,
     dim3 block(8, 4, 4);
     dim3 grid((g.nx + 7) / 8, (g.ny + 3) / 4, zb * n_beams);
     if (tex)
-        k_raytrace<true><<<grid, block, 0, st>>>(rlsp, tex, g, bs, zb, ray_step_cap(g), raw,
-                                                 status);
+        k_raytrace<true><<<grid, block, 0, st>>>(rlsp, tex, rec, g, bs, zb, ray_step_cap(g),
+                                                 raw, status);
     else
-        k_raytrace<false><<<grid, block, 0, st>>>(rlsp, tex, g, bs, zb, ray_step_cap(g), raw,
-                                                  status);
+        k_raytrace<false><<<grid, block, 0, st>>>(rlsp, tex, nullptr, g, bs, zb,
+                                                  ray_step_cap(g), raw, status);
     PbStatus s = check_launch("k_raytrace");
     if (s != PB_OK) return s;
     k_smooth<<<grid, block, 0, st>>>(raw, g, bs, d, ss, zb, wet);
@@ -495,8 +552,8 @@ size_t batch_wet_size() { return sizeof(BatchWet); }
 
 // Fills the batch records of one plan's beams; returns the bricks they use.
 long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbBeamGeom *beams,
-                         int n_beams, const float *rlsp, cudaTextureObject_t tex, float *raw,
-                         float *wet, long long brick_start)
+                         int n_beams, const float *rlsp, cudaTextureObject_t tex,
+                         const float2 *rec, float *raw, float *wet, long long brick_start)
 {
     BatchWet *W = static_cast<BatchWet *>(items_host) + first;
     SmoothDirs d;
@@ -512,6 +569,7 @@ long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbB
         w.geom = beams[b];
         w.rlsp = rlsp;
         w.tex = tex;
+        w.rec = rec;
         w.raw = raw + b * V;
         w.wet = wet + b * V;
         for (int m = 0; m < 9; ++m) w.rot[m] = ss.rot[b][m];
@@ -543,33 +601,151 @@ PbStatus launch_wet_batch(const void *items_dev, int n_items, long long n_bricks
     return check_launch("k_smooth_batch");
 }
 
+// Cells of a volume with border 0: cell (ci, cj, ck) holds the 2x2x2
+// texels with base (ci-1, cj-1, ck-1) -- the texels a linear fetch reads
+// for a coordinate inside it.  A cell is flat when its eight texels are
+// equal.  Two adjacent flat cells share texels, so a connected flat region
+// has one value.
+constexpr int kRunCap = 15;   // largest stored distance (cells)
+
+// Pass 0: flat cells -> their value, else NaN; 1-D distance along x to the
+// nearest non-flat cell (cells outside the cell grid count as non-flat),
+// capped at kRunCap.
+__global__ void __launch_bounds__(256)
+k_cell_flat(const float *__restrict__ rho, PbGrid g, float *__restrict__ value)
+{
+    const int cx = g.nx + 1, cy = g.ny + 1, cz = g.nz + 1;
+    const int64_t n = (int64_t)cx * cy * cz;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int ci = (int)(c % cx);
+        const int cj = (int)((c / cx) % cy);
+        const int ck = (int)(c / ((int64_t)cx * cy));
+        float v0 = 0.0f;
+        bool flat = true;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int i = ci - 1 + (t & 1), j = cj - 1 + ((t >> 1) & 1), k = ck - 1 + (t >> 2);
+            const bool in = i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz;
+            const float v = in ? __ldg(rho + i + (int64_t)g.nx * (j + (int64_t)g.ny * k)) : 0.0f;
+            if (t == 0) v0 = v;
+            else flat &= (v == v0);
+        }
+        value[c] = (flat && v0 == v0) ? v0 : __int_as_float(0x7fc00000);
+    }
+}
+
+// Separable L-infinity distance to the nearest non-flat cell, capped at
+// kRunCap: axis 0 starts from the flat flags, axes 1 and 2 combine the
+// previous pass with max(|offset|, d).
+template <int AXIS>
+__global__ void __launch_bounds__(256)
+k_cell_dist(PbGrid g, const float *__restrict__ value, const unsigned char *__restrict__ din,
+            unsigned char *__restrict__ dout)
+{
+    const int cx = g.nx + 1, cy = g.ny + 1, cz = g.nz + 1;
+    const int64_t n = (int64_t)cx * cy * cz;
+    const int len = AXIS == 0 ? cx : (AXIS == 1 ? cy : cz);
+    const int64_t stride = AXIS == 0 ? 1 : (AXIS == 1 ? (int64_t)cx : (int64_t)cx * cy);
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int pos = AXIS == 0 ? (int)(c % cx)
+                                  : (AXIS == 1 ? (int)((c / cx) % cy) : (int)(c / ((int64_t)cx * cy)));
+        int best = kRunCap;
+        for (int k = -kRunCap; k <= kRunCap; ++k) {
+            const int q = pos + k;
+            const int ak = k < 0 ? -k : k;
+            if (ak >= best) continue;
+            int d;
+            if (q < 0 || q >= len) {
+                d = 0;
+            } else if (AXIS == 0) {
+                const float v = __ldg(value + c + k);
+                d = (v == v) ? kRunCap : 0;
+            } else {
+                d = __ldg(din + c + k * stride);
+            }
+            const int m = ak > d ? ak : d;
+            if (m < best) best = m;
+        }
+        dout[c] = (unsigned char)best;
+    }
+}
+
+// Record per cell: (value, distance); distance 0 for non-flat cells.
+__global__ void __launch_bounds__(256)
+k_cell_records(PbGrid g, const float *__restrict__ value, const unsigned char *__restrict__ dist,
+               float2 *__restrict__ rec)
+{
+    const int64_t n = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const float v = value[c];
+        rec[c] = make_float2(v == v ? v : 0.0f, v == v ? (float)dist[c] : 0.0f);
+    }
+}
+
 // 3-D texture over an RLSP volume: float channel, linear filter, border 0,
-// unnormalised coordinates (TextureClasses.cu:14-41).
+// unnormalised coordinates (TextureClasses.cu:14-41), and the cell records
+// the ray trace uses to take runs of samples in flat regions at once.
 struct RlspTexture {
     cudaArray_t arr = nullptr;
     cudaTextureObject_t tex = 0;
+    float2 *rec = nullptr;            // (nx+1)(ny+1)(nz+1) cell records
+    float *value = nullptr;           // work: flat values
+    unsigned char *d0 = nullptr, *d1 = nullptr;  // work: distance passes
     int nx = 0, ny = 0, nz = 0;
 };
 
+static PbStatus texture_fill(RlspTexture *t, const float *rlsp, cudaStream_t st)
+{
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<float *>(rlsp), sizeof(float) * (size_t)t->nx, t->nx,
+                                   t->ny);
+    p.dstArray = t->arr;
+    p.extent = make_cudaExtent(t->nx, t->ny, t->nz);
+    p.kind = cudaMemcpyDeviceToDevice;
+    PbStatus s = check_cuda(cudaMemcpy3DAsync(&p, st), "cudaMemcpy3DAsync");
+    if (s != PB_OK) return s;
+    const PbGrid g{t->nx, t->ny, t->nz, 1.0f};
+    const int blocks = 148 * 8;
+    k_cell_flat<<<blocks, 256, 0, st>>>(rlsp, g, t->value);
+    k_cell_dist<0><<<blocks, 256, 0, st>>>(g, t->value, nullptr, t->d0);
+    k_cell_dist<1><<<blocks, 256, 0, st>>>(g, t->value, t->d0, t->d1);
+    k_cell_dist<2><<<blocks, 256, 0, st>>>(g, t->value, t->d1, t->d0);
+    k_cell_records<<<blocks, 256, 0, st>>>(g, t->value, t->d0, t->rec);
+    return check_launch("cell records");
+}
+
+static void texture_free(RlspTexture *t)
+{
+    if (t->tex) cudaDestroyTextureObject(t->tex);
+    if (t->arr) cudaFreeArray(t->arr);
+    cudaFree(t->rec);
+    cudaFree(t->value);
+    cudaFree(t->d0);
+    cudaFree(t->d1);
+    delete t;
+}
+
 PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st)
 {
+    const size_t ncell = (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+    if (ncell > (size_t)INT32_MAX)
+        return set_error(PB_ERR_INVALID, "grid too large for a texture (%zu cells)", ncell);
     RlspTexture *t = new (std::nothrow) RlspTexture;
     if (!t) return set_error(PB_ERR_NOMEM, "host allocation failed");
+    t->nx = g.nx;
+    t->ny = g.ny;
+    t->nz = g.nz;
     cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
     cudaExtent ext = make_cudaExtent(g.nx, g.ny, g.nz);
     PbStatus s = check_cuda(cudaMalloc3DArray(&t->arr, &ch, ext, cudaArrayDefault),
                             "cudaMalloc3DArray");
-    if (s != PB_OK) {
-        delete t;
-        return s;
-    }
-    cudaMemcpy3DParms p{};
-    p.srcPtr = make_cudaPitchedPtr(const_cast<float *>(rlsp), sizeof(float) * (size_t)g.nx, g.nx,
-                                   g.ny);
-    p.dstArray = t->arr;
-    p.extent = ext;
-    p.kind = cudaMemcpyDeviceToDevice;
-    s = check_cuda(cudaMemcpy3DAsync(&p, st), "cudaMemcpy3DAsync");
+    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->rec, sizeof(float2) * ncell), "cudaMalloc");
+    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->value, sizeof(float) * ncell), "cudaMalloc");
+    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d0, ncell), "cudaMalloc");
+    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d1, ncell), "cudaMalloc");
     if (s == PB_OK) {
         cudaResourceDesc rd{};
         rd.resType = cudaResourceTypeArray;
@@ -582,28 +758,18 @@ PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaS
         s = check_cuda(cudaCreateTextureObject(&t->tex, &rd, &td, nullptr),
                        "cudaCreateTextureObject");
     }
+    if (s == PB_OK) s = texture_fill(t, rlsp, st);
     if (s != PB_OK) {
-        cudaFreeArray(t->arr);
-        delete t;
+        texture_free(t);
         return s;
     }
-    t->nx = g.nx;
-    t->ny = g.ny;
-    t->nz = g.nz;
     *out = reinterpret_cast<uint64_t>(t);
     return PB_OK;
 }
 
 PbStatus texture_update(uint64_t h, const float *rlsp, cudaStream_t st)
 {
-    RlspTexture *t = reinterpret_cast<RlspTexture *>(h);
-    cudaMemcpy3DParms p{};
-    p.srcPtr = make_cudaPitchedPtr(const_cast<float *>(rlsp), sizeof(float) * (size_t)t->nx, t->nx,
-                                   t->ny);
-    p.dstArray = t->arr;
-    p.extent = make_cudaExtent(t->nx, t->ny, t->nz);
-    p.kind = cudaMemcpyDeviceToDevice;
-    return check_cuda(cudaMemcpy3DAsync(&p, st), "cudaMemcpy3DAsync");
+    return texture_fill(reinterpret_cast<RlspTexture *>(h), rlsp, st);
 }
 
 bool texture_matches(uint64_t h, const PbGrid &g)
@@ -617,13 +783,15 @@ cudaTextureObject_t texture_object(uint64_t h)
     return h ? reinterpret_cast<const RlspTexture *>(h)->tex : 0;
 }
 
+const float2 *texture_cells(uint64_t h)
+{
+    return h ? reinterpret_cast<const RlspTexture *>(h)->rec : nullptr;
+}
+
 void texture_destroy(uint64_t h)
 {
     RlspTexture *t = reinterpret_cast<RlspTexture *>(h);
-    if (!t) return;
-    cudaDestroyTextureObject(t->tex);
-    cudaFreeArray(t->arr);
-    delete t;
+    if (t) texture_free(t);
 }
 
 }  // namespace pb
