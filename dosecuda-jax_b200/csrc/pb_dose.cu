@@ -87,21 +87,58 @@ __device__ __forceinline__ float2 axis_r2(float2 nx, float2 ny, float2 tx, float
     return __fmul2_rn(S, it2);
 }
 
+// Per-layer constants of the Gaussian parameters (uniform over a block).
+struct LayerK {
+    float r80, off;          // R80, 0.7 R80
+    float ca, cb, cc;        // sigma_air = A d^2 + B d + C
+    float d0, inv_step;      // depth table: first depth, 1 / (second - first)
+    float c_log, c_sh;       // 0.0014 R80, 0.22 R80
+    float k_wh, c_wh;        // 1 / (11.2 - 0.023 R80), 0.35 (0.0017 R80^2 - R80)
+    float r3sq, c_lin;       // (R80 + 3)^2, 1.61e-9 (R80 + 3)^2
+};
+
+__device__ __forceinline__ LayerK layer_consts(float r80, const float *cabc, const float *s_dep,
+                                               int lut_len)
+{
+    LayerK K;
+    K.r80 = r80;
+    K.off = 0.7f * r80;
+    K.ca = __ldg(cabc);
+    K.cb = __ldg(cabc + 1);
+    K.cc = __ldg(cabc + 2);
+    K.d0 = s_dep[0];
+    const float step = lut_len > 1 ? s_dep[1] - s_dep[0] : 0.0f;
+    K.inv_step = step > 0.0f ? 1.0f / step : 0.0f;
+    K.c_log = 0.0014f * r80;
+    K.c_sh = 0.22f * r80;
+    K.k_wh = 1.0f / (11.2f - 0.023f * r80);
+    K.c_wh = 0.35f * (0.0017f * r80 * r80 - r80);
+    const float r3 = r80 + 3.0f;
+    K.r3sq = r3 * r3;
+    K.c_lin = 1.61e-9f * K.r3sq;
+    return K;
+}
+
 // Per-(voxel, layer) Gaussian parameters.  wet_mm is 10*WET (cm), dist the
 // distance to the source (mm).  Exponent scales are pre-multiplied by
 // log2(e) for ex2.
-__device__ __forceinline__ void layer_params(float wet_mm, float dist, float r80,
+//
+// The LUT row is the first depth >= wet_mm (lowerBound,
+// CudaClasses.cuh:130-144): guessed from the first depth and the first step
+// (exact for the uniform 1 mm tables of the beam models), then moved until
+// it is that row, so any ascending depth table gives the binary search's
+// row.  The halo closed forms (IMPTClasses.cu:104-121) and the Gaussian
+// prefactors use the SFU's log2 and reciprocal (relative error ~1e-7).
+__device__ __forceinline__ void layer_params(float wet_mm, float dist, const LayerK &K,
                                              const float *s_dep, const float *s_sig,
-                                             const float *s_idd, int lut_len,
-                                             float ca, float cb, float cc,
-                                             float &pf, float &hf, float &ps2,
-                                             float &hs2)
+                                             const float *s_idd, int lut_len, float &pf,
+                                             float &hf, float &ps2, float &hs2)
 {
-    int lo = 0, hi = lut_len;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (wet_mm <= s_dep[mid]) hi = mid; else lo = mid + 1;
-    }
+    const float gs = ceilf((wet_mm - K.d0) * K.inv_step);
+    int lo = gs > 0.0f ? (gs < (float)lut_len ? (int)gs : lut_len) : 0;
+    if (wet_mm != wet_mm) lo = lut_len;   // NaN compares false: the search ends high
+    while (lo > 0 && s_dep[lo - 1] >= wet_mm) --lo;
+    while (lo < lut_len && s_dep[lo] < wet_mm) ++lo;
     float idd, sms;
     if (lo == lut_len) {
         idd = s_idd[lo - 1];
@@ -110,34 +147,33 @@ __device__ __forceinline__ void layer_params(float wet_mm, float dist, float r80
         idd = s_idd[0];
         sms = s_sig[0];
     } else {
-        const float f = (wet_mm - s_dep[lo - 1]) / (s_dep[lo] - s_dep[lo - 1]);
+        const float f = __fdividef(wet_mm - s_dep[lo - 1], s_dep[lo] - s_dep[lo - 1]);
         idd = fmaf(s_idd[lo] - s_idd[lo - 1], f, s_idd[lo - 1]);
         sms = fmaf(s_sig[lo] - s_sig[lo - 1], f, s_sig[lo - 1]);
     }
-    const float d = dist - wet_mm + 0.7f * r80;
-    const float st = fmaf(fmaf(ca, d, cb), d, cc) + sms;
-    const float w = fminf(fmaxf(wet_mm, 0.1f), r80 - 0.1f);
-    const float a1 = w - r80 - 5.0f;
-    float sh = 2.85f + 0.0014f * r80 * logf(w + 3.0f) + 0.06f * w - 7.4e-5f * w * w -
-               (0.22f * r80) / (a1 * a1);
-    const float r3 = r80 + 3.0f;
-    float wh = 0.052f * logf(1.13f + w / (11.2f - 0.023f * r80)) +
-               0.35f * (0.0017f * r80 * r80 - r80) / (r3 * r3 - w * w) -
-               1.61e-9f * w * r3 * r3;
+    const float d = dist - wet_mm + K.off;
+    const float st = fmaf(fmaf(K.ca, d, K.cb), d, K.cc) + sms;
+    const float w = fminf(fmaxf(wet_mm, 0.1f), K.r80 - 0.1f);
+    const float a1 = w - K.r80 - 5.0f;
+    float sh = 2.85f + K.c_log * __logf(w + 3.0f) + 0.06f * w - 7.4e-5f * w * w -
+               __fdividef(K.c_sh, a1 * a1);
+    float wh = 0.052f * __logf(fmaf(w, K.k_wh, 1.13f)) +
+               __fdividef(K.c_wh, K.r3sq - w * w) - K.c_lin * w;
     sh = fmaxf(sh, 0.0f);
     wh = fminf(fmaxf(wh, 0.0f), 0.9f);
     const float st2 = st * st;
     const float sht2 = fmaf(sh, sh, st2);
-    pf = (1.0f - wh) * idd / (kTwoPi * st2);
-    hf = wh * idd / (kTwoPi * sht2);
-    ps2 = st2 != 0.0f ? (-0.5f * kLog2e) / st2 : -INFINITY;
-    hs2 = sht2 != 0.0f ? (-0.5f * kLog2e) / sht2 : -INFINITY;
+    const float rp = __fdividef(1.0f, st2), rh = __fdividef(1.0f, sht2);
+    const float iddn = idd * (1.0f / kTwoPi);
+    pf = (1.0f - wh) * iddn * rp;
+    hf = wh * iddn * rh;
+    ps2 = st2 != 0.0f ? (-0.5f * kLog2e) * rp : -INFINITY;
+    hs2 = sht2 != 0.0f ? (-0.5f * kLog2e) * rh : -INFINITY;
 }
 
-// True unless every voxel of the tile is further than the cull radius from
-// the spot's axis.  nhs = smallest |hs2| among the tile's active voxels.
-__device__ __forceinline__ bool cull_keep(float xs, float ys, float it2,
-                                          const TileBounds &tb, float nhs)
+// Squared distance (times 1/|t|^2) from the spot's axis to the tile's BEV
+// box, a lower bound over the tile's voxels of the axis_r2 value.
+__device__ __forceinline__ float cull_r2(float xs, float ys, float it2, const TileBounds &tb)
 {
     const float p0 = xs * tb.gx0, p1 = xs * tb.gx1;
     const float lox = tb.x0 - fmaxf(p0, p1), hix = tb.x1 - fminf(p0, p1);
@@ -145,8 +181,18 @@ __device__ __forceinline__ bool cull_keep(float xs, float ys, float it2,
     const float q0 = ys * tb.gy0, q1 = ys * tb.gy1;
     const float loy = tb.y0 - fmaxf(q0, q1), hiy = tb.y1 - fminf(q0, q1);
     const float dy = fmaxf(0.0f, fmaxf(loy, -hiy));
-    const float e = (dx * dx + dy * dy) * it2 * nhs;
-    return !(e >= kCullLog2);
+    return (dx * dx + dy * dy) * it2;
+}
+
+// Spot classes per tile and layer: the halo term is below 2^-24 of its
+// peak at every voxel of the tile (0, skipped); only the primary term is
+// (1, halo only); neither (2, both terms).  nhs / nps are the smallest
+// |hs2| / |ps2| among the tile's active voxels (the widest halo and primary
+// Gaussians); the halo is never narrower than the primary, so nps >= nhs.
+__device__ __forceinline__ int cull_class(float e, float nhs, float nps)
+{
+    if (e * nhs >= kCullLog2) return 0;
+    return (e * nps >= kCullLog2) ? 1 : 2;
 }
 
 __device__ __forceinline__ void neumaier(float &s, float &c, float x)
@@ -160,7 +206,7 @@ __device__ __forceinline__ void neumaier(float &s, float &c, float x)
 template <int NV, int NT>
 __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y,
                                                   const float *GX, const float *GY,
-                                                  const bool *valid, float (*s_red)[9])
+                                                  const bool *valid, float (*s_red)[10])
 {
     constexpr int kWarps = NT / 32;
     float v[8] = {INFINITY, -INFINITY, INFINITY, -INFINITY,
@@ -195,17 +241,26 @@ __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y
     return tb;
 }
 
+// Block-wide maxima of two values (slots 8 and 9 of s_red).
 template <int NT>
-__device__ __forceinline__ float block_max_slot8(float v, float (*s_red)[9])
+__device__ __forceinline__ void block_max2(float a, float b, float (*s_red)[10], float &ra,
+                                           float &rb)
 {
     constexpr int kWarps = NT / 32;
-    v = warp_max(v);
+    a = warp_max(a);
+    b = warp_max(b);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) s_red[warp][8] = v;
+    if (lane == 0) {
+        s_red[warp][8] = a;
+        s_red[warp][9] = b;
+    }
     __syncthreads();
-    float r = s_red[0][8];
-    for (int w = 1; w < kWarps; ++w) r = fmaxf(r, s_red[w][8]);
-    return r;
+    ra = s_red[0][8];
+    rb = s_red[0][9];
+    for (int w = 1; w < kWarps; ++w) {
+        ra = fmaxf(ra, s_red[w][8]);
+        rb = fmaxf(rb, s_red[w][9]);
+    }
 }
 
 // Voxels of this block's tile owned by this thread: (li, lj, lk + step*q),
@@ -274,8 +329,9 @@ template <int NT, int KCULL>
 struct DoseShared {
     float dep[PB_MAX_LUT_LEN], sig[PB_MAX_LUT_LEN], idd[PB_MAX_LUT_LEN];
     SpotRec spot[NT * KCULL];
-    float red[NT / 32][9];
+    float red[NT / 32][10];
     int wcount[KCULL][NT / 32];
+    int wcount_h[KCULL][NT / 32];
 };
 
 // Forward dose of one 8x8x8 tile of one plan by one block of NT threads,
@@ -298,8 +354,9 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
     constexpr int kWarps = kThreads / 32;
     float *s_dep = sh.dep, *s_sig = sh.sig, *s_idd = sh.idd;
     SpotRec *s_spot = sh.spot;
-    float (*s_red)[9] = sh.red;
+    float (*s_red)[10] = sh.red;
     int (*s_wcount)[kWarps] = sh.wcount;
+    int (*s_wcount_h)[kWarps] = sh.wcount_h;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int vidx[kVpt];
@@ -362,11 +419,11 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
             if (!__syncthreads_or(any)) continue;
             stage_lut<kThreads>(B, L.energy_id, s_dep, s_sig, s_idd);
             __syncthreads();
-            const float *cabc = B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2;
-            const float ca = __ldg(cabc), cb = __ldg(cabc + 1), cc = __ldg(cabc + 2);
+            const LayerK K = layer_consts(
+                L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, s_dep, B.lut_len);
             float pf[kVpt], hf[kVpt];
             float2 PS[NP], HS[NP];
-            float hmax = -INFINITY;
+            float hmax = -INFINITY, pmax = -INFINITY;
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
                 float ps2 = 0.0f, hs2 = 0.0f;
@@ -378,9 +435,10 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                     const float gx = (q & 1) ? GXP[p].y : GXP[p].x;
                     const float w = (q & 1) ? WP[p].y : WP[p].x;
                     const float Z = B.geom.vsadx * (1.0f - gx);
-                    layer_params(w, source_distance(B, X, Y, Z), L.r80, s_dep, s_sig, s_idd,
-                                 B.lut_len, ca, cb, cc, pf[q], hf[q], ps2, hs2);
+                    layer_params(w, source_distance(B, X, Y, Z), K, s_dep, s_sig, s_idd,
+                                 B.lut_len, pf[q], hf[q], ps2, hs2);
                     hmax = fmaxf(hmax, hs2);
+                    pmax = fmaxf(pmax, ps2);
                 }
                 if (q & 1) {
                     PS[q >> 1].y = ps2;
@@ -390,50 +448,65 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                     HS[q >> 1].x = hs2;
                 }
             }
-            const float nhs = -block_max_slot8<kThreads>(hmax, s_red);
+            float nhs, nps;
+            block_max2<kThreads>(hmax, pmax, s_red, nhs, nps);
+            nhs = -nhs;
+            nps = -nps;
             float2 AP[NP], AH[NP];
 #pragma unroll
             for (int p = 0; p < NP; ++p) AP[p] = AH[p] = make_float2(0.0f, 0.0f);
 
+            // Spots with both terms are compacted to the front of s_spot,
+            // halo-only spots to the back.
+            constexpr int kCap = kThreads * kCull;
             const int s0 = B.spot_start + L.spot_start;
-            for (int base = 0; base < L.n_spots; base += kThreads * kCull) {
-                bool keep[kCull];
+            for (int base = 0; base < L.n_spots; base += kCap) {
+                int cls[kCull];
                 float4 ga[kCull], gb[kCull];
-                unsigned m[kCull];
+                unsigned m2[kCull], m1[kCull];
 #pragma unroll
                 for (int c = 0; c < kCull; ++c) {
                     const int si = base + c * kThreads + threadIdx.x;
-                    keep[c] = false;
+                    cls[c] = 0;
                     if (si < L.n_spots) {
                         ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
                         gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                        keep[c] = cull_keep(ga[c].x, ga[c].y, gb[c].y, tb, nhs);
+                        cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, gb[c].y, tb), nhs, nps);
                     }
-                    m[c] = __ballot_sync(0xffffffffu, keep[c]);
-                    if (lane == 0) s_wcount[c][warp] = __popc(m[c]);
+                    m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
+                    m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
+                    if (lane == 0) {
+                        s_wcount[c][warp] = __popc(m2[c]);
+                        s_wcount_h[c][warp] = __popc(m1[c]);
+                    }
                 }
                 __syncthreads();
-                int total = 0;
+                int n2 = 0, n1 = 0;
+                const unsigned below = (1u << lane) - 1u;
 #pragma unroll
                 for (int c = 0; c < kCull; ++c) {
-                    int pos = 0;
+                    int pos2 = 0, pos1 = 0;
                     for (int w = 0; w < kWarps; ++w) {
-                        if (w == warp) pos = total + __popc(m[c] & ((1u << lane) - 1u));
-                        total += s_wcount[c][w];
+                        if (w == warp) {
+                            pos2 = n2 + __popc(m2[c] & below);
+                            pos1 = n1 + __popc(m1[c] & below);
+                        }
+                        n2 += s_wcount[c][w];
+                        n1 += s_wcount_h[c][w];
                     }
-                    if (keep[c]) {
+                    if (cls[c]) {
                         const float w = __ldg(mu + s0 + base + c * kThreads + threadIdx.x);
                         SpotRec r;
                         r.a = make_float4(-ga[c].x, -ga[c].x, -ga[c].y, -ga[c].y);
                         r.b = make_float4(ga[c].z, ga[c].z, -ga[c].w, -ga[c].w);
                         r.c = make_float4(-gb[c].x, -gb[c].x, gb[c].y, gb[c].y);
                         r.d = make_float4(w, w, 0.0f, 0.0f);
-                        s_spot[pos] = r;
+                        s_spot[cls[c] == 2 ? pos2 : kCap - 1 - pos1] = r;
                     }
                 }
                 __syncthreads();
 #pragma unroll 2
-                for (int c = 0; c < total; ++c) {
+                for (int c = 0; c < n2; ++c) {
                     const SpotRec r = s_spot[c];
                     const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
                                  ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
@@ -442,6 +515,18 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                         const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
                                                   GXP[p], GYP[p]);
                         AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS[p], qq)), AP[p]);
+                        AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
+                    }
+                }
+#pragma unroll 2
+                for (int c = kCap - n1; c < kCap; ++c) {
+                    const SpotRec r = s_spot[c];
+                    const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
+                                 ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
+                                                  GXP[p], GYP[p]);
                         AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
                     }
                 }
@@ -538,8 +623,9 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
     __shared__ VoxRec s_vox[kAdjThreads * kAdjVpt];
     __shared__ int s_cand[kAdjThreads * kSpt];
     __shared__ float s_gsum[kAdjThreads * kSpt];
-    __shared__ float s_red[kWarps][9];
+    __shared__ float s_red[kWarps][10];
     __shared__ int s_wcount[kAdjVpt > kSpt ? kAdjVpt : kSpt][kWarps];
+    __shared__ int s_wcount_h[kSpt][kWarps];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int vi[kAdjVpt], vj[kAdjVpt], vk[kAdjVpt];
@@ -602,16 +688,17 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                     nact += s_wcount[q][w];
                 }
             }
-            const float *cabc = B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2;
-            const float ca = __ldg(cabc), cb = __ldg(cabc + 1), cc = __ldg(cabc + 2);
-            float hmax = -INFINITY;
+            const LayerK K = layer_consts(
+                L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, s_dep, B.lut_len);
+            float hmax = -INFINITY, pmax = -INFINITY;
 #pragma unroll
             for (int q = 0; q < kAdjVpt; ++q) {
                 if (act[q]) {
                     float pf, hf, ps2, hs2;
-                    layer_params(WMM[q], source_distance(B, X[q], Y[q], Z[q]), L.r80, s_dep,
-                                 s_sig, s_idd, B.lut_len, ca, cb, cc, pf, hf, ps2, hs2);
+                    layer_params(WMM[q], source_distance(B, X[q], Y[q], Z[q]), K, s_dep, s_sig,
+                                 s_idd, B.lut_len, pf, hf, ps2, hs2);
                     hmax = fmaxf(hmax, hs2);
+                    pmax = fmaxf(pmax, ps2);
                     VoxRec r;
                     r.xy = make_float4(X[q], X[q], Y[q], Y[q]);
                     r.g = make_float4(GX[q], GX[q], GY[q], GY[q]);
@@ -622,72 +709,108 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                 }
             }
             // includes the barrier that publishes s_vox and frees s_wcount
-            const float nhs = -block_max_slot8<kAdjThreads>(hmax, s_red);
+            float nhs, nps;
+            block_max2<kAdjThreads>(hmax, pmax, s_red, nhs, nps);
+            nhs = -nhs;
+            nps = -nps;
 
+            // Candidates: spots with both terms first (n2), then halo-only
+            // spots (n1); cull_class as in the forward.
             const int s0 = B.spot_start + L.spot_start;
             for (int base = 0; base < L.n_spots; base += kAdjThreads * kSpt) {
-                bool keep[kSpt];
-                unsigned m[kSpt];
+                int cls[kSpt];
+                unsigned m2[kSpt], m1[kSpt];
 #pragma unroll
                 for (int c = 0; c < kSpt; ++c) {
                     const int si = base + c * kAdjThreads + threadIdx.x;
-                    keep[c] = false;
+                    cls[c] = 0;
                     if (si < L.n_spots) {
                         const float4 ga = __ldg(geo + 2 * (int64_t)(s0 + si));
                         const float4 gb = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                        keep[c] = cull_keep(ga.x, ga.y, gb.y, tb, nhs);
+                        cls[c] = cull_class(cull_r2(ga.x, ga.y, gb.y, tb), nhs, nps);
                     }
-                    m[c] = __ballot_sync(0xffffffffu, keep[c]);
-                    if (lane == 0) s_wcount[c][warp] = __popc(m[c]);
+                    m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
+                    m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
+                    if (lane == 0) {
+                        s_wcount[c][warp] = __popc(m2[c]);
+                        s_wcount_h[c][warp] = __popc(m1[c]);
+                    }
                 }
                 __syncthreads();
-                int total = 0;
+                int n2 = 0;
+#pragma unroll
+                for (int c = 0; c < kSpt; ++c)
+                    for (int w = 0; w < kWarps; ++w) n2 += s_wcount[c][w];
+                int c2 = 0, c1 = n2;
+                const unsigned below = (1u << lane) - 1u;
 #pragma unroll
                 for (int c = 0; c < kSpt; ++c) {
-                    int pos = 0;
+                    int pos2 = 0, pos1 = 0;
                     for (int w = 0; w < kWarps; ++w) {
-                        if (w == warp) pos = total + __popc(m[c] & ((1u << lane) - 1u));
-                        total += s_wcount[c][w];
-                    }
-                    if (keep[c]) s_cand[pos] = s0 + base + c * kAdjThreads + threadIdx.x;
-                }
-                __syncthreads();
-                // Work items (spot pair, voxel stripe): every thread busy even
-                // when few spots survive the culling.  Partial sums meet in
-                // shared memory, then one atomic per spot goes to global.
-                const int npair = (total + 1) >> 1;
-                const int stripes = npair >= kAdjThreads ? 1 : kAdjThreads / npair;
-                const int items = npair * stripes;
-                for (int it = threadIdx.x; it < items; it += kAdjThreads) {
-                    const int sp = it % npair, vs = it / npair;
-                    float2 nx, ny, tx, nty, ncs, it2;
-                    float4 ga[2], gb[2];
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int c = 2 * sp + h;
-                        ga[h] = make_float4(0.f, 0.f, 0.f, 0.f);
-                        gb[h] = make_float4(0.f, 1.f, 0.f, 0.f);
-                        if (c < total) {
-                            ga[h] = __ldg(geo + 2 * (int64_t)s_cand[c]);
-                            gb[h] = __ldg(geo + 2 * (int64_t)s_cand[c] + 1);
+                        if (w == warp) {
+                            pos2 = c2 + __popc(m2[c] & below);
+                            pos1 = c1 + __popc(m1[c] & below);
                         }
+                        c2 += s_wcount[c][w];
+                        c1 += s_wcount_h[c][w];
                     }
-                    nx = make_float2(-ga[0].x, -ga[1].x);
-                    ny = make_float2(-ga[0].y, -ga[1].y);
-                    tx = make_float2(ga[0].z, ga[1].z);
-                    nty = make_float2(-ga[0].w, -ga[1].w);
-                    ncs = make_float2(-gb[0].x, -gb[1].x);
-                    it2 = make_float2(gb[0].y, gb[1].y);
-                    float2 acc = make_float2(0.0f, 0.0f);
-                    for (int c = vs; c < nact; c += stripes) {
-                        const VoxRec v = s_vox[c];
-                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
-                                                  hi2(v.xy), lo2(v.g), hi2(v.g));
-                        acc = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qq)), acc);
-                        acc = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qq)), acc);
+                    if (cls[c])
+                        s_cand[cls[c] == 2 ? pos2 : pos1] = s0 + base + c * kAdjThreads + threadIdx.x;
+                }
+                const int total = c1;
+                __syncthreads();
+                // Two passes, both-term spots then halo-only spots, each over
+                // work items (spot pair, voxel stripe) so that every thread is
+                // busy even when few spots survive the culling (an odd spot
+                // is paired with an empty slot).  Partial sums meet in shared
+                // memory, then one atomic per spot goes to global.
+#pragma unroll 1
+                for (int pass = 0; pass < 2; ++pass) {
+                    const int first = pass ? n2 : 0, cnt = pass ? total - n2 : n2;
+                    const int npair = (cnt + 1) >> 1;
+                    if (npair == 0) continue;
+                    const int stripes = npair >= kAdjThreads ? 1 : kAdjThreads / npair;
+                    const int items = npair * stripes;
+                    for (int it = threadIdx.x; it < items; it += kAdjThreads) {
+                        const int sp = it % npair, vs = it / npair;
+                        float4 ga[2], gb[2];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int c = 2 * sp + h;
+                            ga[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+                            gb[h] = make_float4(0.f, 1.f, 0.f, 0.f);
+                            if (c < cnt) {
+                                ga[h] = __ldg(geo + 2 * (int64_t)s_cand[first + c]);
+                                gb[h] = __ldg(geo + 2 * (int64_t)s_cand[first + c] + 1);
+                            }
+                        }
+                        const float2 nx = make_float2(-ga[0].x, -ga[1].x);
+                        const float2 ny = make_float2(-ga[0].y, -ga[1].y);
+                        const float2 tx = make_float2(ga[0].z, ga[1].z);
+                        const float2 nty = make_float2(-ga[0].w, -ga[1].w);
+                        const float2 ncs = make_float2(-gb[0].x, -gb[1].x);
+                        const float2 it2 = make_float2(gb[0].y, gb[1].y);
+                        float2 acc = make_float2(0.0f, 0.0f);
+                        if (pass == 0) {
+                            for (int c = vs; c < nact; c += stripes) {
+                                const VoxRec v = s_vox[c];
+                                const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
+                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
+                                acc = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qq)), acc);
+                                acc = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qq)), acc);
+                            }
+                        } else {
+                            for (int c = vs; c < nact; c += stripes) {
+                                const VoxRec v = s_vox[c];
+                                const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
+                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
+                                acc = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qq)), acc);
+                            }
+                        }
+                        if (acc.x != 0.0f) atomicAdd(&s_gsum[first + 2 * sp], acc.x);
+                        if (acc.y != 0.0f && 2 * sp + 1 < cnt)
+                            atomicAdd(&s_gsum[first + 2 * sp + 1], acc.y);
                     }
-                    if (acc.x != 0.0f) atomicAdd(&s_gsum[2 * sp], acc.x);
-                    if (acc.y != 0.0f && 2 * sp + 1 < total) atomicAdd(&s_gsum[2 * sp + 1], acc.y);
                 }
                 __syncthreads();
                 for (int c = threadIdx.x; c < total; c += kAdjThreads) {

@@ -142,7 +142,10 @@ def test_texture_mode_matches_reference(pkg, small, cube, curve, reference_modul
         bd = dp.forward(beam_doses=True)[1].cpu().numpy().reshape(dp.n_beams, *g.HU.shape)
         rw, rd = _reference_plan(reference_module, case, curve)
         for b in range(dp.n_beams):
-            assert np.quantile(np.abs(wet[b] - rw[b]), 0.999) <= 1e-4
+            # the reference sums its samples in FP32, this path in FP64: on
+            # these short rays they differ by < 7e-5 cm everywhere; a sample
+            # taken from a wrong cell would show as >= 1e-2 cm
+            assert np.abs(wet[b] - rw[b]).max() <= 1e-4
             assert max_rel(bd[b], rd[b]) <= 1e-3
 
 
