@@ -40,6 +40,7 @@ constexpr int kAdjThreads = 256;    // adjoint block
 constexpr int kAdjVpt = 2;          // adjoint: voxels per thread (z, z+4)
 constexpr int kSpt = 2;             // adjoint: spots culled per thread per chunk
 constexpr float kCullLog2 = 24.0f;  // skip factors below 2^-24
+constexpr int kAdjDynSmem = 64 * kAdjThreads * kAdjVpt;   // the adjoint's voxel records
 
 struct PlanArgs {
     PbGrid g;
@@ -65,6 +66,8 @@ struct __align__(16) VoxRec {
     float4 s;    // (ps2, ps2, hs2, hs2)
     float4 f;    // (w*Pf, w*Pf, w*Hf, w*Hf)
 };
+
+static_assert(sizeof(VoxRec) == 64, "voxel record size");
 
 struct TileBounds {
     float x0, x1, y0, y1, gx0, gx1, gy0, gy1;
@@ -620,9 +623,17 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 {
     __shared__ float s_dep[PB_MAX_LUT_LEN], s_sig[PB_MAX_LUT_LEN], s_idd[PB_MAX_LUT_LEN];
     constexpr int kWarps = kAdjThreads / 32;
-    __shared__ VoxRec s_vox[kAdjThreads * kAdjVpt];
-    __shared__ int s_cand[kAdjThreads * kSpt];
-    __shared__ float s_gsum[kAdjThreads * kSpt];
+    extern __shared__ __align__(16) unsigned char s_dyn[];   // kAdjDynSmem bytes
+    VoxRec *s_vox = reinterpret_cast<VoxRec *>(s_dyn);       // kAdjThreads * kAdjVpt
+    // Candidate spots of one compaction round: index, gradient partial and
+    // the geometry terms of axis_r2 (negated where axis_r2 wants them so),
+    // one array per term so that a spot pair is one float2 load each.  The
+    // halo-only class starts at an even slot; the slot between the classes
+    // (odd n2) is padding.
+    constexpr int kCand = kAdjThreads * kSpt + 2;
+    __shared__ int s_cand[kCand];
+    __shared__ float s_gsum[kCand];
+    __shared__ __align__(8) float s_cg[6][kCand];
     __shared__ float s_red[kWarps][10];
     __shared__ int s_wcount[kAdjVpt > kSpt ? kAdjVpt : kSpt][kWarps];
     __shared__ int s_wcount_h[kSpt][kWarps];
@@ -641,7 +652,10 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
         anyw |= (wv[q] != 0.0f);
     }
     if (!__syncthreads_or(anyw)) return;
-    for (int c = threadIdx.x; c < kAdjThreads * kSpt; c += kAdjThreads) s_gsum[c] = 0.0f;
+    for (int c = threadIdx.x; c < kCand; c += kAdjThreads) {
+        s_gsum[c] = 0.0f;
+        for (int t = 0; t < 6; ++t) s_cg[t][c] = 0.0f;   // padding slots stay finite
+    }
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
@@ -720,14 +734,15 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
             for (int base = 0; base < L.n_spots; base += kAdjThreads * kSpt) {
                 int cls[kSpt];
                 unsigned m2[kSpt], m1[kSpt];
+                float4 ga[kSpt], gb[kSpt];
 #pragma unroll
                 for (int c = 0; c < kSpt; ++c) {
                     const int si = base + c * kAdjThreads + threadIdx.x;
                     cls[c] = 0;
                     if (si < L.n_spots) {
-                        const float4 ga = __ldg(geo + 2 * (int64_t)(s0 + si));
-                        const float4 gb = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                        cls[c] = cull_class(cull_r2(ga.x, ga.y, gb.y, tb), nhs, nps);
+                        ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
+                        gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
+                        cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, gb[c].y, tb), nhs, nps);
                     }
                     m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
                     m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
@@ -741,7 +756,8 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 #pragma unroll
                 for (int c = 0; c < kSpt; ++c)
                     for (int w = 0; w < kWarps; ++w) n2 += s_wcount[c][w];
-                int c2 = 0, c1 = n2;
+                const int f1 = (n2 + 1) & ~1;   // first halo-only slot
+                int c2 = 0, c1 = f1;
                 const unsigned below = (1u << lane) - 1u;
 #pragma unroll
                 for (int c = 0; c < kSpt; ++c) {
@@ -754,10 +770,18 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                         c2 += s_wcount[c][w];
                         c1 += s_wcount_h[c][w];
                     }
-                    if (cls[c])
-                        s_cand[cls[c] == 2 ? pos2 : pos1] = s0 + base + c * kAdjThreads + threadIdx.x;
+                    if (cls[c]) {
+                        const int at = cls[c] == 2 ? pos2 : pos1;
+                        s_cand[at] = s0 + base + c * kAdjThreads + threadIdx.x;
+                        s_cg[0][at] = -ga[c].x;
+                        s_cg[1][at] = -ga[c].y;
+                        s_cg[2][at] = ga[c].z;
+                        s_cg[3][at] = -ga[c].w;
+                        s_cg[4][at] = -gb[c].x;
+                        s_cg[5][at] = gb[c].y;
+                    }
                 }
-                const int total = c1;
+                const int total = c1;   // slots used, padding included
                 __syncthreads();
                 // Two passes, both-term spots then halo-only spots, each over
                 // work items (spot pair, voxel stripe) so that every thread is
@@ -766,56 +790,73 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                 // memory, then one atomic per spot goes to global.
 #pragma unroll 1
                 for (int pass = 0; pass < 2; ++pass) {
-                    const int first = pass ? n2 : 0, cnt = pass ? total - n2 : n2;
+                    const int first = pass ? f1 : 0, cnt = pass ? total - f1 : n2;
                     const int npair = (cnt + 1) >> 1;
                     if (npair == 0) continue;
                     const int stripes = npair >= kAdjThreads ? 1 : kAdjThreads / npair;
                     const int items = npair * stripes;
                     for (int it = threadIdx.x; it < items; it += kAdjThreads) {
                         const int sp = it % npair, vs = it / npair;
-                        float4 ga[2], gb[2];
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int c = 2 * sp + h;
-                            ga[h] = make_float4(0.f, 0.f, 0.f, 0.f);
-                            gb[h] = make_float4(0.f, 1.f, 0.f, 0.f);
-                            if (c < cnt) {
-                                ga[h] = __ldg(geo + 2 * (int64_t)s_cand[first + c]);
-                                gb[h] = __ldg(geo + 2 * (int64_t)s_cand[first + c] + 1);
-                            }
-                        }
-                        const float2 nx = make_float2(-ga[0].x, -ga[1].x);
-                        const float2 ny = make_float2(-ga[0].y, -ga[1].y);
-                        const float2 tx = make_float2(ga[0].z, ga[1].z);
-                        const float2 nty = make_float2(-ga[0].w, -ga[1].w);
-                        const float2 ncs = make_float2(-gb[0].x, -gb[1].x);
-                        const float2 it2 = make_float2(gb[0].y, gb[1].y);
-                        float2 acc = make_float2(0.0f, 0.0f);
+                        // a pair's second slot may be padding or the next
+                        // class's first spot: finite either way, and its sum
+                        // is dropped below
+                        const int c0 = first + 2 * sp;
+                        const float2 nx = *reinterpret_cast<const float2 *>(&s_cg[0][c0]);
+                        const float2 ny = *reinterpret_cast<const float2 *>(&s_cg[1][c0]);
+                        const float2 tx = *reinterpret_cast<const float2 *>(&s_cg[2][c0]);
+                        const float2 nty = *reinterpret_cast<const float2 *>(&s_cg[3][c0]);
+                        const float2 ncs = *reinterpret_cast<const float2 *>(&s_cg[4][c0]);
+                        const float2 it2 = *reinterpret_cast<const float2 *>(&s_cg[5][c0]);
+                        float2 acc0 = make_float2(0.0f, 0.0f), acc1 = acc0;
+                        int c = vs;
                         if (pass == 0) {
-                            for (int c = vs; c < nact; c += stripes) {
-                                const VoxRec v = s_vox[c];
-                                const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
+                            float2 accp0 = acc0, accp1 = acc0;
+                            for (; c + stripes < nact; c += 2 * stripes) {
+                                const VoxRec v = s_vox[c], u = s_vox[c + stripes];
+                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
                                                           hi2(v.xy), lo2(v.g), hi2(v.g));
-                                acc = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qq)), acc);
-                                acc = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qq)), acc);
+                                const float2 qu = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(u.xy),
+                                                          hi2(u.xy), lo2(u.g), hi2(u.g));
+                                accp0 = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qv)), accp0);
+                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
+                                accp1 = __ffma2_rn(lo2(u.f), ex2x2(__fmul2_rn(lo2(u.s), qu)), accp1);
+                                acc1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), qu)), acc1);
                             }
-                        } else {
-                            for (int c = vs; c < nact; c += stripes) {
+                            if (c < nact) {
                                 const VoxRec v = s_vox[c];
-                                const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
+                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
                                                           hi2(v.xy), lo2(v.g), hi2(v.g));
-                                acc = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qq)), acc);
+                                accp0 = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qv)), accp0);
+                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
+                            }
+                            acc0 = __fadd2_rn(acc0, accp0);
+                            acc1 = __fadd2_rn(acc1, accp1);
+                        } else {
+                            for (; c + stripes < nact; c += 2 * stripes) {
+                                const VoxRec v = s_vox[c], u = s_vox[c + stripes];
+                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
+                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
+                                const float2 qu = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(u.xy),
+                                                          hi2(u.xy), lo2(u.g), hi2(u.g));
+                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
+                                acc1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), qu)), acc1);
+                            }
+                            if (c < nact) {
+                                const VoxRec v = s_vox[c];
+                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
+                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
+                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
                             }
                         }
-                        if (acc.x != 0.0f) atomicAdd(&s_gsum[first + 2 * sp], acc.x);
-                        if (acc.y != 0.0f && 2 * sp + 1 < cnt)
-                            atomicAdd(&s_gsum[first + 2 * sp + 1], acc.y);
+                        const float2 acc = __fadd2_rn(acc0, acc1);
+                        if (acc.x != 0.0f) atomicAdd(&s_gsum[c0], acc.x);
+                        if (acc.y != 0.0f && 2 * sp + 1 < cnt) atomicAdd(&s_gsum[c0 + 1], acc.y);
                     }
                 }
                 __syncthreads();
                 for (int c = threadIdx.x; c < total; c += kAdjThreads) {
                     const float a = s_gsum[c];
-                    if (a != 0.0f) atomicAdd(grad + s_cand[c], a);
+                    if (a != 0.0f) atomicAdd(grad + s_cand[c], a);   // padding stays 0
                     s_gsum[c] = 0.0f;
                 }
                 __syncthreads();
@@ -1014,7 +1055,13 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                             "cudaMemsetAsync(grad)");
     if (s != PB_OK) return s;
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
-    k_adjoint<<<(unsigned)tiles, kAdjThreads, 0, st>>>(A, wet, layers,
+    // the voxel records are dynamic shared memory: with the static arrays
+    // they exceed the 48 KB a launch gets without opting in
+    s = check_cuda(cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kAdjDynSmem),
+                   "cudaFuncSetAttribute(k_adjoint)");
+    if (s != PB_OK) return s;
+    k_adjoint<<<(unsigned)tiles, kAdjThreads, kAdjDynSmem, st>>>(A, wet, layers,
                                                     reinterpret_cast<const float4 *>(geo), w,
                                                     grad);
     return check_launch("k_adjoint");
