@@ -173,6 +173,18 @@ __device__ __forceinline__ float ray_sample(const float *__restrict__ rho,
 // reference's own.  TEX = false interpolates with exact FP32 trilinear
 // weights from global memory and forms the direction in FP64, the CPU
 // oracle's arithmetic.
+// floor(a) for -2^22 <= a < 2^22 on the FP32 adder: adding 1.5 * 2^23 with
+// rounding toward -infinity leaves floor(a) in the low mantissa bits.
+__device__ __forceinline__ int floor_small(float a)
+{
+    return __float_as_int(__fadd_rd(a, 12582912.0f)) - 0x4B400000;
+}
+
+__device__ __forceinline__ float floor_small_f(float a)
+{
+    return __fsub_rn(__fadd_rd(a, 12582912.0f), 12582912.0f);
+}
+
 // Run of samples, starting with the one at (x, y, z), whose texture values
 // are certainly the flat value v of the current cell.  Every cell within
 // L-infinity distance r-1 of a flat cell with distance r is flat, with the
@@ -183,15 +195,17 @@ __device__ __forceinline__ float ray_sample(const float *__restrict__ rho,
 // floor, may read the cell next to that one: one more.  Hence samples with
 // m*dmax <= r-3 read only cells of value v, and a flat 2x2x2 neighbourhood
 // filters to exactly v.  Returns 0 where no run is certain.
-__device__ __forceinline__ int flat_run(const float2 *__restrict__ rec, const PbGrid &g,
-                                        float x, float y, float z, float dmax, float &v)
+__device__ __forceinline__ float flat_run(const float2 *__restrict__ rec, int cx, int cy,
+                                          float x, float y, float z, float inv_dmax, float &v)
 {
-    const int i = __float2int_rd(x - 0.5f) + 1, j = __float2int_rd(y - 0.5f) + 1,
-              k = __float2int_rd(z - 0.5f) + 1;
-    const float2 r = __ldg(rec + i + (int64_t)(g.nx + 1) * (j + (int64_t)(g.ny + 1) * k));
+    const int i = floor_small(__fsub_rn(x, 0.5f)) + 1, j = floor_small(__fsub_rn(y, 0.5f)) + 1,
+              k = floor_small(__fsub_rn(z, 0.5f)) + 1;
+    const float2 r = __ldg(rec + i + cx * (j + cy * k));
     v = r.x;
-    if (r.y < 3.0f) return 0;
-    return __float2int_rd((r.y - 3.0f) / dmax) + 1;
+    if (r.y < 3.0f) return 0.0f;
+    // floor((r - 3) / dmax) + 1, every rounding downward so that the run
+    // never exceeds the bound
+    return floor_small_f(__fmul_rd(r.y - 3.0f, inv_dmax)) + 1.0f;
 }
 
 constexpr int kTexBurst = 4;   // texture samples taken per look at a non-flat record
@@ -223,27 +237,30 @@ __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
     double acc = 0.0;
     int n = 0;
     if (TEX && rec) {
-        // runs through flat regions, the texture unit elsewhere
+        // runs through flat regions, the texture unit elsewhere; the sample
+        // counter is kept in FP32 (exact below 2^24)
         const float dmax = fmaxf(fabsf(inv_s * ux), fmaxf(fabsf(inv_s * uy), fabsf(inv_s * uz))) +
                            1e-6f;
-        while (n < nsafe) {
-            const float t = (float)n;
+        const float inv_dmax = __frcp_rd(dmax);
+        const float nsf = (float)nsafe;
+        const int cx = g.nx + 1, cy = g.ny + 1;
+        float t = 0.0f;
+        while (t < nsf) {
             const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
             const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
             const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
             float v;
-            int run = flat_run(rec, g, x, y, z, dmax, v);
-            if (run > 0) {
-                run = min(run, nsafe - n);
-                acc += (double)run * (double)fmaxf(v, 0.0f);
-                n += run;
+            const float run = flat_run(rec, cx, cy, x, y, z, inv_dmax, v);
+            if (run > 0.0f) {
+                const float m = fminf(run, nsf - t);
+                acc += (double)(m * fmaxf(v, 0.0f));
+                t += m;
             } else {
                 // not flat here: the texture unit for the next few samples
                 // before looking at the records again
                 float part = fmaxf(tex3D<float>(tex, x, y, z), 0.0f);
-                const int e = min(n + kTexBurst, nsafe);
-                for (++n; n < e; ++n) {
-                    const float t = (float)n;
+                const float e = fminf(t + (float)kTexBurst, nsf);
+                for (t += 1.0f; t < e; t += 1.0f) {
                     const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
                     const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
                     const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
@@ -252,6 +269,7 @@ __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
                 acc += (double)part;
             }
         }
+        n = (int)t;
     } else {
         for (; n + 8 <= nsafe; n += 8) {
             float r[8];
@@ -417,6 +435,39 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
         (float)((M[3] * dhx + M[4] * dhy + M[5] * dhz + (double)B.iso[1]) * inv_s_d);
     const float m0z =
         (float)((M[6] * dhx + M[7] * dhy + M[8] * dhz + (double)B.iso[2]) * inv_s_d);
+    // Interior voxels: every sample index (within 9*|dm| + 1 of m0, the
+    // reference-order path within one more) lies inside the grid, so the
+    // bounds tests and the sample count are dropped and the radii run to a
+    // precomputed count: the radii 1..9 with dr < lim.
+    float ex = 0.0f, ey = 0.0f, ez = 0.0f;
+#pragma unroll
+    for (int dd = 0; dd < 6; ++dd) {
+        ex = fmaxf(ex, fabsf(dm[dd][0]));
+        ey = fmaxf(ey, fabsf(dm[dd][1]));
+        ez = fmaxf(ez, fabsf(dm[dd][2]));
+    }
+    ex = fmaf(9.0f, ex, 2.0f);
+    ey = fmaf(9.0f, ey, 2.0f);
+    ez = fmaf(9.0f, ez, 2.0f);
+    if (m0x >= ex && m0x <= (float)(g.nx - 1) - ex && m0y >= ey &&
+        m0y <= (float)(g.ny - 1) - ey && m0z >= ez && m0z <= (float)(g.nz - 1) - ez &&
+        (int64_t)g.nx * g.ny * g.nz < ((int64_t)1 << 31)) {
+        const float nrf = lim > 9.0f ? 9.0f : __fsub_rn(ceilf(lim), 1.0f);
+        const int sy = g.nx, sz = g.nx * g.ny;
+        for (int dd = 0; dd < 6; ++dd) {
+            const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
+            for (float dr = 1.0f; dr <= nrf; dr = __fadd_rn(dr, 1.0f)) {
+                bool near = false;
+                int ii = round_fadd(fmaf(dr, dmx, m0x), tie, near);
+                int jj = round_fadd(fmaf(dr, dmy, m0y), tie, near);
+                int kk = round_fadd(fmaf(dr, dmz, m0z), tie, near);
+                if (near)
+                    exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], ii, jj, kk);
+                sum += __ldg(R + (ii + sy * jj + sz * kk));
+            }
+        }
+        return __fdiv_rn(sum, __fadd_rn(__fmul_rn(6.0f, nrf), 1.0f));
+    }
     for (int dd = 0; dd < 6; ++dd) {
         const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
         for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f)) {
