@@ -175,6 +175,9 @@ PbStatus pb_build_layers(const float *spot_list, int n_spots, const float *dvp, 
         L.energy_id = e;
         L.r80 = dvp[(size_t)dvp_len * e + 1];
         L.energy = dvp[(size_t)dvp_len * e];
+        L.sx0 = L.sx1 = L.sy0 = L.sy1 = 0.0f;   // culling bounds: see pb_layer_bounds
+        L.sh_max = L.mcs_max = 0.0f;
+        L.bound_ok = 0;
         start += cnt;
     }
     *n_layers_out = nl;
@@ -307,6 +310,28 @@ PbStatus pb_count_pairs(const PbGrid *grid, const PbBeam *beams, int n_beams,
     if (!count_dev) return set_error(PB_ERR_INVALID, "count is NULL");
     return launch_count_pairs(*grid, beams, n_beams, wet_dev, layers_dev, count_dev,
                               static_cast<cudaStream_t>(stream));
+}
+
+PbStatus pb_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers_dev,
+                         const float *spot_geo_dev, void *stream)
+{
+    if (!beams || n_beams <= 0 || n_beams > PB_MAX_BEAMS)
+        return set_error(PB_ERR_INVALID, "n_beams must be in [1, %d] (got %d)", PB_MAX_BEAMS,
+                         n_beams);
+    for (int b = 0; b < n_beams; ++b) {
+        const PbBeam &B = beams[b];
+        if (B.n_layers < 0 || B.layer_start < 0 || B.spot_start < 0 || B.n_spots < 0)
+            return set_error(PB_ERR_INVALID, "beam %d: negative layer/spot range", b);
+        if (B.n_layers == 0) continue;
+        if (!layers_dev || !spot_geo_dev)
+            return set_error(PB_ERR_INVALID, "layers/spot geometry is NULL");
+        if (!B.sigmas_dev) return set_error(PB_ERR_INVALID, "beam %d: model table is NULL", b);
+        if (B.lut_len <= 0 || B.lut_len > PB_MAX_LUT_LEN)
+            return set_error(PB_ERR_INVALID, "beam %d: lut_len must be in [1, %d] (got %d)", b,
+                             PB_MAX_LUT_LEN, B.lut_len);
+    }
+    return launch_layer_bounds(beams, n_beams, layers_dev, spot_geo_dev,
+                               static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"
@@ -500,6 +525,8 @@ PbStatus pb_proton_spot_host(int gpu_id, double vsadx, double vsady, const float
         B.n_energies = n_energies;
         B.lut_len = lut_len;
         B.dvp_len = dvp_len;
+        PB_TRY(launch_layer_bounds(&B, 1, static_cast<PbLayer *>(D.buf[kBufLayers].p),
+                                   static_cast<const float *>(D.buf[kBufGeo].p), st));
         PB_TRY(launch_dose(g, &B, 1, static_cast<const float *>(D.buf[kBufWet].p),
                            static_cast<const PbLayer *>(D.buf[kBufLayers].p),
                            static_cast<const float *>(D.buf[kBufGeo].p),

@@ -70,8 +70,12 @@ struct __align__(16) VoxRec {
 static_assert(sizeof(VoxRec) == 64, "voxel record size");
 
 struct TileBounds {
-    float x0, x1, y0, y1, gx0, gx1, gy0, gy1;
+    float x0, x1, y0, y1, gx0, gx1, gy0, gy1;  // BEV box and divergence factors
+    float d0, d1, w0;                          // source distance range, least 10*WET
 };
+
+// Slots of the per-warp reduction array: 11 for tile_bounds, 2 for block_max2.
+constexpr int kRedSlots = 13;
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 lo2(const float4 &v) { return make_float2(v.x, v.y); }
@@ -206,14 +210,18 @@ __device__ __forceinline__ void neumaier(float &s, float &c, float x)
 }
 
 // Block-wide min/max of the tile's BEV box over valid voxels.
+// Block-wide box of the tile's valid voxels: BEV x, y and divergence
+// factors (min and max), distance to the source (min and max), 10*WET (min).
 template <int NV, int NT>
 __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y,
                                                   const float *GX, const float *GY,
-                                                  const bool *valid, float (*s_red)[10])
+                                                  const float *D, const float *W,
+                                                  const bool *valid,
+                                                  float (*s_red)[kRedSlots])
 {
     constexpr int kWarps = NT / 32;
-    float v[8] = {INFINITY, -INFINITY, INFINITY, -INFINITY,
-                  INFINITY, -INFINITY, INFINITY, -INFINITY};
+    float v[11] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
+                   INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY};
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
         if (!valid[q]) continue;
@@ -221,49 +229,98 @@ __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y
         v[2] = fminf(v[2], Y[q]);  v[3] = fmaxf(v[3], Y[q]);
         v[4] = fminf(v[4], GX[q]); v[5] = fmaxf(v[5], GX[q]);
         v[6] = fminf(v[6], GY[q]); v[7] = fmaxf(v[7], GY[q]);
+        v[8] = fminf(v[8], D[q]);  v[9] = fmaxf(v[9], D[q]);
+        v[10] = fminf(v[10], W[q]);
     }
+    // slot m: odd = max, even = min
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
+    for (int m = 0; m < 11; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
 #pragma unroll
-        for (int m = 0; m < 8; ++m) s_red[warp][m] = v[m];
+        for (int m = 0; m < 11; ++m) s_red[warp][m] = v[m];
     }
     __syncthreads();
-    float r[8];
+    float r[11];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) r[m] = s_red[0][m];
+    for (int m = 0; m < 11; ++m) r[m] = s_red[0][m];
     for (int w = 1; w < kWarps; ++w) {
 #pragma unroll
-        for (int m = 0; m < 8; ++m)
+        for (int m = 0; m < 11; ++m)
             r[m] = (m & 1) ? fmaxf(r[m], s_red[w][m]) : fminf(r[m], s_red[w][m]);
     }
     TileBounds tb;
     tb.x0 = r[0]; tb.x1 = r[1]; tb.y0 = r[2]; tb.y1 = r[3];
     tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
+    tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10];
     return tb;
 }
 
-// Block-wide maxima of two values (slots 8 and 9 of s_red).
+// Block-wide maxima of two values (slots 11 and 12 of s_red).
 template <int NT>
-__device__ __forceinline__ void block_max2(float a, float b, float (*s_red)[10], float &ra,
-                                           float &rb)
+__device__ __forceinline__ void block_max2(float a, float b, float (*s_red)[kRedSlots],
+                                           float &ra, float &rb)
 {
     constexpr int kWarps = NT / 32;
     a = warp_max(a);
     b = warp_max(b);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
-        s_red[warp][8] = a;
-        s_red[warp][9] = b;
+        s_red[warp][11] = a;
+        s_red[warp][12] = b;
     }
     __syncthreads();
-    ra = s_red[0][8];
-    rb = s_red[0][9];
+    ra = s_red[0][11];
+    rb = s_red[0][12];
     for (int w = 1; w < kWarps; ++w) {
-        ra = fmaxf(ra, s_red[w][8]);
-        rb = fmaxf(rb, s_red[w][9]);
+        ra = fmaxf(ra, s_red[w][11]);
+        rb = fmaxf(rb, s_red[w][12]);
     }
+}
+
+// True when no spot of layer L can pass cull_class at any voxel of the
+// tile, judged from the layer's bounds alone (before any per-voxel work).
+// A spot's cull value is (dx^2 + dy^2) * it2 * nhs; here dx, dy are taken
+// to the box of all the layer's spot axes at the tile's depths (FP32
+// products are monotone, so each spot's own dx, dy are no smaller), it2 to
+// its least value over that box, and nhs to 0.5 log2(e) / sigma^2 with
+// sigma bounding every active voxel's total halo sigma:
+//   sigma^2 <= sh_max^2 + (max |A d^2 + B d + C| + mcs_max)^2
+// over d = dist - wet_mm + 0.7 R80, dist in the tile's range and wet_mm in
+// [the tile's least 10*WET, 1.1 R80].  Margins (1 % on sigma^2, 0.1 % on
+// it2) cover the kernels' FP32 and SFU arithmetic, so a skipped layer is
+// one whose every spot the per-spot cull would drop: the dose is the same.
+__device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &tb,
+                                           const PbBeam &B, float cut)
+{
+    if (!L.bound_ok) return false;
+    const float a0 = L.sx0 * tb.gx0, a1 = L.sx0 * tb.gx1, a2 = L.sx1 * tb.gx0,
+                a3 = L.sx1 * tb.gx1;
+    const float b0 = L.sy0 * tb.gy0, b1 = L.sy0 * tb.gy1, b2 = L.sy1 * tb.gy0,
+                b3 = L.sy1 * tb.gy1;
+    const float pxl = fminf(fminf(a0, a1), fminf(a2, a3)), pxh = fmaxf(fmaxf(a0, a1), fmaxf(a2, a3));
+    const float pyl = fminf(fminf(b0, b1), fminf(b2, b3)), pyh = fmaxf(fmaxf(b0, b1), fmaxf(b2, b3));
+    const float dx = fmaxf(0.0f, fmaxf(tb.x0 - pxh, pxl - tb.x1));
+    const float dy = fmaxf(0.0f, fmaxf(tb.y0 - pyh, pyl - tb.y1));
+    const float r2 = dx * dx + dy * dy;
+    if (!(r2 > 0.0f)) return false;
+    const float mx = fmaxf(L.sx0 * L.sx0, L.sx1 * L.sx1) / (B.geom.vsadx * B.geom.vsadx);
+    const float my = fmaxf(L.sy0 * L.sy0, L.sy1 * L.sy1) / (B.geom.vsady * B.geom.vsady);
+    const float it2 = 0.999f / (1.0f + mx + my);
+    const float *cabc = B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2;
+    const float ca = __ldg(cabc), cb = __ldg(cabc + 1), cc = __ldg(cabc + 2);
+    const float off = 0.7f * L.r80;
+    const float dlo = tb.d0 - cut + off, dhi = tb.d1 - tb.w0 + off;
+    if (!(dlo <= dhi)) return false;   // NaN or an empty tile: no decision
+    float q = fmaxf(fabsf(fmaf(fmaf(ca, dlo, cb), dlo, cc)), fabsf(fmaf(fmaf(ca, dhi, cb), dhi, cc)));
+    if (ca != 0.0f) {
+        const float dv = -cb / (2.0f * ca);
+        if (dv > dlo && dv < dhi) q = fmaxf(q, fabsf(fmaf(fmaf(ca, dv, cb), dv, cc)));
+    }
+    const float st = q + L.mcs_max;
+    const float sig2 = fmaf(L.sh_max, L.sh_max, st * st) * 1.01f + 1e-2f;
+    const float e = r2 * it2 * ((0.5f * kLog2e) / sig2);
+    return e >= kCullLog2;
 }
 
 // Voxels of this block's tile owned by this thread: (li, lj, lk + step*q),
@@ -332,7 +389,7 @@ template <int NT, int KCULL>
 struct DoseShared {
     float dep[PB_MAX_LUT_LEN], sig[PB_MAX_LUT_LEN], idd[PB_MAX_LUT_LEN];
     SpotRec spot[NT * KCULL];
-    float red[NT / 32][10];
+    float red[NT / 32][kRedSlots];
     int wcount[KCULL][NT / 32];
     int wcount_h[KCULL][NT / 32];
 };
@@ -357,7 +414,7 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
     constexpr int kWarps = kThreads / 32;
     float *s_dep = sh.dep, *s_sig = sh.sig, *s_idd = sh.idd;
     SpotRec *s_spot = sh.spot;
-    float (*s_red)[10] = sh.red;
+    float (*s_red)[kRedSlots] = sh.red;
     int (*s_wcount)[kWarps] = sh.wcount;
     int (*s_wcount_h)[kWarps] = sh.wcount_h;
 
@@ -380,7 +437,7 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
         float2 XP[NP], YP[NP], GXP[NP], GYP[NP], WP[NP];
         TileBounds tb;
         {
-            float X[kVpt], Y[kVpt], GX[kVpt], GY[kVpt], W[kVpt];
+            float X[kVpt], Y[kVpt], GX[kVpt], GY[kVpt], W[kVpt], D[kVpt];
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
                 if (valid[q]) {
@@ -388,13 +445,15 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                     float Z;
                     voxel_head(A.g, B, i, jk % A.g.ny, jk / A.g.ny, X[q], Y[q], Z, GX[q], GY[q]);
                     W[q] = __fmul_rn(__ldg(wet + b * V + vidx[q]), 10.0f);
+                    D[q] = source_distance(B, X[q], Y[q], B.geom.vsadx * (1.0f - GX[q]));
                 } else {
                     X[q] = Y[q] = 0.0f;
                     GX[q] = GY[q] = 1.0f;
                     W[q] = INFINITY;
+                    D[q] = 0.0f;
                 }
             }
-            tb = tile_bounds<kVpt, kThreads>(X, Y, GX, GY, valid, s_red);
+            tb = tile_bounds<kVpt, kThreads>(X, Y, GX, GY, D, W, valid, s_red);
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
                 XP[p] = make_float2(X[2 * p], X[2 * p + 1]);
@@ -411,6 +470,7 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
         for (int l = 0; l < B.n_layers; ++l) {
             const PbLayer L = layers[B.layer_start + l];
             const float cut = __fmul_rn(1.1f, L.r80);
+            if (layer_skip(L, tb, B, cut)) continue;   // uniform over the block
             bool act[kVpt];
             bool any = false;
 #pragma unroll
@@ -634,7 +694,7 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
     __shared__ int s_cand[kCand];
     __shared__ float s_gsum[kCand];
     __shared__ __align__(8) float s_cg[6][kCand];
-    __shared__ float s_red[kWarps][10];
+    __shared__ float s_red[kWarps][kRedSlots];
     __shared__ int s_wcount[kAdjVpt > kSpt ? kAdjVpt : kSpt][kWarps];
     __shared__ int s_wcount_h[kSpt][kWarps];
 
@@ -671,11 +731,16 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                 WMM[q] = INFINITY;
             }
         }
-        const TileBounds tb = tile_bounds<kAdjVpt, kAdjThreads>(X, Y, GX, GY, valid, s_red);
+        float D[kAdjVpt];
+#pragma unroll
+        for (int q = 0; q < kAdjVpt; ++q)
+            D[q] = valid[q] ? source_distance(B, X[q], Y[q], Z[q]) : 0.0f;
+        const TileBounds tb = tile_bounds<kAdjVpt, kAdjThreads>(X, Y, GX, GY, D, WMM, valid, s_red);
 
         for (int l = 0; l < B.n_layers; ++l) {
             const PbLayer L = layers[B.layer_start + l];
             const float cut = __fmul_rn(1.1f, L.r80);
+            if (layer_skip(L, tb, B, cut)) continue;   // uniform over the block
             bool act[kAdjVpt];
             bool any = false;
 #pragma unroll
@@ -909,6 +974,115 @@ __global__ void k_objective_final(const double *partial, int nb, double *obj)
     if (threadIdx.x == 0) obj[0] = s[0];
 }
 
+// ----------------------------------------------------------- layer bounds
+
+struct BeamList {
+    int n_beams;
+    PbBeam b[PB_MAX_BEAMS];
+};
+
+constexpr int kBoundThreads = 256;
+constexpr int kHaloSamples = 2048;
+
+// sh(w), the nuclear-halo sigma before its clamp at 0 (IMPTClasses.cu:104-121),
+// in FP64.
+__device__ __forceinline__ double halo_sigma(double w, double r80)
+{
+    const double a1 = w - r80 - 5.0;
+    return 2.85 + 0.0014 * r80 * log(w + 3.0) + 0.06 * w - 7.4e-5 * w * w -
+           (0.22 * r80) / (a1 * a1);
+}
+
+// One block per (beam, layer): the culling bounds of PbLayer.
+//   spot box     min / max of the spots' x and y
+//   mcs_max      max |sigma| over the layer's LUT row (interpolation and the
+//                end clamps stay within the row's values)
+//   sh_max       max over the kernels' clamped depth w in [0.1, R80 - 0.1]
+//                (the single point R80 - 0.1 when that is below 0.1) of
+//                max(sh(w), 0): the maximum over kHaloSamples equally spaced
+//                points plus Lip * h / 2, with Lip a bound on |sh'(w)| there:
+//                |0.0014 R80| / (w + 3) + |0.06 - 1.48e-4 w| + 0.44 |R80| / 5.1^3
+//                (|w - R80 - 5| >= 5.1 on the interval).
+// bound_ok stays 0 when the layer has no spot or a value is not finite.
+__global__ void __launch_bounds__(kBoundThreads)
+k_layer_bounds(const __grid_constant__ BeamList A, PbLayer *layers, const float4 *geo)
+{
+    const PbBeam &B = A.b[blockIdx.y];
+    if ((int)blockIdx.x >= B.n_layers) return;
+    PbLayer *Lp = layers + B.layer_start + blockIdx.x;
+    const PbLayer L = *Lp;
+    __shared__ float s_v[kBoundThreads / 32][6];
+    __shared__ double s_h[kBoundThreads / 32];
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    bool bad = false;
+    float x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY, mm = 0.0f;
+    const int s0 = B.spot_start + L.spot_start;
+    for (int i = threadIdx.x; i < L.n_spots; i += kBoundThreads) {
+        const float4 g = geo[2 * (int64_t)(s0 + i)];
+        bad |= !(isfinite(g.x) && isfinite(g.y));
+        x0 = fminf(x0, g.x);
+        x1 = fmaxf(x1, g.x);
+        y0 = fminf(y0, g.y);
+        y1 = fmaxf(y1, g.y);
+    }
+    const float *sig = B.sigmas_dev + (size_t)L.energy_id * B.lut_len;
+    for (int i = threadIdx.x; i < B.lut_len; i += kBoundThreads) {
+        const float v = sig[i];
+        bad |= !isfinite(v);
+        mm = fmaxf(mm, fabsf(v));
+    }
+    const double r80 = (double)L.r80;
+    const double hi_w = (double)(L.r80 - 0.1f);
+    const double lo_w = hi_w > 0.1 ? 0.1 : hi_w;
+    const double h = (hi_w - lo_w) / (kHaloSamples - 1);
+    double shm = 0.0;
+    for (int k = threadIdx.x; k < kHaloSamples; k += kBoundThreads) {
+        const double v = halo_sigma(lo_w + h * k, r80);
+        shm = v > shm ? v : shm;
+    }
+    const double lip = fabs(0.0014 * r80) / (lo_w + 3.0) +
+                       fmax(fabs(0.06 - 1.48e-4 * lo_w), fabs(0.06 - 1.48e-4 * hi_w)) +
+                       0.44 * fabs(r80) / (5.1 * 5.1 * 5.1);
+    x0 = warp_min(x0);
+    x1 = warp_max(x1);
+    y0 = warp_min(y0);
+    y1 = warp_max(y1);
+    mm = warp_max(mm);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) shm = fmax(shm, __shfl_xor_sync(0xffffffffu, shm, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (bad) atomicOr(&s_bad, 1);
+    if (lane == 0) {
+        s_v[warp][0] = x0;
+        s_v[warp][1] = x1;
+        s_v[warp][2] = y0;
+        s_v[warp][3] = y1;
+        s_v[warp][4] = mm;
+        s_h[warp] = shm;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < kBoundThreads / 32; ++w) {
+        x0 = fminf(x0, s_v[w][0]);
+        x1 = fmaxf(x1, s_v[w][1]);
+        y0 = fminf(y0, s_v[w][2]);
+        y1 = fmaxf(y1, s_v[w][3]);
+        mm = fmaxf(mm, s_v[w][4]);
+        shm = fmax(shm, s_h[w]);
+    }
+    shm += lip * h * 0.5;
+    const bool ok = L.n_spots > 0 && !s_bad && isfinite(shm) && isfinite(r80);
+    Lp->sx0 = x0;
+    Lp->sx1 = x1;
+    Lp->sy0 = y0;
+    Lp->sy1 = y1;
+    Lp->sh_max = (float)shm * 1.0001f + 1e-3f;
+    Lp->mcs_max = mm;
+    Lp->bound_ok = ok ? 1 : 0;
+}
+
 // --------------------------------------------------------------- pair count
 
 __global__ void __launch_bounds__(256)
@@ -1079,6 +1253,22 @@ PbStatus launch_objective(const float *dose, const float *presc, const float *we
     if (s != PB_OK) return s;
     k_objective_final<<<1, 256, 0, st>>>(partial, kObjBlocks, obj);
     return check_launch("k_objective_final");
+}
+
+PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
+                            const float *geo, cudaStream_t st)
+{
+    BeamList A;
+    A.n_beams = n_beams;
+    int max_layers = 0;
+    for (int b = 0; b < n_beams; ++b) {
+        A.b[b] = beams[b];
+        if (beams[b].n_layers > max_layers) max_layers = beams[b].n_layers;
+    }
+    if (max_layers == 0) return PB_OK;
+    k_layer_bounds<<<dim3((unsigned)max_layers, (unsigned)n_beams), kBoundThreads, 0, st>>>(
+        A, layers, reinterpret_cast<const float4 *>(geo));
+    return check_launch("k_layer_bounds");
 }
 
 PbStatus launch_count_pairs(const PbGrid &g, const PbBeam *beams, int n_beams,

@@ -74,6 +74,8 @@ PbStatus launch_objective(const float *dose, const float *presc,
                           float *resid, void *work, cudaStream_t st);
 size_t objective_work_size();
 
+PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
+                            const float *geo, cudaStream_t st);
 PbStatus launch_count_pairs(const PbGrid &g, const PbBeam *beams, int n_beams,
                             const float *wet, const PbLayer *layers,
                             unsigned long long *count, cudaStream_t st);

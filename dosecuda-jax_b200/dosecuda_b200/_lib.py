@@ -56,7 +56,11 @@ class PbSpot(ctypes.Structure):
 class PbLayer(ctypes.Structure):
     _fields_ = [("spot_start", ctypes.c_int), ("n_spots", ctypes.c_int),
                 ("energy_id", ctypes.c_int), ("r80", ctypes.c_float),
-                ("energy", ctypes.c_float)]
+                ("energy", ctypes.c_float),
+                ("sx0", ctypes.c_float), ("sx1", ctypes.c_float),
+                ("sy0", ctypes.c_float), ("sy1", ctypes.c_float),
+                ("sh_max", ctypes.c_float), ("mcs_max", ctypes.c_float),
+                ("bound_ok", ctypes.c_int)]
 
 
 class PbBeam(ctypes.Structure):
@@ -90,7 +94,9 @@ PB_BATCH_DOSE = 2
 # numpy views of the structs (same layout) for bulk host arrays
 SPOT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("mu", "<f4"), ("energy_id", "<i4")])
 LAYER_DTYPE = np.dtype([("spot_start", "<i4"), ("n_spots", "<i4"), ("energy_id", "<i4"),
-                        ("r80", "<f4"), ("energy", "<f4")])
+                        ("r80", "<f4"), ("energy", "<f4"),
+                        ("sx0", "<f4"), ("sx1", "<f4"), ("sy0", "<f4"), ("sy1", "<f4"),
+                        ("sh_max", "<f4"), ("mcs_max", "<f4"), ("bound_ok", "<i4")])
 
 # Every entry point the header declares, with its argument types.
 _VP = ctypes.c_void_p
@@ -123,6 +129,7 @@ _SIGS = {
     "pb_objective_work_size": (ctypes.c_size_t, []),
     "pb_objective": (_I, [_VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP]),
     "pb_count_pairs": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),
+    "pb_layer_bounds": (_I, [_VP, _I, _VP, _VP, _VP]),
     "pb_proton_raytrace_host": (_I, [_I, _D, _D, _VP, _VP, _F, _VP, _VP, _D, _D, _VP]),
     "pb_proton_spot_host": (_I, [_I, _D, _D, _VP, _VP, _VP, _VP, _I, _I, _I, _VP, _VP, _F,
                                  _VP, _VP, _D, _D, _VP, _I, _VP]),

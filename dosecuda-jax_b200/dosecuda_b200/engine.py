@@ -173,6 +173,11 @@ class DevicePlan:
             B.n_energies = t.n_energies
             B.lut_len = t.lut_len
             B.dvp_len = t.dvp_len
+        # per-layer culling bounds (spot box, halo and MCS sigma bounds) on the device
+        if self.layer_offsets[-1]:
+            check(_lib.lib.pb_layer_bounds(ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                                           ptr(self.layers), ptr(self.spot_geo),
+                                           _stream(self.device)), "pb_layer_bounds")
         self.wet: Optional[torch.Tensor] = None
         self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._tex = ctypes.c_uint64(0)

@@ -72,10 +72,17 @@ typedef struct {
 } PbSpot;
 
 /* An energy layer (IMPTClasses.cuh:17-26); spot_start is relative to the
- * beam's first spot. */
+ * beam's first spot.  The fields after `energy` have no counterpart in the
+ * reference: bounds that let the dose kernels skip a layer for a whole
+ * voxel tile without evaluating it (pb_layer_bounds fills them on the
+ * device; pb_build_layers leaves bound_ok = 0, which disables the test). */
 typedef struct {
     int spot_start, n_spots, energy_id;
     float r80, energy;
+    float sx0, sx1, sy0, sy1;    /* box of the spots' (x, y) at the isocentre */
+    float sh_max;                /* >= the nuclear-halo sigma at any depth, mm */
+    float mcs_max;               /* >= |sigma_mcs| of the layer's LUT row, mm  */
+    int bound_ok;                /* 1 when the four lines above are filled    */
 } PbLayer;
 
 /* One beam of a plan as the dose kernels see it.  Model tables are device
@@ -184,6 +191,16 @@ PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams,
                  const float *wet_dev, const PbLayer *layers_dev,
                  const float *spot_geo_dev, const float *mu_dev, float scale,
                  float *dose_dev, float *beam_dose_dev, void *stream);
+
+/* Culling bounds of every layer of every beam (the fields after `energy`
+ * of PbLayer), computed on the device from the spot geometry and the beam
+ * models; call it once after the layers and spot geometry are on the
+ * device (and again if either changes).  With bound_ok set, pb_dose,
+ * pb_dose_adjoint and the batch kernels skip a layer for a voxel tile when
+ * no spot of the layer can pass their per-spot cull there; the results
+ * are the same as without the bounds.  No counterpart in the reference. */
+PbStatus pb_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers_dev,
+                         const float *spot_geo_dev, void *stream);
 
 /* Forward kernel shapes (block threads x voxels per thread over an 8x8x8
  * tile, spots culled per thread per round) the autotuner chooses from.

@@ -70,7 +70,12 @@ def test_build_layers_matches_oracle(oracle):
         sl = _random_spots(rng, n, dvp.shape[0])
         s1, l1, perm = _lib.build_layers(sl, dvp)
         s2, l2 = oracle.build_layers(sl, dvp)
-        assert s1.tobytes() == s2.tobytes() and l1.tobytes() == l2.tobytes()
+        assert s1.tobytes() == s2.tobytes()
+        # the reference's five layer fields; the culling bounds are left unset
+        assert len(l1) == len(l2)
+        for f in ("spot_start", "n_spots", "energy_id", "r80", "energy"):
+            assert np.array_equal(l1[f], l2[f])
+        assert not l1["bound_ok"].any()
         # perm maps each sorted spot to its input row
         if n:
             assert np.array_equal(sl[perm][:, 0], s1["x"])

@@ -335,6 +335,71 @@ def test_full_size_sampled_voxels_vs_oracle(pkg, oracle, curve):
     assert np.abs(dose[idx] - want).max() <= 2e-4 * dose.max()
 
 
+def _without_layer_bounds(dp):
+    """A copy of dp's device layer records with bound_ok cleared."""
+    words = dp.layers.view(torch.int32).reshape(-1, 12).clone()
+    words[:, 11] = 0
+    return words.view(torch.uint8).reshape(-1)
+
+
+@pytest.mark.parametrize("which", ["small", "full"])
+def test_layer_bounds_change_no_result(pkg, small, which):
+    """The per-(tile, layer) skip from pb_layer_bounds drops only layers the
+    per-spot cull would empty: dose, per-beam dose and gradient are
+    bit-identical with the bounds cleared."""
+    phantoms = pkg[2]
+    case = small if which == "small" else phantoms.config_gradient()
+    dp = case.grid.prepareIMPTPlan(case.plan, 0)
+    words = dp.layers.view(torch.int32).reshape(-1, 12)
+    assert int(words[:, 11].min()) == 1          # every layer got its bounds
+    presc, wts = case.objective_fields()
+    d1, bd1 = dp.forward(beam_doses=True)
+    from dosecuda_b200 import engine
+    resid = torch.empty_like(d1)
+    engine.objective(d1, torch.from_numpy(presc.reshape(-1)).to(DEV),
+                     torch.from_numpy(wts.reshape(-1)).to(DEV), resid)
+    g1 = dp.adjoint(resid).clone()
+    bounded = dp.layers
+    dp.layers = _without_layer_bounds(dp)
+    try:
+        d2, bd2 = dp.forward(beam_doses=True)
+        g2 = dp.adjoint(resid)
+    finally:
+        dp.layers = bounded
+    assert torch.equal(d1, d2) and torch.equal(bd1, bd2)
+    # the adjoint sums tile partials with float atomics in any order
+    assert torch.allclose(g1, g2, rtol=1e-5, atol=1e-6 * float(g1.abs().max()))
+
+
+def test_layer_bounds_values(pkg, small):
+    """pb_layer_bounds against a host recomputation: spot boxes and the LUT
+    row maxima exactly, the halo-sigma bound at least the formula's maximum
+    on a dense depth grid."""
+    g, plan = small.grid, small.plan
+    dp = g.prepareIMPTPlan(plan, 0)
+    rec = dp.layers.cpu().numpy().view(pkg[0]._lib.LAYER_DTYPE)
+    geo = dp.spot_geo.cpu().numpy()
+    for b in range(dp.n_beams):
+        t = dp.tables[b]
+        sig = t.sigmas.cpu().numpy()
+        for l in range(dp.n_layers[b]):
+            L = rec[dp.layer_offsets[b] + l]
+            s0 = dp.spot_offsets[b] + int(L["spot_start"])
+            xy = geo[s0:s0 + int(L["n_spots"]), :2]
+            assert L["bound_ok"] == 1
+            assert (L["sx0"], L["sx1"]) == (xy[:, 0].min(), xy[:, 0].max())
+            assert (L["sy0"], L["sy1"]) == (xy[:, 1].min(), xy[:, 1].max())
+            assert L["mcs_max"] == np.abs(sig[int(L["energy_id"])]).max()
+            r80 = float(L["r80"])
+            hi = float(np.float32(r80) - np.float32(0.1))
+            w = np.linspace(min(0.1, hi), hi, 20001)
+            a1 = w - r80 - 5.0
+            sh = 2.85 + 0.0014 * r80 * np.log(w + 3.0) + 0.06 * w - 7.4e-5 * w * w - \
+                (0.22 * r80) / (a1 * a1)
+            assert L["sh_max"] >= max(sh.max(), 0.0)
+            assert L["sh_max"] <= max(sh.max(), 0.0) + 0.05
+
+
 def test_count_pairs_matches_oracle(pkg, small, oracle):
     g, plan = small.grid, small.plan
     dp = g.prepareIMPTPlan(plan, 0)
