@@ -687,13 +687,13 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
     VoxRec *s_vox = reinterpret_cast<VoxRec *>(s_dyn);       // kAdjThreads * kAdjVpt
     // Candidate spots of one compaction round: index, gradient partial and
     // the geometry terms of axis_r2 (negated where axis_r2 wants them so),
-    // one array per term so that a spot pair is one float2 load each.  The
-    // halo-only class starts at an even slot; the slot between the classes
-    // (odd n2) is padding.
-    constexpr int kCand = kAdjThreads * kSpt + 2;
+    // one array per term so that four consecutive spots are one float4 load
+    // each.  The halo-only class starts at a multiple of four; the slots
+    // between the classes are padding.
+    constexpr int kCand = kAdjThreads * kSpt + 8;
     __shared__ int s_cand[kCand];
     __shared__ float s_gsum[kCand];
-    __shared__ __align__(8) float s_cg[6][kCand];
+    __shared__ __align__(16) float s_cg[6][kCand];
     __shared__ float s_red[kWarps][kRedSlots];
     __shared__ int s_wcount[kAdjVpt > kSpt ? kAdjVpt : kSpt][kWarps];
     __shared__ int s_wcount_h[kSpt][kWarps];
@@ -821,7 +821,7 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 #pragma unroll
                 for (int c = 0; c < kSpt; ++c)
                     for (int w = 0; w < kWarps; ++w) n2 += s_wcount[c][w];
-                const int f1 = (n2 + 1) & ~1;   // first halo-only slot
+                const int f1 = (n2 + 3) & ~3;   // first halo-only slot
                 int c2 = 0, c1 = f1;
                 const unsigned below = (1u << lane) - 1u;
 #pragma unroll
@@ -849,73 +849,83 @@ k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                 const int total = c1;   // slots used, padding included
                 __syncthreads();
                 // Two passes, both-term spots then halo-only spots, each over
-                // work items (spot pair, voxel stripe) so that every thread is
-                // busy even when few spots survive the culling (an odd spot
-                // is paired with an empty slot).  Partial sums meet in shared
-                // memory, then one atomic per spot goes to global.
+                // work items (four spots, voxel stripe) so that every thread is
+                // busy even when few spots survive the culling; each voxel
+                // record read from shared memory serves four spots as two
+                // packed pairs.  A group's slots past the class's last spot
+                // (padding or the next class) hold finite values and their
+                // sums are dropped.  Partial sums meet in shared memory, then
+                // one atomic per spot goes to global.
 #pragma unroll 1
                 for (int pass = 0; pass < 2; ++pass) {
                     const int first = pass ? f1 : 0, cnt = pass ? total - f1 : n2;
-                    const int npair = (cnt + 1) >> 1;
-                    if (npair == 0) continue;
-                    const int stripes = npair >= kAdjThreads ? 1 : kAdjThreads / npair;
-                    const int items = npair * stripes;
+                    const int nq = (cnt + 3) >> 2;
+                    if (nq == 0) continue;
+                    const int stripes = nq >= kAdjThreads ? 1 : kAdjThreads / nq;
+                    const int items = nq * stripes;
                     for (int it = threadIdx.x; it < items; it += kAdjThreads) {
-                        const int sp = it % npair, vs = it / npair;
-                        // a pair's second slot may be padding or the next
-                        // class's first spot: finite either way, and its sum
-                        // is dropped below
-                        const int c0 = first + 2 * sp;
-                        const float2 nx = *reinterpret_cast<const float2 *>(&s_cg[0][c0]);
-                        const float2 ny = *reinterpret_cast<const float2 *>(&s_cg[1][c0]);
-                        const float2 tx = *reinterpret_cast<const float2 *>(&s_cg[2][c0]);
-                        const float2 nty = *reinterpret_cast<const float2 *>(&s_cg[3][c0]);
-                        const float2 ncs = *reinterpret_cast<const float2 *>(&s_cg[4][c0]);
-                        const float2 it2 = *reinterpret_cast<const float2 *>(&s_cg[5][c0]);
-                        float2 acc0 = make_float2(0.0f, 0.0f), acc1 = acc0;
+                        const int sq = it % nq, vs = it / nq;
+                        const int c0 = first + 4 * sq;
+                        const float4 g0 = *reinterpret_cast<const float4 *>(&s_cg[0][c0]);
+                        const float4 g1 = *reinterpret_cast<const float4 *>(&s_cg[1][c0]);
+                        const float4 g2 = *reinterpret_cast<const float4 *>(&s_cg[2][c0]);
+                        const float4 g3 = *reinterpret_cast<const float4 *>(&s_cg[3][c0]);
+                        const float4 g4 = *reinterpret_cast<const float4 *>(&s_cg[4][c0]);
+                        const float4 g5 = *reinterpret_cast<const float4 *>(&s_cg[5][c0]);
+                        const float2 nxa = lo2(g0), nya = lo2(g1), txa = lo2(g2), ntya = lo2(g3),
+                                     ncsa = lo2(g4), it2a = lo2(g5);
+                        const float2 nxb = hi2(g0), nyb = hi2(g1), txb = hi2(g2), ntyb = hi2(g3),
+                                     ncsb = hi2(g4), it2b = hi2(g5);
+                        float2 ha = make_float2(0.0f, 0.0f), hb = ha;
                         int c = vs;
                         if (pass == 0) {
-                            float2 accp0 = acc0, accp1 = acc0;
-                            for (; c + stripes < nact; c += 2 * stripes) {
-                                const VoxRec v = s_vox[c], u = s_vox[c + stripes];
-                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
-                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
-                                const float2 qu = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(u.xy),
-                                                          hi2(u.xy), lo2(u.g), hi2(u.g));
-                                accp0 = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qv)), accp0);
-                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
-                                accp1 = __ffma2_rn(lo2(u.f), ex2x2(__fmul2_rn(lo2(u.s), qu)), accp1);
-                                acc1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), qu)), acc1);
-                            }
-                            if (c < nact) {
+                            float2 pa = ha, pb = ha;
+                            for (; c < nact; c += stripes) {
                                 const VoxRec v = s_vox[c];
-                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
-                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
-                                accp0 = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qv)), accp0);
-                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
+                                const float2 qa = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
+                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
+                                const float2 qb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
+                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
+                                pa = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qa)), pa);
+                                ha = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qa)), ha);
+                                pb = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qb)), pb);
+                                hb = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qb)), hb);
                             }
-                            acc0 = __fadd2_rn(acc0, accp0);
-                            acc1 = __fadd2_rn(acc1, accp1);
+                            ha = __fadd2_rn(ha, pa);
+                            hb = __fadd2_rn(hb, pb);
                         } else {
+                            float2 ha1 = ha, hb1 = ha;
                             for (; c + stripes < nact; c += 2 * stripes) {
                                 const VoxRec v = s_vox[c], u = s_vox[c + stripes];
-                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
-                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
-                                const float2 qu = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(u.xy),
-                                                          hi2(u.xy), lo2(u.g), hi2(u.g));
-                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
-                                acc1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), qu)), acc1);
+                                const float2 qa = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
+                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
+                                const float2 qb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
+                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
+                                const float2 ra = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
+                                                          lo2(u.xy), hi2(u.xy), lo2(u.g), hi2(u.g));
+                                const float2 rb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
+                                                          lo2(u.xy), hi2(u.xy), lo2(u.g), hi2(u.g));
+                                ha = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qa)), ha);
+                                hb = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qb)), hb);
+                                ha1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), ra)), ha1);
+                                hb1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), rb)), hb1);
                             }
                             if (c < nact) {
                                 const VoxRec v = s_vox[c];
-                                const float2 qv = axis_r2(nx, ny, tx, nty, ncs, it2, lo2(v.xy),
-                                                          hi2(v.xy), lo2(v.g), hi2(v.g));
-                                acc0 = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qv)), acc0);
+                                const float2 qa = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
+                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
+                                const float2 qb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
+                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
+                                ha = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qa)), ha);
+                                hb = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qb)), hb);
                             }
+                            ha = __fadd2_rn(ha, ha1);
+                            hb = __fadd2_rn(hb, hb1);
                         }
-                        const float2 acc = __fadd2_rn(acc0, acc1);
-                        if (acc.x != 0.0f) atomicAdd(&s_gsum[c0], acc.x);
-                        if (acc.y != 0.0f && 2 * sp + 1 < cnt) atomicAdd(&s_gsum[c0 + 1], acc.y);
+                        const float sum[4] = {ha.x, ha.y, hb.x, hb.y};
+#pragma unroll
+                        for (int h = 0; h < 4; ++h)
+                            if (sum[h] != 0.0f && 4 * sq + h < cnt) atomicAdd(&s_gsum[c0 + h], sum[h]);
                     }
                 }
                 __syncthreads();
