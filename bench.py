@@ -46,6 +46,10 @@ for _p in (os.path.join(ROOT, "dosecuda-jax_b200"), ROOT):
 METRIC = "IMPT dose+grad ms/plan (20k spots, 256²×160) vs plain fwd; spot-voxel evals/s"
 UNIT = "spot-voxel evals/s"
 L2_FLUSH_BYTES = 256 << 20
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_dose launch of the
+# default workload (seed 3, texture WET), from the ncu --set full capture
+# summarised in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md
+K_DOSE_TRAFFIC = 169_797_120 + 32_388_608
 
 
 def _peaks():
@@ -238,6 +242,14 @@ def run_mine(args, world, rank, local):
     bytes_dose = 4 * V * (dp.n_beams + 1) + 36 * n_spots + \
         sum(t.dvp.numel() + 3 * t.depths.numel() for t in dp.tables) * 4
     achieved = bytes_dose / (kms["dose"] * 1e-3) / 1e9
+    # SFU roofline of the same kernel: the exp2 operations one launch issues
+    # (counted with its own culling decisions) over its time, against the
+    # exp2 throughput measured on this GPU now
+    n_ex2, n_eval = dp.count_evaluated()
+    ex2_peak = engine.measure_ex2_rate(dev)
+    ex2_achieved = n_ex2 / (kms["dose"] * 1e-3)
+    # DRAM traffic of one k_dose launch from the ncu capture of this workload
+    traffic = K_DOSE_TRAFFIC if (args.seed == 3 and args.wet_mode == "texture") else None
     line = {
         "metric": METRIC,
         "value": E_all / (ms_step * 1e-3),
@@ -268,7 +280,14 @@ def run_mine(args, world, rank, local):
         "roofline": {"kernel": "k_dose (forward pencil-beam sum)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": f"of {peak_kind}",
-                     "algorithmic_bytes_per_launch": bytes_dose, "traffic": None},
+                     "algorithmic_bytes_per_launch": bytes_dose, "traffic": traffic},
+        "compute_roofline": {"kernel": "k_dose", "bound": "sfu (exp2)",
+                             "achieved": ex2_achieved, "peak": ex2_peak, "unit": "exp2/s",
+                             "frac": ex2_achieved / ex2_peak,
+                             "peak_kind": "measured now on this GPU (pb_measure_ex2_rate)",
+                             "exp2_per_launch": n_ex2,
+                             "spot_voxel_evaluations_per_launch": n_eval,
+                             "dense_pairs_E": E},
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -396,16 +396,22 @@ struct DoseShared {
 
 // Forward dose of one 8x8x8 tile of one plan by one block of NT threads,
 // VPT = 512 / NT voxels per thread; spots are culled KCULL per thread per
-// compaction round.  BEAM_OUT: also write each beam's dose.
-template <int NT, int VPT, int KCULL, bool BEAM_OUT>
+// compaction round.  BEAM_OUT: also write each beam's dose.  COUNT: take
+// every decision of the forward but, instead of evaluating the surviving
+// spots, add to count[0] the SFU exponentials and to count[1] the
+// spot-voxel evaluations the forward would issue (every one of the tile's
+// 512 voxel slots against each surviving spot), and write no dose.
+template <int NT, int VPT, int KCULL, bool BEAM_OUT, bool COUNT = false>
 __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                                           const float *__restrict__ wet,
                                           const PbLayer *__restrict__ layers,
                                           const float4 *__restrict__ geo,
                                           const float *__restrict__ mu, float *__restrict__ dose,
                                           float *__restrict__ beam_dose,
-                                          DoseShared<NT, KCULL> &sh)
+                                          DoseShared<NT, KCULL> &sh,
+                                          unsigned long long *count = nullptr)
 {
+    unsigned long long n_ex2 = 0, n_eval = 0;
     static_assert(NT * VPT == 512, "a block covers one 8x8x8 tile");
     constexpr int kVpt = VPT;
     constexpr int kThreads = NT;
@@ -558,7 +564,8 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                         n1 += s_wcount_h[c][w];
                     }
                     if (cls[c]) {
-                        const float w = __ldg(mu + s0 + base + c * kThreads + threadIdx.x);
+                        const float w =
+                            COUNT ? 0.0f : __ldg(mu + s0 + base + c * kThreads + threadIdx.x);
                         SpotRec r;
                         r.a = make_float4(-ga[c].x, -ga[c].x, -ga[c].y, -ga[c].y);
                         r.b = make_float4(ga[c].z, ga[c].z, -ga[c].w, -ga[c].w);
@@ -568,29 +575,34 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                     }
                 }
                 __syncthreads();
+                if constexpr (COUNT) {
+                    n_ex2 += 512ull * (unsigned long long)(2 * n2 + n1);
+                    n_eval += 512ull * (unsigned long long)(n2 + n1);
+                } else {
 #pragma unroll 2
-                for (int c = 0; c < n2; ++c) {
-                    const SpotRec r = s_spot[c];
-                    const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
-                                 ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
+                    for (int c = 0; c < n2; ++c) {
+                        const SpotRec r = s_spot[c];
+                        const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
+                                     ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) {
-                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
-                                                  GXP[p], GYP[p]);
-                        AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS[p], qq)), AP[p]);
-                        AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
+                        for (int p = 0; p < NP; ++p) {
+                            const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
+                                                      GXP[p], GYP[p]);
+                            AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS[p], qq)), AP[p]);
+                            AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
+                        }
                     }
-                }
 #pragma unroll 2
-                for (int c = kCap - n1; c < kCap; ++c) {
-                    const SpotRec r = s_spot[c];
-                    const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
-                                 ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
+                    for (int c = kCap - n1; c < kCap; ++c) {
+                        const SpotRec r = s_spot[c];
+                        const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
+                                     ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) {
-                        const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
-                                                  GXP[p], GYP[p]);
-                        AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
+                        for (int p = 0; p < NP; ++p) {
+                            const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
+                                                      GXP[p], GYP[p]);
+                            AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
+                        }
                     }
                 }
                 __syncthreads();
@@ -613,9 +625,16 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
         }
         __syncthreads();  // s_red is rewritten by the next beam's tile_bounds
     }
+    if constexpr (COUNT) {
+        if (threadIdx.x == 0) {
+            atomicAdd(count, n_ex2);
+            atomicAdd(count + 1, n_eval);
+        }
+    } else {
 #pragma unroll
-    for (int q = 0; q < kVpt; ++q)
-        if (valid[q]) dose[vidx[q]] = (tot_s[q] + tot_c[q]) * A.scale;
+        for (int q = 0; q < kVpt; ++q)
+            if (valid[q]) dose[vidx[q]] = (tot_s[q] + tot_c[q]) * A.scale;
+    }
 }
 
 #ifndef PB_DOSE_MIN_BLOCKS
@@ -633,6 +652,39 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 {
     __shared__ DoseShared<NT, KCULL> sh;
     dose_tile<NT, VPT, KCULL, BEAM_OUT>(A, blockIdx.x, wet, layers, geo, mu, dose, beam_dose, sh);
+}
+
+// The forward's SFU exponentials and spot-voxel evaluations, counted with
+// its own decisions (dose_tile with COUNT); shape of pb_dose's kernel.
+__global__ void __launch_bounds__(128, dose_min_blocks<128>())
+k_dose_count(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+             const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
+             unsigned long long *count)
+{
+    __shared__ DoseShared<128, 2> sh;
+    dose_tile<128, 4, 2, false, true>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr, nullptr,
+                                      sh, count);
+}
+
+// SFU exp2 throughput: kEx2Chains independent chains x <- 2^(-x) per
+// thread (each stays in (0.5, 1)); the result is stored only if it takes a
+// value it never takes, so that nothing is removed as dead code.
+constexpr int kEx2Chains = 8;
+__device__ float g_ex2_sink;
+
+__global__ void __launch_bounds__(256) k_ex2_rate(int iters)
+{
+    float x[kEx2Chains];
+#pragma unroll
+    for (int c = 0; c < kEx2Chains; ++c) x[c] = 0.5f + 0.01f * (float)(c + (threadIdx.x & 7));
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < kEx2Chains; ++c) x[c] = ex2(-x[c]);
+    }
+    float t = 0.0f;
+#pragma unroll
+    for (int c = 0; c < kEx2Chains; ++c) t += x[c];
+    if (t == 12345.0f) g_ex2_sink = t;
 }
 
 // One plan of a batch as the persistent kernel reads it.
@@ -1279,6 +1331,53 @@ PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
     k_layer_bounds<<<dim3((unsigned)max_layers, (unsigned)n_beams), kBoundThreads, 0, st>>>(
         A, layers, reinterpret_cast<const float4 *>(geo));
     return check_launch("k_layer_bounds");
+}
+
+PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beams,
+                                const float *wet, const PbLayer *layers, const float *geo,
+                                unsigned long long *count, cudaStream_t st)
+{
+    PlanArgs A;
+    fill_args(A, g, beams, n_beams, 1.0f);
+    PbStatus s = check_cuda(cudaMemsetAsync(count, 0, 2 * sizeof(unsigned long long), st),
+                            "cudaMemsetAsync(count)");
+    if (s != PB_OK) return s;
+    const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
+    k_dose_count<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers,
+                                                  reinterpret_cast<const float4 *>(geo), count);
+    return check_launch("k_dose_count");
+}
+
+PbStatus measure_ex2_rate(double *ops_per_s, cudaStream_t st)
+{
+    int dev = 0, sms = 0;
+    PbStatus s = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (s == PB_OK)
+        s = check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+                       "cudaDeviceGetAttribute");
+    if (s != PB_OK) return s;
+    const int blocks = sms * 8, iters = 4096;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    s = check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    if (s == PB_OK) s = check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    float best = 0.0f;
+    for (int rep = 0; rep < 4 && s == PB_OK; ++rep) {   // the first run warms up
+        s = check_cuda(cudaEventRecord(e0, st), "cudaEventRecord");
+        if (s == PB_OK) {
+            k_ex2_rate<<<blocks, 256, 0, st>>>(iters);
+            s = check_launch("k_ex2_rate");
+        }
+        if (s == PB_OK) s = check_cuda(cudaEventRecord(e1, st), "cudaEventRecord");
+        if (s == PB_OK) s = check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+        float ms = 0.0f;
+        if (s == PB_OK) s = check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+        if (s == PB_OK && rep > 0 && (best == 0.0f || ms < best)) best = ms;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s != PB_OK) return s;
+    *ops_per_s = (double)blocks * 256.0 * iters * kEx2Chains / (best * 1e-3);
+    return PB_OK;
 }
 
 PbStatus launch_count_pairs(const PbGrid &g, const PbBeam *beams, int n_beams,

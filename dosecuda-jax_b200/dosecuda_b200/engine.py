@@ -308,6 +308,29 @@ class DevicePlan:
         return int(c.item())
 
 
+    def count_evaluated(self):
+        """(SFU exp2 operations, spot-voxel evaluations) one forward issues,
+        counted with the forward kernel's own culling decisions."""
+        self._need_wet()
+        c = torch.zeros(2, dtype=torch.int64, device=self.device)
+        check(_lib.lib.pb_count_evaluated(ctypes.byref(self.grid),
+                                          ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                                          ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
+                                          ptr(c), _stream(self.device)), "pb_count_evaluated")
+        v = c.cpu().tolist()
+        return int(v[0]), int(v[1])
+
+
+def measure_ex2_rate(device) -> float:
+    """Measured SFU exp2 throughput of a device (operations/s)."""
+    device = require_cuda(device)
+    r = ctypes.c_double(0.0)
+    with torch.cuda.device(device):
+        check(_lib.lib.pb_measure_ex2_rate(ctypes.byref(r), _stream(device)),
+              "pb_measure_ex2_rate")
+    return float(r.value)
+
+
 _OBJ_WORK = {}
 
 

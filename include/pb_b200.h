@@ -202,6 +202,24 @@ PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams,
 PbStatus pb_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers_dev,
                          const float *spot_geo_dev, void *stream);
 
+/* ------------------------------------------------------- measurement */
+
+/* What the forward pencil-beam sum issues, counted with its own culling
+ * decisions (no dose is computed): count_dev[0] = SFU exp2 operations,
+ * count_dev[1] = spot-voxel evaluations (each surviving spot against the
+ * 512 voxel slots of a tile).  With a time, count_dev[0] gives the SFU
+ * roofline fraction of pb_dose.  No counterpart in the reference. */
+PbStatus pb_count_evaluated(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                            const float *wet_dev, const PbLayer *layers_dev,
+                            const float *spot_geo_dev, unsigned long long *count_dev,
+                            void *stream);
+
+/* Measured SFU exp2 throughput of the current device (operations/s): a
+ * fixed kernel of independent exp2 chains on every SM, best of three
+ * timed runs.  Synchronises with the stream.  No counterpart in the
+ * reference. */
+PbStatus pb_measure_ex2_rate(double *ops_per_s, void *stream);
+
 /* Forward kernel shapes (block threads x voxels per thread over an 8x8x8
  * tile, spots culled per thread per round) the autotuner chooses from.
  * pb_dose uses variant 0. */

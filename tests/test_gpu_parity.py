@@ -359,14 +359,18 @@ def test_layer_bounds_change_no_result(pkg, small, which):
     engine.objective(d1, torch.from_numpy(presc.reshape(-1)).to(DEV),
                      torch.from_numpy(wts.reshape(-1)).to(DEV), resid)
     g1 = dp.adjoint(resid).clone()
+    n1 = dp.count_evaluated()
     bounded = dp.layers
     dp.layers = _without_layer_bounds(dp)
     try:
         d2, bd2 = dp.forward(beam_doses=True)
         g2 = dp.adjoint(resid)
+        n2 = dp.count_evaluated()
     finally:
         dp.layers = bounded
     assert torch.equal(d1, d2) and torch.equal(bd1, bd2)
+    # the same spots survive the cull: the same exp2 and evaluation counts
+    assert n1 == n2 and n1[1] <= n1[0] <= 2 * n1[1] and n1[1] > 0
     # the adjoint sums tile partials with float atomics in any order
     assert torch.allclose(g1, g2, rtol=1e-5, atol=1e-6 * float(g1.abs().max()))
 
