@@ -14,33 +14,31 @@
 //   t x ray = ( Y - ys(1-Z/VSADY), -(X - xs(1-Z/VSADX)),
 //               (xs/VSADX) Y - (ys/VSADY) X - xs ys (1/VSADX - 1/VSADY) ).
 //
-// Forward work decomposition: one block of 128 threads per 8x8x8 voxel
-// tile, four voxels per thread; all beams and layers of the plan are looped
-// inside the block, so each voxel's dose is written once, compensated
-// (Neumaier) across layers and beams, with no atomics.  Per (tile, layer)
-// the layer's LUT row is staged in shared memory and the layer's spots are
-// culled against the tile: a spot is skipped when, for every voxel of the
-// tile, its Gaussian factor is below 2^-24 of the voxel's peak factor (bound
-// from the tile's BEV box and the widest halo sigma in the tile).  Surviving
-// spots are compacted into shared memory (each value stored twice), and
-// every thread evaluates each spot on its four voxels as two packed FP32x2
-// voxel pairs (two spot-voxel pairs per instruction) with the SFU's ex2.
+// Work decomposition: one block of 128 threads per 8x8x8 voxel tile, four
+// voxels per thread; all beams and layers of the plan are looped inside the
+// block, so each voxel's dose is written once, compensated (Neumaier) across
+// layers and beams, with no atomics.  Per (tile, layer): a test on the
+// layer's bounds (pb_layer_bounds) skips layers no spot of which can reach
+// the tile; the layer's LUT row is staged in shared memory; the layer's
+// spots are culled against the tile -- a Gaussian term is skipped when, at
+// every voxel of the tile, it is below 2^-24 of the voxel's peak factor
+// (bound from the tile's BEV box and the widest sigma in the tile), which
+// leaves spots with both terms and spots with the halo term only.
+// Surviving spots are compacted into shared memory (each value stored
+// twice), and every thread evaluates each spot on its four voxels as two
+// packed FP32x2 voxel pairs (two spot-voxel pairs per instruction) with the
+// SFU's ex2.
 //
-// The adjoint uses the same tiles and culling; per (tile, layer) the active
-// voxels (dObj/dD != 0, inside the range cut) are compacted into shared
-// memory; the surviving spots, taken as packed pairs, are split with the
-// voxels into (spot pair, voxel stripe) work items so that every thread is
-// busy; partial sums meet in shared memory and each spot's sum goes to its
-// gradient with one global atomic per (tile, layer).
+// The adjoint is the same tile code (dose_tile in adjoint mode): the same
+// decisions, with the voxels where dObj/dD = 0 inactive; the per-spot sums
+// over a thread's voxels meet across the warp with a transposed butterfly,
+// across the block in shared memory, and go to the gradient with one global
+// atomic per spot per (tile, layer).
 #include "pb_internal.h"
 
 namespace pb {
 
-constexpr int kAdjThreads = 256;    // adjoint block
-constexpr int kAdjVpt = 2;          // adjoint: voxels per thread (z, z+4)
-constexpr int kSpt = 2;             // adjoint: spots culled per thread per chunk
 constexpr float kCullLog2 = 24.0f;  // skip factors below 2^-24
-constexpr int kAdjDynSmem = 64 * kAdjThreads * kAdjVpt;   // the adjoint's voxel records
 
 struct PlanArgs {
     PbGrid g;
@@ -59,15 +57,6 @@ struct __align__(16) SpotRec {
     float4 d;  // (mu, mu, 0, 0)
 };
 
-// One voxel's layer record, each value duplicated for FP32x2 use.
-struct __align__(16) VoxRec {
-    float4 xy;   // (X, X, Y, Y)
-    float4 g;    // (gx, gx, gy, gy)
-    float4 s;    // (ps2, ps2, hs2, hs2)
-    float4 f;    // (w*Pf, w*Pf, w*Hf, w*Hf)
-};
-
-static_assert(sizeof(VoxRec) == 64, "voxel record size");
 
 struct TileBounds {
     float x0, x1, y0, y1, gx0, gx1, gy0, gy1;  // BEV box and divergence factors
@@ -380,28 +369,63 @@ __device__ __forceinline__ void stage_lut(const PbBeam &B, int e, float *s_dep,
 
 // ------------------------------------------------------------------ forward
 
-#ifndef PB_ADJ_MIN_BLOCKS
-#define PB_ADJ_MIN_BLOCKS 3
-#endif
 
-// Shared memory of one forward tile.
+// What dose_tile computes: the dose, the forward's operation counts, or the
+// adjoint (gradient with respect to the spot weights).
+constexpr int kModeDose = 0, kModeCount = 1, kModeAdjoint = 2;
+
+// Shared memory of one tile.  The spot list has 8 slots past its end: the
+// adjoint reads spots in groups of 8.
 template <int NT, int KCULL>
 struct DoseShared {
     float dep[PB_MAX_LUT_LEN], sig[PB_MAX_LUT_LEN], idd[PB_MAX_LUT_LEN];
-    SpotRec spot[NT * KCULL];
+    SpotRec spot[NT * KCULL + 8];
+    float gsum[NT * KCULL + 8];   // adjoint: per-slot gradient partials
     float red[NT / 32][kRedSlots];
     int wcount[KCULL][NT / 32];
     int wcount_h[KCULL][NT / 32];
 };
 
-// Forward dose of one 8x8x8 tile of one plan by one block of NT threads,
-// VPT = 512 / NT voxels per thread; spots are culled KCULL per thread per
-// compaction round.  BEAM_OUT: also write each beam's dose.  COUNT: take
-// every decision of the forward but, instead of evaluating the surviving
-// spots, add to count[0] the SFU exponentials and to count[1] the
-// spot-voxel evaluations the forward would issue (every one of the tile's
-// 512 voxel slots against each surviving spot), and write no dose.
-template <int NT, int VPT, int KCULL, bool BEAM_OUT, bool COUNT = false>
+// Sum over the warp of eight per-lane values v[0..7] (one per spot) with a
+// transposed butterfly (9 shuffles): on return, the lanes whose two lowest
+// bits are 0 hold the total of spot `slot` (each of the 8 spots once).
+__device__ __forceinline__ float warp_sum8(float (&v)[8], int lane, int &slot)
+{
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float send = h16 ? v[i] : v[i + 4], keep = h16 ? v[i + 4] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const float send = h8 ? v[i] : v[i + 2], keep = h8 ? v[i + 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const float send = h4 ? v[0] : v[1], keep = h4 ? v[1] : v[0];
+    float t = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    t += __shfl_xor_sync(0xffffffffu, t, 2);
+    t += __shfl_xor_sync(0xffffffffu, t, 1);
+    slot = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
+    return t;
+}
+
+// One 8x8x8 tile of one plan by one block of NT threads, VPT = 512 / NT
+// voxels per thread; spots are culled KCULL per thread per compaction round.
+//   kModeDose     the dose (BEAM_OUT: also each beam's dose)
+//   kModeCount    every decision of the forward, but instead of evaluating
+//                 the surviving spots, add to count[0] the SFU exponentials
+//                 and to count[1] the spot-voxel evaluations the forward
+//                 issues (each surviving spot against the tile's 512 voxel
+//                 slots); no dose
+//   kModeAdjoint  grad[spot] += scale * sum over the tile's voxels of
+//                 wfield[v] * d dose[v] / d mu[spot], with the voxels where
+//                 wfield is 0 inactive.  Each thread evaluates its voxels
+//                 against the surviving spots in groups of 8; the per-spot
+//                 sums meet across the warp (warp_sum8), across the warps in
+//                 shared memory, then go to grad with one global atomic per
+//                 spot per (tile, layer).
+template <int NT, int VPT, int KCULL, bool BEAM_OUT, int MODE = kModeDose>
 __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                                           const float *__restrict__ wet,
                                           const PbLayer *__restrict__ layers,
@@ -409,8 +433,12 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                                           const float *__restrict__ mu, float *__restrict__ dose,
                                           float *__restrict__ beam_dose,
                                           DoseShared<NT, KCULL> &sh,
-                                          unsigned long long *count = nullptr)
+                                          unsigned long long *count = nullptr,
+                                          const float *__restrict__ wfield = nullptr,
+                                          float *__restrict__ grad = nullptr)
 {
+    constexpr bool COUNT = MODE == kModeCount;
+    constexpr bool ADJ = MODE == kModeAdjoint;
     unsigned long long n_ex2 = 0, n_eval = 0;
     static_assert(NT * VPT == 512, "a block covers one 8x8x8 tile");
     constexpr int kVpt = VPT;
@@ -436,6 +464,17 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
     float tot_s[kVpt], tot_c[kVpt];
 #pragma unroll
     for (int q = 0; q < kVpt; ++q) tot_s[q] = tot_c[q] = 0.0f;
+    float wv[kVpt];   // adjoint: scale * dObj/dD per voxel
+    if constexpr (ADJ) {
+        bool anyw = false;
+#pragma unroll
+        for (int q = 0; q < kVpt; ++q) {
+            wv[q] = valid[q] ? __ldg(wfield + vidx[q]) * A.scale : 0.0f;
+            anyw |= (wv[q] != 0.0f);
+        }
+        if (!__syncthreads_or(anyw)) return;
+        for (int c = threadIdx.x; c < kCull * kThreads + 8; c += kThreads) sh.gsum[c] = 0.0f;
+    }
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
@@ -483,6 +522,7 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
             for (int q = 0; q < kVpt; ++q) {
                 const float w = (q & 1) ? WP[q >> 1].y : WP[q >> 1].x;
                 act[q] = valid[q] && !(w > cut);
+                if constexpr (ADJ) act[q] = act[q] && wv[q] != 0.0f;
                 any |= act[q];
             }
             if (!__syncthreads_or(any)) continue;
@@ -521,6 +561,15 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
             block_max2<kThreads>(hmax, pmax, s_red, nhs, nps);
             nhs = -nhs;
             nps = -nps;
+            // adjoint: the voxels' weighted prefactors as packed pairs
+            float2 FP[NP], FH[NP];
+            if constexpr (ADJ) {
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    FP[p] = make_float2(wv[2 * p] * pf[2 * p], wv[2 * p + 1] * pf[2 * p + 1]);
+                    FH[p] = make_float2(wv[2 * p] * hf[2 * p], wv[2 * p + 1] * hf[2 * p + 1]);
+                }
+            }
             float2 AP[NP], AH[NP];
 #pragma unroll
             for (int p = 0; p < NP; ++p) AP[p] = AH[p] = make_float2(0.0f, 0.0f);
@@ -564,8 +613,10 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                         n1 += s_wcount_h[c][w];
                     }
                     if (cls[c]) {
+                        // the adjoint keeps the spot's index where the dose keeps its weight
+                        const int si = s0 + base + c * kThreads + threadIdx.x;
                         const float w =
-                            COUNT ? 0.0f : __ldg(mu + s0 + base + c * kThreads + threadIdx.x);
+                            MODE == kModeDose ? __ldg(mu + si) : __int_as_float(si);
                         SpotRec r;
                         r.a = make_float4(-ga[c].x, -ga[c].x, -ga[c].y, -ga[c].y);
                         r.b = make_float4(ga[c].z, ga[c].z, -ga[c].w, -ga[c].w);
@@ -578,6 +629,59 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                 if constexpr (COUNT) {
                     n_ex2 += 512ull * (unsigned long long)(2 * n2 + n1);
                     n_eval += 512ull * (unsigned long long)(n2 + n1);
+                } else if constexpr (ADJ) {
+                    // both terms: slots [0, n2); halo only: [kCap - n1, kCap);
+                    // a group's slots past its class hold other records or
+                    // padding, and their sums are dropped
+                    for (int c0 = 0; c0 < n2; c0 += 8) {
+                        float v[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const SpotRec r = s_spot[c0 + k];
+                            float2 t = make_float2(0.0f, 0.0f);
+#pragma unroll
+                            for (int p = 0; p < NP; ++p) {
+                                const float2 qq = axis_r2(lo2(r.a), hi2(r.a), lo2(r.b), hi2(r.b),
+                                                          lo2(r.c), hi2(r.c), XP[p], YP[p],
+                                                          GXP[p], GYP[p]);
+                                t = __ffma2_rn(FP[p], ex2x2(__fmul2_rn(PS[p], qq)), t);
+                                t = __ffma2_rn(FH[p], ex2x2(__fmul2_rn(HS[p], qq)), t);
+                            }
+                            v[k] = t.x + t.y;
+                        }
+                        int slot;
+                        const float sum = warp_sum8(v, lane, slot);
+                        if ((lane & 3) == 0 && c0 + slot < n2 && sum != 0.0f)
+                            atomicAdd(&sh.gsum[c0 + slot], sum);
+                    }
+                    for (int c0 = kCap - n1; c0 < kCap; c0 += 8) {
+                        float v[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const SpotRec r = s_spot[c0 + k];
+                            float2 t = make_float2(0.0f, 0.0f);
+#pragma unroll
+                            for (int p = 0; p < NP; ++p) {
+                                const float2 qq = axis_r2(lo2(r.a), hi2(r.a), lo2(r.b), hi2(r.b),
+                                                          lo2(r.c), hi2(r.c), XP[p], YP[p],
+                                                          GXP[p], GYP[p]);
+                                t = __ffma2_rn(FH[p], ex2x2(__fmul2_rn(HS[p], qq)), t);
+                            }
+                            v[k] = t.x + t.y;
+                        }
+                        int slot;
+                        const float sum = warp_sum8(v, lane, slot);
+                        if ((lane & 3) == 0 && c0 + slot < kCap && sum != 0.0f)
+                            atomicAdd(&sh.gsum[c0 + slot], sum);
+                    }
+                    __syncthreads();
+                    // each surviving spot's tile sum to its gradient
+                    for (int c = threadIdx.x; c < n2 + n1; c += kThreads) {
+                        const int sl = c < n2 ? c : kCap - n1 + (c - n2);
+                        const float a = sh.gsum[sl];
+                        if (a != 0.0f) atomicAdd(grad + __float_as_int(s_spot[sl].d.x), a);
+                        sh.gsum[sl] = 0.0f;
+                    }
                 } else {
 #pragma unroll 2
                     for (int c = 0; c < n2; ++c) {
@@ -607,14 +711,16 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                 }
                 __syncthreads();
             }
+            if constexpr (!ADJ) {
 #pragma unroll
-            for (int q = 0; q < kVpt; ++q) {
-                if (act[q]) {
-                    const float ap = (q & 1) ? AP[q >> 1].y : AP[q >> 1].x;
-                    const float ah = (q & 1) ? AH[q >> 1].y : AH[q >> 1].x;
-                    const float ld = fmaf(pf[q], ap, hf[q] * ah);
-                    if (BEAM_OUT) neumaier(bs_s[q], bs_c[q], ld);
-                    neumaier(tot_s[q], tot_c[q], ld);
+                for (int q = 0; q < kVpt; ++q) {
+                    if (act[q]) {
+                        const float ap = (q & 1) ? AP[q >> 1].y : AP[q >> 1].x;
+                        const float ah = (q & 1) ? AH[q >> 1].y : AH[q >> 1].x;
+                        const float ld = fmaf(pf[q], ap, hf[q] * ah);
+                        if (BEAM_OUT) neumaier(bs_s[q], bs_c[q], ld);
+                        neumaier(tot_s[q], tot_c[q], ld);
+                    }
                 }
             }
         }
@@ -630,7 +736,7 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
             atomicAdd(count, n_ex2);
             atomicAdd(count + 1, n_eval);
         }
-    } else {
+    } else if constexpr (!ADJ) {
 #pragma unroll
         for (int q = 0; q < kVpt; ++q)
             if (valid[q]) dose[vidx[q]] = (tot_s[q] + tot_c[q]) * A.scale;
@@ -662,8 +768,19 @@ k_dose_count(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
              unsigned long long *count)
 {
     __shared__ DoseShared<128, 2> sh;
-    dose_tile<128, 4, 2, false, true>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr, nullptr,
-                                      sh, count);
+    dose_tile<128, 4, 2, false, kModeCount>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr,
+                                            nullptr, sh, count);
+}
+
+// Spot-weight gradient: dose_tile in adjoint mode, shape of pb_dose's kernel.
+__global__ void __launch_bounds__(128, dose_min_blocks<128>())
+k_adjoint_tile(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+               const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
+               const float *__restrict__ wfield, float *__restrict__ grad)
+{
+    __shared__ DoseShared<128, 2> sh;
+    dose_tile<128, 4, 2, false, kModeAdjoint>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr,
+                                              nullptr, sh, nullptr, wfield, grad);
 }
 
 // SFU exp2 throughput: kEx2Chains independent chains x <- 2^(-x) per
@@ -723,273 +840,6 @@ k_dose_batch(const BatchDose *__restrict__ plans, int n_plans, long long n_items
         dose_tile<NT, VPT, KCULL, false>(D.A, (int)(it - D.tile_start), D.wet, D.layers, D.geo,
                                          D.mu, D.dose, nullptr, sh);
         __syncthreads();
-    }
-}
-
-// ------------------------------------------------------------------ adjoint
-
-__global__ void __launch_bounds__(kAdjThreads, PB_ADJ_MIN_BLOCKS)
-k_adjoint(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
-          const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
-          const float *__restrict__ wfield, float *__restrict__ grad)
-{
-    __shared__ float s_dep[PB_MAX_LUT_LEN], s_sig[PB_MAX_LUT_LEN], s_idd[PB_MAX_LUT_LEN];
-    constexpr int kWarps = kAdjThreads / 32;
-    extern __shared__ __align__(16) unsigned char s_dyn[];   // kAdjDynSmem bytes
-    VoxRec *s_vox = reinterpret_cast<VoxRec *>(s_dyn);       // kAdjThreads * kAdjVpt
-    // Candidate spots of one compaction round: index, gradient partial and
-    // the geometry terms of axis_r2 (negated where axis_r2 wants them so),
-    // one array per term so that four consecutive spots are one float4 load
-    // each.  The halo-only class starts at a multiple of four; the slots
-    // between the classes are padding.
-    constexpr int kCand = kAdjThreads * kSpt + 8;
-    __shared__ int s_cand[kCand];
-    __shared__ float s_gsum[kCand];
-    __shared__ __align__(16) float s_cg[6][kCand];
-    __shared__ float s_red[kWarps][kRedSlots];
-    __shared__ int s_wcount[kAdjVpt > kSpt ? kAdjVpt : kSpt][kWarps];
-    __shared__ int s_wcount_h[kSpt][kWarps];
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int vi[kAdjVpt], vj[kAdjVpt], vk[kAdjVpt];
-    bool valid[kAdjVpt];
-    int vidx[kAdjVpt];
-    tile_voxels<kAdjVpt>(A, blockIdx.x, vi, vj, vk, valid, vidx);
-    const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
-    float wv[kAdjVpt];
-    bool anyw = false;
-#pragma unroll
-    for (int q = 0; q < kAdjVpt; ++q) {
-        wv[q] = valid[q] ? __ldg(wfield + vidx[q]) * A.scale : 0.0f;
-        anyw |= (wv[q] != 0.0f);
-    }
-    if (!__syncthreads_or(anyw)) return;
-    for (int c = threadIdx.x; c < kCand; c += kAdjThreads) {
-        s_gsum[c] = 0.0f;
-        for (int t = 0; t < 6; ++t) s_cg[t][c] = 0.0f;   // padding slots stay finite
-    }
-
-    for (int b = 0; b < A.n_beams; ++b) {
-        const PbBeam &B = A.beams[b];
-        float X[kAdjVpt], Y[kAdjVpt], Z[kAdjVpt], GX[kAdjVpt], GY[kAdjVpt], WMM[kAdjVpt];
-#pragma unroll
-        for (int q = 0; q < kAdjVpt; ++q) {
-            if (valid[q]) {
-                voxel_head(A.g, B, vi[q], vj[q], vk[q], X[q], Y[q], Z[q], GX[q], GY[q]);
-                WMM[q] = __fmul_rn(__ldg(wet + b * V + vidx[q]), 10.0f);
-            } else {
-                X[q] = Y[q] = Z[q] = 0.0f;
-                GX[q] = GY[q] = 1.0f;
-                WMM[q] = INFINITY;
-            }
-        }
-        float D[kAdjVpt];
-#pragma unroll
-        for (int q = 0; q < kAdjVpt; ++q)
-            D[q] = valid[q] ? source_distance(B, X[q], Y[q], Z[q]) : 0.0f;
-        const TileBounds tb = tile_bounds<kAdjVpt, kAdjThreads>(X, Y, GX, GY, D, WMM, valid, s_red);
-
-        for (int l = 0; l < B.n_layers; ++l) {
-            const PbLayer L = layers[B.layer_start + l];
-            const float cut = __fmul_rn(1.1f, L.r80);
-            if (layer_skip(L, tb, B, cut)) continue;   // uniform over the block
-            bool act[kAdjVpt];
-            bool any = false;
-#pragma unroll
-            for (int q = 0; q < kAdjVpt; ++q) {
-                act[q] = valid[q] && wv[q] != 0.0f && !(WMM[q] > cut);
-                any |= act[q];
-            }
-            if (!__syncthreads_or(any)) continue;
-            // Compaction slots of the active voxels (order q, warp, lane).
-            unsigned mq[kAdjVpt];
-#pragma unroll
-            for (int q = 0; q < kAdjVpt; ++q) {
-                mq[q] = __ballot_sync(0xffffffffu, act[q]);
-                if (lane == 0) s_wcount[q][warp] = __popc(mq[q]);
-            }
-            stage_lut<kAdjThreads>(B, L.energy_id, s_dep, s_sig, s_idd);
-            __syncthreads();
-            int nact = 0, pos[kAdjVpt];
-#pragma unroll
-            for (int q = 0; q < kAdjVpt; ++q) {
-                pos[q] = 0;
-                for (int w = 0; w < kWarps; ++w) {
-                    if (w == warp) pos[q] = nact + __popc(mq[q] & ((1u << lane) - 1u));
-                    nact += s_wcount[q][w];
-                }
-            }
-            const LayerK K = layer_consts(
-                L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, s_dep, B.lut_len);
-            float hmax = -INFINITY, pmax = -INFINITY;
-#pragma unroll
-            for (int q = 0; q < kAdjVpt; ++q) {
-                if (act[q]) {
-                    float pf, hf, ps2, hs2;
-                    layer_params(WMM[q], source_distance(B, X[q], Y[q], Z[q]), K, s_dep, s_sig,
-                                 s_idd, B.lut_len, pf, hf, ps2, hs2);
-                    hmax = fmaxf(hmax, hs2);
-                    pmax = fmaxf(pmax, ps2);
-                    VoxRec r;
-                    r.xy = make_float4(X[q], X[q], Y[q], Y[q]);
-                    r.g = make_float4(GX[q], GX[q], GY[q], GY[q]);
-                    r.s = make_float4(ps2, ps2, hs2, hs2);
-                    const float a = wv[q] * pf, h = wv[q] * hf;
-                    r.f = make_float4(a, a, h, h);
-                    s_vox[pos[q]] = r;
-                }
-            }
-            // includes the barrier that publishes s_vox and frees s_wcount
-            float nhs, nps;
-            block_max2<kAdjThreads>(hmax, pmax, s_red, nhs, nps);
-            nhs = -nhs;
-            nps = -nps;
-
-            // Candidates: spots with both terms first (n2), then halo-only
-            // spots (n1); cull_class as in the forward.
-            const int s0 = B.spot_start + L.spot_start;
-            for (int base = 0; base < L.n_spots; base += kAdjThreads * kSpt) {
-                int cls[kSpt];
-                unsigned m2[kSpt], m1[kSpt];
-                float4 ga[kSpt], gb[kSpt];
-#pragma unroll
-                for (int c = 0; c < kSpt; ++c) {
-                    const int si = base + c * kAdjThreads + threadIdx.x;
-                    cls[c] = 0;
-                    if (si < L.n_spots) {
-                        ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
-                        gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                        cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, gb[c].y, tb), nhs, nps);
-                    }
-                    m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
-                    m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
-                    if (lane == 0) {
-                        s_wcount[c][warp] = __popc(m2[c]);
-                        s_wcount_h[c][warp] = __popc(m1[c]);
-                    }
-                }
-                __syncthreads();
-                int n2 = 0;
-#pragma unroll
-                for (int c = 0; c < kSpt; ++c)
-                    for (int w = 0; w < kWarps; ++w) n2 += s_wcount[c][w];
-                const int f1 = (n2 + 3) & ~3;   // first halo-only slot
-                int c2 = 0, c1 = f1;
-                const unsigned below = (1u << lane) - 1u;
-#pragma unroll
-                for (int c = 0; c < kSpt; ++c) {
-                    int pos2 = 0, pos1 = 0;
-                    for (int w = 0; w < kWarps; ++w) {
-                        if (w == warp) {
-                            pos2 = c2 + __popc(m2[c] & below);
-                            pos1 = c1 + __popc(m1[c] & below);
-                        }
-                        c2 += s_wcount[c][w];
-                        c1 += s_wcount_h[c][w];
-                    }
-                    if (cls[c]) {
-                        const int at = cls[c] == 2 ? pos2 : pos1;
-                        s_cand[at] = s0 + base + c * kAdjThreads + threadIdx.x;
-                        s_cg[0][at] = -ga[c].x;
-                        s_cg[1][at] = -ga[c].y;
-                        s_cg[2][at] = ga[c].z;
-                        s_cg[3][at] = -ga[c].w;
-                        s_cg[4][at] = -gb[c].x;
-                        s_cg[5][at] = gb[c].y;
-                    }
-                }
-                const int total = c1;   // slots used, padding included
-                __syncthreads();
-                // Two passes, both-term spots then halo-only spots, each over
-                // work items (four spots, voxel stripe) so that every thread is
-                // busy even when few spots survive the culling; each voxel
-                // record read from shared memory serves four spots as two
-                // packed pairs.  A group's slots past the class's last spot
-                // (padding or the next class) hold finite values and their
-                // sums are dropped.  Partial sums meet in shared memory, then
-                // one atomic per spot goes to global.
-#pragma unroll 1
-                for (int pass = 0; pass < 2; ++pass) {
-                    const int first = pass ? f1 : 0, cnt = pass ? total - f1 : n2;
-                    const int nq = (cnt + 3) >> 2;
-                    if (nq == 0) continue;
-                    const int stripes = nq >= kAdjThreads ? 1 : kAdjThreads / nq;
-                    const int items = nq * stripes;
-                    for (int it = threadIdx.x; it < items; it += kAdjThreads) {
-                        const int sq = it % nq, vs = it / nq;
-                        const int c0 = first + 4 * sq;
-                        const float4 g0 = *reinterpret_cast<const float4 *>(&s_cg[0][c0]);
-                        const float4 g1 = *reinterpret_cast<const float4 *>(&s_cg[1][c0]);
-                        const float4 g2 = *reinterpret_cast<const float4 *>(&s_cg[2][c0]);
-                        const float4 g3 = *reinterpret_cast<const float4 *>(&s_cg[3][c0]);
-                        const float4 g4 = *reinterpret_cast<const float4 *>(&s_cg[4][c0]);
-                        const float4 g5 = *reinterpret_cast<const float4 *>(&s_cg[5][c0]);
-                        const float2 nxa = lo2(g0), nya = lo2(g1), txa = lo2(g2), ntya = lo2(g3),
-                                     ncsa = lo2(g4), it2a = lo2(g5);
-                        const float2 nxb = hi2(g0), nyb = hi2(g1), txb = hi2(g2), ntyb = hi2(g3),
-                                     ncsb = hi2(g4), it2b = hi2(g5);
-                        float2 ha = make_float2(0.0f, 0.0f), hb = ha;
-                        int c = vs;
-                        if (pass == 0) {
-                            float2 pa = ha, pb = ha;
-                            for (; c < nact; c += stripes) {
-                                const VoxRec v = s_vox[c];
-                                const float2 qa = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
-                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
-                                const float2 qb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
-                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
-                                pa = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qa)), pa);
-                                ha = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qa)), ha);
-                                pb = __ffma2_rn(lo2(v.f), ex2x2(__fmul2_rn(lo2(v.s), qb)), pb);
-                                hb = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qb)), hb);
-                            }
-                            ha = __fadd2_rn(ha, pa);
-                            hb = __fadd2_rn(hb, pb);
-                        } else {
-                            float2 ha1 = ha, hb1 = ha;
-                            for (; c + stripes < nact; c += 2 * stripes) {
-                                const VoxRec v = s_vox[c], u = s_vox[c + stripes];
-                                const float2 qa = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
-                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
-                                const float2 qb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
-                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
-                                const float2 ra = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
-                                                          lo2(u.xy), hi2(u.xy), lo2(u.g), hi2(u.g));
-                                const float2 rb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
-                                                          lo2(u.xy), hi2(u.xy), lo2(u.g), hi2(u.g));
-                                ha = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qa)), ha);
-                                hb = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qb)), hb);
-                                ha1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), ra)), ha1);
-                                hb1 = __ffma2_rn(hi2(u.f), ex2x2(__fmul2_rn(hi2(u.s), rb)), hb1);
-                            }
-                            if (c < nact) {
-                                const VoxRec v = s_vox[c];
-                                const float2 qa = axis_r2(nxa, nya, txa, ntya, ncsa, it2a,
-                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
-                                const float2 qb = axis_r2(nxb, nyb, txb, ntyb, ncsb, it2b,
-                                                          lo2(v.xy), hi2(v.xy), lo2(v.g), hi2(v.g));
-                                ha = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qa)), ha);
-                                hb = __ffma2_rn(hi2(v.f), ex2x2(__fmul2_rn(hi2(v.s), qb)), hb);
-                            }
-                            ha = __fadd2_rn(ha, ha1);
-                            hb = __fadd2_rn(hb, hb1);
-                        }
-                        const float sum[4] = {ha.x, ha.y, hb.x, hb.y};
-#pragma unroll
-                        for (int h = 0; h < 4; ++h)
-                            if (sum[h] != 0.0f && 4 * sq + h < cnt) atomicAdd(&s_gsum[c0 + h], sum[h]);
-                    }
-                }
-                __syncthreads();
-                for (int c = threadIdx.x; c < total; c += kAdjThreads) {
-                    const float a = s_gsum[c];
-                    if (a != 0.0f) atomicAdd(grad + s_cand[c], a);   // padding stays 0
-                    s_gsum[c] = 0.0f;
-                }
-                __syncthreads();
-            }
-        }
-        __syncthreads();  // s_red is rewritten by the next beam's tile_bounds
     }
 }
 
@@ -1291,16 +1141,10 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                             "cudaMemsetAsync(grad)");
     if (s != PB_OK) return s;
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
-    // the voxel records are dynamic shared memory: with the static arrays
-    // they exceed the 48 KB a launch gets without opting in
-    s = check_cuda(cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        kAdjDynSmem),
-                   "cudaFuncSetAttribute(k_adjoint)");
-    if (s != PB_OK) return s;
-    k_adjoint<<<(unsigned)tiles, kAdjThreads, kAdjDynSmem, st>>>(A, wet, layers,
+    k_adjoint_tile<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers,
                                                     reinterpret_cast<const float4 *>(geo), w,
                                                     grad);
-    return check_launch("k_adjoint");
+    return check_launch("k_adjoint_tile");
 }
 
 size_t objective_work_size() { return sizeof(double) * kObjBlocks; }
