@@ -98,20 +98,20 @@ __device__ __forceinline__ LayerK layer_consts(float r80, const float *cabc, con
 {
     LayerK K;
     K.r80 = r80;
-    K.off = 0.7f * r80;
+    K.off = __fmul_rn(0.7f, r80);
     K.ca = __ldg(cabc);
     K.cb = __ldg(cabc + 1);
     K.cc = __ldg(cabc + 2);
     K.d0 = s_dep[0];
-    const float step = lut_len > 1 ? s_dep[1] - s_dep[0] : 0.0f;
-    K.inv_step = step > 0.0f ? 1.0f / step : 0.0f;
-    K.c_log = 0.0014f * r80;
-    K.c_sh = 0.22f * r80;
-    K.k_wh = 1.0f / (11.2f - 0.023f * r80);
-    K.c_wh = 0.35f * (0.0017f * r80 * r80 - r80);
-    const float r3 = r80 + 3.0f;
-    K.r3sq = r3 * r3;
-    K.c_lin = 1.61e-9f * K.r3sq;
+    const float step = lut_len > 1 ? __fsub_rn(s_dep[1], s_dep[0]) : 0.0f;
+    K.inv_step = step > 0.0f ? __fdiv_rn(1.0f, step) : 0.0f;
+    K.c_log = __fmul_rn(0.0014f, r80);
+    K.c_sh = __fmul_rn(0.22f, r80);
+    K.k_wh = __fdiv_rn(1.0f, __fsub_rn(11.2f, __fmul_rn(0.023f, r80)));
+    K.c_wh = __fmul_rn(0.35f, __fsub_rn(__fmul_rn(__fmul_rn(0.0017f, r80), r80), r80));
+    const float r3 = __fadd_rn(r80, 3.0f);
+    K.r3sq = __fmul_rn(r3, r3);
+    K.c_lin = __fmul_rn(1.61e-9f, K.r3sq);
     return K;
 }
 
@@ -125,12 +125,15 @@ __device__ __forceinline__ LayerK layer_consts(float r80, const float *cabc, con
 // it is that row, so any ascending depth table gives the binary search's
 // row.  The halo closed forms (IMPTClasses.cu:104-121) and the Gaussian
 // prefactors use the SFU's log2 and reciprocal (relative error ~1e-7).
+// Every operation is an explicitly rounded intrinsic, so that no
+// instantiation of the tile code contracts them differently: all kernel
+// shapes give the same bits.
 __device__ __forceinline__ void layer_params(float wet_mm, float dist, const LayerK &K,
                                              const float *s_dep, const float *s_sig,
                                              const float *s_idd, int lut_len, float &pf,
                                              float &hf, float &ps2, float &hs2)
 {
-    const float gs = ceilf((wet_mm - K.d0) * K.inv_step);
+    const float gs = ceilf(__fmul_rn(__fsub_rn(wet_mm, K.d0), K.inv_step));
     int lo = gs > 0.0f ? (gs < (float)lut_len ? (int)gs : lut_len) : 0;
     if (wet_mm != wet_mm) lo = lut_len;   // NaN compares false: the search ends high
     while (lo > 0 && s_dep[lo - 1] >= wet_mm) --lo;
@@ -143,28 +146,32 @@ __device__ __forceinline__ void layer_params(float wet_mm, float dist, const Lay
         idd = s_idd[0];
         sms = s_sig[0];
     } else {
-        const float f = __fdividef(wet_mm - s_dep[lo - 1], s_dep[lo] - s_dep[lo - 1]);
-        idd = fmaf(s_idd[lo] - s_idd[lo - 1], f, s_idd[lo - 1]);
-        sms = fmaf(s_sig[lo] - s_sig[lo - 1], f, s_sig[lo - 1]);
+        const float f = __fdividef(__fsub_rn(wet_mm, s_dep[lo - 1]),
+                                   __fsub_rn(s_dep[lo], s_dep[lo - 1]));
+        idd = __fmaf_rn(__fsub_rn(s_idd[lo], s_idd[lo - 1]), f, s_idd[lo - 1]);
+        sms = __fmaf_rn(__fsub_rn(s_sig[lo], s_sig[lo - 1]), f, s_sig[lo - 1]);
     }
-    const float d = dist - wet_mm + K.off;
-    const float st = fmaf(fmaf(K.ca, d, K.cb), d, K.cc) + sms;
-    const float w = fminf(fmaxf(wet_mm, 0.1f), K.r80 - 0.1f);
-    const float a1 = w - K.r80 - 5.0f;
-    float sh = 2.85f + K.c_log * __logf(w + 3.0f) + 0.06f * w - 7.4e-5f * w * w -
-               __fdividef(K.c_sh, a1 * a1);
-    float wh = 0.052f * __logf(fmaf(w, K.k_wh, 1.13f)) +
-               __fdividef(K.c_wh, K.r3sq - w * w) - K.c_lin * w;
+    const float d = __fadd_rn(__fsub_rn(dist, wet_mm), K.off);
+    const float st = __fadd_rn(__fmaf_rn(__fmaf_rn(K.ca, d, K.cb), d, K.cc), sms);
+    const float w = fminf(fmaxf(wet_mm, 0.1f), __fsub_rn(K.r80, 0.1f));
+    const float a1 = __fsub_rn(__fsub_rn(w, K.r80), 5.0f);
+    float sh = __fadd_rn(2.85f, __fmul_rn(K.c_log, __logf(__fadd_rn(w, 3.0f))));
+    sh = __fadd_rn(sh, __fmul_rn(0.06f, w));
+    sh = __fsub_rn(sh, __fmul_rn(__fmul_rn(7.4e-5f, w), w));
+    sh = __fsub_rn(sh, __fdividef(K.c_sh, __fmul_rn(a1, a1)));
+    float wh = __fmul_rn(0.052f, __logf(__fmaf_rn(w, K.k_wh, 1.13f)));
+    wh = __fadd_rn(wh, __fdividef(K.c_wh, __fsub_rn(K.r3sq, __fmul_rn(w, w))));
+    wh = __fsub_rn(wh, __fmul_rn(K.c_lin, w));
     sh = fmaxf(sh, 0.0f);
     wh = fminf(fmaxf(wh, 0.0f), 0.9f);
-    const float st2 = st * st;
-    const float sht2 = fmaf(sh, sh, st2);
+    const float st2 = __fmul_rn(st, st);
+    const float sht2 = __fmaf_rn(sh, sh, st2);
     const float rp = __fdividef(1.0f, st2), rh = __fdividef(1.0f, sht2);
-    const float iddn = idd * (1.0f / kTwoPi);
-    pf = (1.0f - wh) * iddn * rp;
-    hf = wh * iddn * rh;
-    ps2 = st2 != 0.0f ? (-0.5f * kLog2e) * rp : -INFINITY;
-    hs2 = sht2 != 0.0f ? (-0.5f * kLog2e) * rh : -INFINITY;
+    const float iddn = __fmul_rn(idd, 1.0f / kTwoPi);
+    pf = __fmul_rn(__fmul_rn(__fsub_rn(1.0f, wh), iddn), rp);
+    hf = __fmul_rn(__fmul_rn(wh, iddn), rh);
+    ps2 = st2 != 0.0f ? __fmul_rn(-0.5f * kLog2e, rp) : -INFINITY;
+    hs2 = sht2 != 0.0f ? __fmul_rn(-0.5f * kLog2e, rh) : -INFINITY;
 }
 
 // Squared distance (times 1/|t|^2) from the spot's axis to the tile's BEV
@@ -177,7 +184,7 @@ __device__ __forceinline__ float cull_r2(float xs, float ys, float it2, const Ti
     const float q0 = ys * tb.gy0, q1 = ys * tb.gy1;
     const float loy = tb.y0 - fmaxf(q0, q1), hiy = tb.y1 - fminf(q0, q1);
     const float dy = fmaxf(0.0f, fmaxf(loy, -hiy));
-    return (dx * dx + dy * dy) * it2;
+    return __fmul_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), it2);
 }
 
 // Spot classes per tile and layer: the halo term is below 2^-24 of its
@@ -351,8 +358,8 @@ __device__ __forceinline__ void voxel_head(const PbGrid &g, const PbBeam &B, int
 // frame (CudaClasses.cu:17-51 rotated into the nozzle frame).
 __device__ __forceinline__ float source_distance(const PbBeam &B, float X, float Y, float Z)
 {
-    const float dz = 0.5f * (B.geom.vsadx + B.geom.vsady) - Z;
-    return sqrtf(fmaf(X, X, fmaf(Y, Y, dz * dz)));
+    const float dz = __fsub_rn(__fmul_rn(0.5f, __fadd_rn(B.geom.vsadx, B.geom.vsady)), Z);
+    return sqrtf(__fmaf_rn(X, X, __fmaf_rn(Y, Y, __fmul_rn(dz, dz))));
 }
 
 template <int NT>
@@ -533,21 +540,27 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
             float pf[kVpt], hf[kVpt];
             float2 PS[NP], HS[NP];
             float hmax = -INFINITY, pmax = -INFINITY;
+            // every voxel's parameters without branching, so that the four
+            // voxels' dependent chains overlap; inactive voxels take a
+            // harmless depth and are masked out afterwards
 #pragma unroll
             for (int q = 0; q < kVpt; ++q) {
-                float ps2 = 0.0f, hs2 = 0.0f;
-                pf[q] = hf[q] = 0.0f;
-                if (act[q]) {
+                float ps2, hs2;
+                {
                     const int p = q >> 1;
                     const float X = (q & 1) ? XP[p].y : XP[p].x;
                     const float Y = (q & 1) ? YP[p].y : YP[p].x;
                     const float gx = (q & 1) ? GXP[p].y : GXP[p].x;
-                    const float w = (q & 1) ? WP[p].y : WP[p].x;
+                    const float w = act[q] ? ((q & 1) ? WP[p].y : WP[p].x) : 0.0f;
                     const float Z = B.geom.vsadx * (1.0f - gx);
                     layer_params(w, source_distance(B, X, Y, Z), K, s_dep, s_sig, s_idd,
                                  B.lut_len, pf[q], hf[q], ps2, hs2);
+                }
+                if (act[q]) {
                     hmax = fmaxf(hmax, hs2);
                     pmax = fmaxf(pmax, ps2);
+                } else {
+                    pf[q] = hf[q] = ps2 = hs2 = 0.0f;
                 }
                 if (q & 1) {
                     PS[q >> 1].y = ps2;
