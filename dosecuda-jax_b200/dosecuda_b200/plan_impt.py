@@ -297,4 +297,48 @@ class IMPTPlan(Plan):
         raise NotImplementedError("writePlanDicom writes DICOM through pydicom")
 
     def readPlanDicom(self, plan_path):
-        raise NotImplementedError("readPlanDicom reads DICOM through pydicom")
+        """Beams and spots of an RT Ion Plan (plan_impt.py:635-674).
+
+        plan_path is a file, read with pydicom (which must then be
+        installed), or an RT Ion Plan dataset already read (any object with
+        the DICOM attributes used below).  Per beam: the range-shifter label
+        (RangeShifterSequence[0].RangeShifterID, else '0'), gantry, couch
+        and isocentre from the first control point, and the spots of every
+        even-numbered control point (the odd ones close each layer), with
+        the energy id of its NominalBeamEnergy in the first beam model.
+        The fraction count is FractionGroupSequence[0].NumberOfFractionsPlanned.
+        """
+        if isinstance(plan_path, (str, bytes, os.PathLike)):
+            try:
+                import pydicom
+            except ImportError as e:
+                raise ImportError("readPlanDicom needs pydicom to read a file; pass a dataset "
+                                  "already read instead") from e
+            ds = pydicom.dcmread(plan_path, force=True)
+        else:
+            ds = plan_path
+        n_beams = len(ds.IonBeamSequence)
+        self.n_fractions = float(ds.FractionGroupSequence[0].NumberOfFractionsPlanned)
+        self.beam_list = []
+        self.n_beams = 0
+        for i in range(n_beams):
+            ibs = ds.IonBeamSequence[i]
+            beam = IMPTBeam()
+            n_rs = getattr(ibs, "NumberOfRangeShifters", 0)
+            if n_rs and ibs.RangeShifterSequence[0].RangeShifterID is not None:
+                beam.dicom_rangeshifter_label = ibs.RangeShifterSequence[0].RangeShifterID
+            else:
+                beam.dicom_rangeshifter_label = '0'
+            cp0 = ibs.IonControlPointSequence[0]
+            beam.gantry_angle = float(cp0.GantryAngle)
+            beam.couch_angle = float(cp0.PatientSupportAngle)
+            beam.iso = np.array(cp0.IsocenterPosition, dtype=np.single)
+            if hasattr(ibs, "BeamName"):
+                beam.BeamName = ibs.BeamName
+            if hasattr(ibs, "BeamDescription"):
+                beam.BeamDescription = ibs.BeamDescription
+            for j in range(0, len(ibs.IonControlPointSequence), 2):
+                cp = ibs.IonControlPointSequence[j]
+                energy_id = self.beam_models[0].energyIDFromLabel(float(cp.NominalBeamEnergy))
+                beam.addSpotData(cp, energy_id)
+            self.addBeam(beam)

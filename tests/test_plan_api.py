@@ -190,3 +190,62 @@ def test_phantoms_are_seeded():
     c = phantoms.water_cube()
     assert c.grid.HU.shape == (120, 120, 120) and c.n_spots == 121 * 10
     assert (c.grid.HU == 0).sum() == 80 ** 3
+
+
+def _ion_plan_dataset(labels):
+    """A synthetic RT Ion Plan in the shape pydicom gives (attributes and
+    sequences): two beams, the second with range shifter '4'; control points
+    in pairs (layer start with spots, layer end), as planning systems write
+    them."""
+    ns = types.SimpleNamespace
+
+    def layer(energy, xy, mu, first=None):
+        cp = ns(NominalBeamEnergy=float(energy), ScanSpotPositionMap=list(np.ravel(xy)),
+                ScanSpotMetersetWeights=list(mu))
+        if first is not None:
+            cp.GantryAngle, cp.PatientSupportAngle, cp.IsocenterPosition = first
+        end = ns(NominalBeamEnergy=float(energy), ScanSpotPositionMap=list(np.ravel(xy)),
+                 ScanSpotMetersetWeights=[0.0] * len(mu))
+        return [cp, end]
+
+    b1 = ns(BeamName="RAO", NumberOfRangeShifters=0,
+            IonControlPointSequence=layer(labels[40], [[0, 0], [5, 0]], [1.0, 2.0],
+                                          (30.0, 0.0, [1.0, 2.0, 3.0]))
+            + layer(labels[45], [[0, 5]], [0.5]))
+    b2 = ns(BeamName="LAO", BeamDescription="second", NumberOfRangeShifters=1,
+            RangeShifterSequence=[ns(RangeShifterID="4")],
+            IonControlPointSequence=layer(labels[20], [[-5, -5], [5, 5], [0, 0]],
+                                          [1.0, 1.0, 3.0], (330.0, 90.0, [4.0, 5.0, 6.0])))
+    return ns(IonBeamSequence=[b1, b2],
+              FractionGroupSequence=[ns(NumberOfFractionsPlanned="30")])
+
+
+def test_read_plan_dicom_from_dataset(plan):
+    """readPlanDicom (plan_impt.py:635-674) on a dataset already read: beams,
+    angles, isocentres, range shifters, spots of the even control points with
+    their energy ids, and the fraction count."""
+    from dosecuda_b200.plan_impt import IMPTPlan
+    p = IMPTPlan()
+    labels = p.beam_models[0].energy_labels
+    p.readPlanDicom(_ion_plan_dataset(labels))
+    assert p.n_fractions == 30.0 and p.n_beams == 2
+    b1, b2 = p.beam_list
+    assert (b1.gantry_angle, b1.couch_angle) == (30.0, 0.0)
+    assert (b2.gantry_angle, b2.couch_angle) == (330.0, 90.0)
+    assert b1.iso.dtype == np.float32 and list(b1.iso) == [1.0, 2.0, 3.0]
+    assert b1.dicom_rangeshifter_label == "0" and b2.dicom_rangeshifter_label == "4"
+    assert b1.BeamName == "RAO" and b2.BeamDescription == "second"
+    assert b1.BeamDescription == "PBS_Beam 1"
+    assert b1.spot_list.dtype == np.float32 and b1.spot_list.shape == (3, 4)
+    assert np.array_equal(b1.spot_list, np.array([[0, 0, 1, 40], [5, 0, 2, 40], [0, 5, 0.5, 45]],
+                                                 np.float32))
+    assert b1.n_spots == 3 and b2.n_spots == 3
+    assert np.array_equal(b2.spot_list[:, 3], [20, 20, 20])
+
+
+def test_read_plan_dicom_file_needs_pydicom(plan, tmp_path):
+    import importlib.util
+    if importlib.util.find_spec("pydicom") is not None:
+        pytest.skip("pydicom is installed")
+    with pytest.raises(ImportError, match="pydicom"):
+        plan.readPlanDicom(str(tmp_path / "plan.dcm"))
