@@ -207,7 +207,8 @@ __device__ __forceinline__ void neumaier(float &s, float &c, float x)
 
 // Block-wide min/max of the tile's BEV box over valid voxels.
 // Block-wide box of the tile's valid voxels: BEV x, y and divergence
-// factors (min and max), distance to the source (min and max), 10*WET (min).
+// factors (min and max), distance to the source (min and max), 10*WET (min,
+// with NaN taken as -infinity).
 template <int NV, int NT>
 __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y,
                                                   const float *GX, const float *GY,
@@ -226,7 +227,7 @@ __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y
         v[4] = fminf(v[4], GX[q]); v[5] = fmaxf(v[5], GX[q]);
         v[6] = fminf(v[6], GY[q]); v[7] = fmaxf(v[7], GY[q]);
         v[8] = fminf(v[8], D[q]);  v[9] = fmaxf(v[9], D[q]);
-        v[10] = fminf(v[10], W[q]);
+        v[10] = fminf(v[10], W[q] == W[q] ? W[q] : -INFINITY);   // a NaN depth is never skipped
     }
     // slot m: odd = max, even = min
 #pragma unroll
@@ -294,8 +295,10 @@ __device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &t
                 a3 = L.sx1 * tb.gx1;
     const float b0 = L.sy0 * tb.gy0, b1 = L.sy0 * tb.gy1, b2 = L.sy1 * tb.gy0,
                 b3 = L.sy1 * tb.gy1;
-    const float pxl = fminf(fminf(a0, a1), fminf(a2, a3)), pxh = fmaxf(fmaxf(a0, a1), fmaxf(a2, a3));
-    const float pyl = fminf(fminf(b0, b1), fminf(b2, b3)), pyh = fmaxf(fmaxf(b0, b1), fmaxf(b2, b3));
+    const float pxl = fminf(fminf(a0, a1), fminf(a2, a3));
+    const float pxh = fmaxf(fmaxf(a0, a1), fmaxf(a2, a3));
+    const float pyl = fminf(fminf(b0, b1), fminf(b2, b3));
+    const float pyh = fmaxf(fmaxf(b0, b1), fmaxf(b2, b3));
     const float dx = fmaxf(0.0f, fmaxf(tb.x0 - pxh, pxl - tb.x1));
     const float dy = fmaxf(0.0f, fmaxf(tb.y0 - pyh, pyl - tb.y1));
     const float r2 = dx * dx + dy * dy;
@@ -308,7 +311,8 @@ __device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &t
     const float off = 0.7f * L.r80;
     const float dlo = tb.d0 - cut + off, dhi = tb.d1 - tb.w0 + off;
     if (!(dlo <= dhi)) return false;   // NaN or an empty tile: no decision
-    float q = fmaxf(fabsf(fmaf(fmaf(ca, dlo, cb), dlo, cc)), fabsf(fmaf(fmaf(ca, dhi, cb), dhi, cc)));
+    float q = fmaxf(fabsf(fmaf(fmaf(ca, dlo, cb), dlo, cc)),
+                    fabsf(fmaf(fmaf(ca, dhi, cb), dhi, cc)));
     if (ca != 0.0f) {
         const float dv = -cb / (2.0f * ca);
         if (dv > dlo && dv < dhi) q = fmaxf(q, fabsf(fmaf(fmaf(ca, dv, cb), dv, cc)));
@@ -391,6 +395,8 @@ struct DoseShared {
     float red[NT / 32][kRedSlots];
     int wcount[KCULL][NT / 32];
     int wcount_h[KCULL][NT / 32];
+    int lcount[NT / 32];          // layers kept per warp (one chunk of NT layers)
+    int lsel[NT];                 // the chunk's kept layers, in order
 };
 
 // Sum over the warp of eight per-lane values v[0..7] (one per spot) with a
@@ -505,7 +511,11 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                     D[q] = 0.0f;
                 }
             }
-            tb = tile_bounds<kVpt, kThreads>(X, Y, GX, GY, D, W, valid, s_red);
+            // the least depth only over voxels that can be active
+            float Wa[kVpt];
+#pragma unroll
+            for (int q = 0; q < kVpt; ++q) Wa[q] = (ADJ && wv[q] == 0.0f) ? INFINITY : W[q];
+            tb = tile_bounds<kVpt, kThreads>(X, Y, GX, GY, D, Wa, valid, s_red);
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
                 XP[p] = make_float2(X[2 * p], X[2 * p + 1]);
@@ -519,220 +529,245 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
 #pragma unroll
         for (int q = 0; q < kVpt; ++q) bs_s[q] = bs_c[q] = 0.0f;
 
-        for (int l = 0; l < B.n_layers; ++l) {
-            const PbLayer L = layers[B.layer_start + l];
-            const float cut = __fmul_rn(1.1f, L.r80);
-            if (layer_skip(L, tb, B, cut)) continue;   // uniform over the block
-            bool act[kVpt];
-            bool any = false;
-#pragma unroll
-            for (int q = 0; q < kVpt; ++q) {
-                const float w = (q & 1) ? WP[q >> 1].y : WP[q >> 1].x;
-                act[q] = valid[q] && !(w > cut);
-                if constexpr (ADJ) act[q] = act[q] && wv[q] != 0.0f;
-                any |= act[q];
+        // The layers that can reach the tile, found in parallel (one thread
+        // per layer, NT layers per chunk): some voxel that can be active
+        // lies within the range cut (the tile's least depth), and the
+        // layer's bounds do not rule out every spot (layer_skip).
+        for (int l0 = 0; l0 < B.n_layers; l0 += kThreads) {
+            __syncthreads();   // the previous chunk's list has been read
+            bool keep = false;
+            {
+                const int l = l0 + threadIdx.x;
+                if (l < B.n_layers) {
+                    const PbLayer L = layers[B.layer_start + l];
+                    const float cut = __fmul_rn(1.1f, L.r80);
+                    keep = tb.w0 <= cut && !layer_skip(L, tb, B, cut);
+                }
             }
-            if (!__syncthreads_or(any)) continue;
-            stage_lut<kThreads>(B, L.energy_id, s_dep, s_sig, s_idd);
+            const unsigned lm = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) sh.lcount[warp] = __popc(lm);
             __syncthreads();
-            const LayerK K = layer_consts(
-                L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, s_dep, B.lut_len);
-            float pf[kVpt], hf[kVpt];
-            float2 PS[NP], HS[NP];
-            float hmax = -INFINITY, pmax = -INFINITY;
-            // every voxel's parameters without branching, so that the four
-            // voxels' dependent chains overlap; inactive voxels take a
-            // harmless depth and are masked out afterwards
-#pragma unroll
-            for (int q = 0; q < kVpt; ++q) {
-                float ps2, hs2;
-                {
-                    const int p = q >> 1;
-                    const float X = (q & 1) ? XP[p].y : XP[p].x;
-                    const float Y = (q & 1) ? YP[p].y : YP[p].x;
-                    const float gx = (q & 1) ? GXP[p].y : GXP[p].x;
-                    const float w = act[q] ? ((q & 1) ? WP[p].y : WP[p].x) : 0.0f;
-                    const float Z = B.geom.vsadx * (1.0f - gx);
-                    layer_params(w, source_distance(B, X, Y, Z), K, s_dep, s_sig, s_idd,
-                                 B.lut_len, pf[q], hf[q], ps2, hs2);
-                }
-                if (act[q]) {
-                    hmax = fmaxf(hmax, hs2);
-                    pmax = fmaxf(pmax, ps2);
-                } else {
-                    pf[q] = hf[q] = ps2 = hs2 = 0.0f;
-                }
-                if (q & 1) {
-                    PS[q >> 1].y = ps2;
-                    HS[q >> 1].y = hs2;
-                } else {
-                    PS[q >> 1].x = ps2;
-                    HS[q >> 1].x = hs2;
-                }
+            int nsel = 0, lpos = 0;
+            for (int w = 0; w < kWarps; ++w) {
+                if (w == warp) lpos = nsel + __popc(lm & ((1u << lane) - 1u));
+                nsel += sh.lcount[w];
             }
-            float nhs, nps;
-            block_max2<kThreads>(hmax, pmax, s_red, nhs, nps);
-            nhs = -nhs;
-            nps = -nps;
-            // adjoint: the voxels' weighted prefactors as packed pairs
-            float2 FP[NP], FH[NP];
-            if constexpr (ADJ) {
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    FP[p] = make_float2(wv[2 * p] * pf[2 * p], wv[2 * p + 1] * pf[2 * p + 1]);
-                    FH[p] = make_float2(wv[2 * p] * hf[2 * p], wv[2 * p + 1] * hf[2 * p + 1]);
-                }
-            }
-            float2 AP[NP], AH[NP];
-#pragma unroll
-            for (int p = 0; p < NP; ++p) AP[p] = AH[p] = make_float2(0.0f, 0.0f);
-
-            // Spots with both terms are compacted to the front of s_spot,
-            // halo-only spots to the back.
-            constexpr int kCap = kThreads * kCull;
-            const int s0 = B.spot_start + L.spot_start;
-            for (int base = 0; base < L.n_spots; base += kCap) {
-                int cls[kCull];
-                float4 ga[kCull], gb[kCull];
-                unsigned m2[kCull], m1[kCull];
-#pragma unroll
-                for (int c = 0; c < kCull; ++c) {
-                    const int si = base + c * kThreads + threadIdx.x;
-                    cls[c] = 0;
-                    if (si < L.n_spots) {
-                        ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
-                        gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                        cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, gb[c].y, tb), nhs, nps);
-                    }
-                    m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
-                    m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
-                    if (lane == 0) {
-                        s_wcount[c][warp] = __popc(m2[c]);
-                        s_wcount_h[c][warp] = __popc(m1[c]);
-                    }
-                }
-                __syncthreads();
-                int n2 = 0, n1 = 0;
-                const unsigned below = (1u << lane) - 1u;
-#pragma unroll
-                for (int c = 0; c < kCull; ++c) {
-                    int pos2 = 0, pos1 = 0;
-                    for (int w = 0; w < kWarps; ++w) {
-                        if (w == warp) {
-                            pos2 = n2 + __popc(m2[c] & below);
-                            pos1 = n1 + __popc(m1[c] & below);
-                        }
-                        n2 += s_wcount[c][w];
-                        n1 += s_wcount_h[c][w];
-                    }
-                    if (cls[c]) {
-                        // the adjoint keeps the spot's index where the dose keeps its weight
-                        const int si = s0 + base + c * kThreads + threadIdx.x;
-                        const float w =
-                            MODE == kModeDose ? __ldg(mu + si) : __int_as_float(si);
-                        SpotRec r;
-                        r.a = make_float4(-ga[c].x, -ga[c].x, -ga[c].y, -ga[c].y);
-                        r.b = make_float4(ga[c].z, ga[c].z, -ga[c].w, -ga[c].w);
-                        r.c = make_float4(-gb[c].x, -gb[c].x, gb[c].y, gb[c].y);
-                        r.d = make_float4(w, w, 0.0f, 0.0f);
-                        s_spot[cls[c] == 2 ? pos2 : kCap - 1 - pos1] = r;
-                    }
-                }
-                __syncthreads();
-                if constexpr (COUNT) {
-                    n_ex2 += 512ull * (unsigned long long)(2 * n2 + n1);
-                    n_eval += 512ull * (unsigned long long)(n2 + n1);
-                } else if constexpr (ADJ) {
-                    // both terms: slots [0, n2); halo only: [kCap - n1, kCap);
-                    // a group's slots past its class hold other records or
-                    // padding, and their sums are dropped
-                    for (int c0 = 0; c0 < n2; c0 += 8) {
-                        float v[8];
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const SpotRec r = s_spot[c0 + k];
-                            float2 t = make_float2(0.0f, 0.0f);
-#pragma unroll
-                            for (int p = 0; p < NP; ++p) {
-                                const float2 qq = axis_r2(lo2(r.a), hi2(r.a), lo2(r.b), hi2(r.b),
-                                                          lo2(r.c), hi2(r.c), XP[p], YP[p],
-                                                          GXP[p], GYP[p]);
-                                t = __ffma2_rn(FP[p], ex2x2(__fmul2_rn(PS[p], qq)), t);
-                                t = __ffma2_rn(FH[p], ex2x2(__fmul2_rn(HS[p], qq)), t);
-                            }
-                            v[k] = t.x + t.y;
-                        }
-                        int slot;
-                        const float sum = warp_sum8(v, lane, slot);
-                        if ((lane & 3) == 0 && c0 + slot < n2 && sum != 0.0f)
-                            atomicAdd(&sh.gsum[c0 + slot], sum);
-                    }
-                    for (int c0 = kCap - n1; c0 < kCap; c0 += 8) {
-                        float v[8];
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const SpotRec r = s_spot[c0 + k];
-                            float2 t = make_float2(0.0f, 0.0f);
-#pragma unroll
-                            for (int p = 0; p < NP; ++p) {
-                                const float2 qq = axis_r2(lo2(r.a), hi2(r.a), lo2(r.b), hi2(r.b),
-                                                          lo2(r.c), hi2(r.c), XP[p], YP[p],
-                                                          GXP[p], GYP[p]);
-                                t = __ffma2_rn(FH[p], ex2x2(__fmul2_rn(HS[p], qq)), t);
-                            }
-                            v[k] = t.x + t.y;
-                        }
-                        int slot;
-                        const float sum = warp_sum8(v, lane, slot);
-                        if ((lane & 3) == 0 && c0 + slot < kCap && sum != 0.0f)
-                            atomicAdd(&sh.gsum[c0 + slot], sum);
-                    }
-                    __syncthreads();
-                    // each surviving spot's tile sum to its gradient
-                    for (int c = threadIdx.x; c < n2 + n1; c += kThreads) {
-                        const int sl = c < n2 ? c : kCap - n1 + (c - n2);
-                        const float a = sh.gsum[sl];
-                        if (a != 0.0f) atomicAdd(grad + __float_as_int(s_spot[sl].d.x), a);
-                        sh.gsum[sl] = 0.0f;
-                    }
-                } else {
-#pragma unroll 2
-                    for (int c = 0; c < n2; ++c) {
-                        const SpotRec r = s_spot[c];
-                        const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
-                                     ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
-#pragma unroll
-                        for (int p = 0; p < NP; ++p) {
-                            const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
-                                                      GXP[p], GYP[p]);
-                            AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS[p], qq)), AP[p]);
-                            AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
-                        }
-                    }
-#pragma unroll 2
-                    for (int c = kCap - n1; c < kCap; ++c) {
-                        const SpotRec r = s_spot[c];
-                        const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b), nty = hi2(r.b),
-                                     ncs = lo2(r.c), it2 = hi2(r.c), w = lo2(r.d);
-#pragma unroll
-                        for (int p = 0; p < NP; ++p) {
-                            const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
-                                                      GXP[p], GYP[p]);
-                            AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
-                        }
-                    }
-                }
-                __syncthreads();
-            }
-            if constexpr (!ADJ) {
+            if (keep) sh.lsel[lpos] = l0 + threadIdx.x;
+            __syncthreads();
+            for (int li = 0; li < nsel; ++li) {
+                const int l = sh.lsel[li];
+                const PbLayer L = layers[B.layer_start + l];
+                const float cut = __fmul_rn(1.1f, L.r80);
+                bool act[kVpt];
 #pragma unroll
                 for (int q = 0; q < kVpt; ++q) {
+                    const float w = (q & 1) ? WP[q >> 1].y : WP[q >> 1].x;
+                    act[q] = valid[q] && !(w > cut);
+                    if constexpr (ADJ) act[q] = act[q] && wv[q] != 0.0f;
+                }
+                stage_lut<kThreads>(B, L.energy_id, s_dep, s_sig, s_idd);
+                __syncthreads();
+                const LayerK K = layer_consts(
+                    L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, s_dep, B.lut_len);
+                float pf[kVpt], hf[kVpt];
+                float2 PS[NP], HS[NP];
+                float hmax = -INFINITY, pmax = -INFINITY;
+                // every voxel's parameters without branching, so that the four
+                // voxels' dependent chains overlap; inactive voxels take a
+                // harmless depth and are masked out afterwards
+#pragma unroll
+                for (int q = 0; q < kVpt; ++q) {
+                    float ps2, hs2;
+                    {
+                        const int p = q >> 1;
+                        const float X = (q & 1) ? XP[p].y : XP[p].x;
+                        const float Y = (q & 1) ? YP[p].y : YP[p].x;
+                        const float gx = (q & 1) ? GXP[p].y : GXP[p].x;
+                        const float w = act[q] ? ((q & 1) ? WP[p].y : WP[p].x) : 0.0f;
+                        const float Z = B.geom.vsadx * (1.0f - gx);
+                        layer_params(w, source_distance(B, X, Y, Z), K, s_dep, s_sig, s_idd,
+                                     B.lut_len, pf[q], hf[q], ps2, hs2);
+                    }
                     if (act[q]) {
-                        const float ap = (q & 1) ? AP[q >> 1].y : AP[q >> 1].x;
-                        const float ah = (q & 1) ? AH[q >> 1].y : AH[q >> 1].x;
-                        const float ld = fmaf(pf[q], ap, hf[q] * ah);
-                        if (BEAM_OUT) neumaier(bs_s[q], bs_c[q], ld);
-                        neumaier(tot_s[q], tot_c[q], ld);
+                        hmax = fmaxf(hmax, hs2);
+                        pmax = fmaxf(pmax, ps2);
+                    } else {
+                        pf[q] = hf[q] = ps2 = hs2 = 0.0f;
+                    }
+                    if (q & 1) {
+                        PS[q >> 1].y = ps2;
+                        HS[q >> 1].y = hs2;
+                    } else {
+                        PS[q >> 1].x = ps2;
+                        HS[q >> 1].x = hs2;
+                    }
+                }
+                float nhs, nps;
+                block_max2<kThreads>(hmax, pmax, s_red, nhs, nps);
+                nhs = -nhs;
+                nps = -nps;
+                // adjoint: the voxels' weighted prefactors as packed pairs
+                float2 FP[NP], FH[NP];
+                if constexpr (ADJ) {
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        FP[p] = make_float2(wv[2 * p] * pf[2 * p], wv[2 * p + 1] * pf[2 * p + 1]);
+                        FH[p] = make_float2(wv[2 * p] * hf[2 * p], wv[2 * p + 1] * hf[2 * p + 1]);
+                    }
+                }
+                float2 AP[NP], AH[NP];
+#pragma unroll
+                for (int p = 0; p < NP; ++p) AP[p] = AH[p] = make_float2(0.0f, 0.0f);
+
+                // Spots with both terms are compacted to the front of s_spot,
+                // halo-only spots to the back.
+                constexpr int kCap = kThreads * kCull;
+                const int s0 = B.spot_start + L.spot_start;
+                for (int base = 0; base < L.n_spots; base += kCap) {
+                    int cls[kCull];
+                    float4 ga[kCull], gb[kCull];
+                    unsigned m2[kCull], m1[kCull];
+#pragma unroll
+                    for (int c = 0; c < kCull; ++c) {
+                        const int si = base + c * kThreads + threadIdx.x;
+                        cls[c] = 0;
+                        if (si < L.n_spots) {
+                            ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
+                            gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
+                            cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, gb[c].y, tb), nhs, nps);
+                        }
+                        m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
+                        m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
+                        if (lane == 0) {
+                            s_wcount[c][warp] = __popc(m2[c]);
+                            s_wcount_h[c][warp] = __popc(m1[c]);
+                        }
+                    }
+                    __syncthreads();
+                    int n2 = 0, n1 = 0;
+                    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+                    for (int c = 0; c < kCull; ++c) {
+                        int pos2 = 0, pos1 = 0;
+                        for (int w = 0; w < kWarps; ++w) {
+                            if (w == warp) {
+                                pos2 = n2 + __popc(m2[c] & below);
+                                pos1 = n1 + __popc(m1[c] & below);
+                            }
+                            n2 += s_wcount[c][w];
+                            n1 += s_wcount_h[c][w];
+                        }
+                        if (cls[c]) {
+                            // the adjoint keeps the spot's index where the dose keeps its weight
+                            const int si = s0 + base + c * kThreads + threadIdx.x;
+                            const float w =
+                                MODE == kModeDose ? __ldg(mu + si) : __int_as_float(si);
+                            SpotRec r;
+                            r.a = make_float4(-ga[c].x, -ga[c].x, -ga[c].y, -ga[c].y);
+                            r.b = make_float4(ga[c].z, ga[c].z, -ga[c].w, -ga[c].w);
+                            r.c = make_float4(-gb[c].x, -gb[c].x, gb[c].y, gb[c].y);
+                            r.d = make_float4(w, w, 0.0f, 0.0f);
+                            s_spot[cls[c] == 2 ? pos2 : kCap - 1 - pos1] = r;
+                        }
+                    }
+                    __syncthreads();
+                    if constexpr (COUNT) {
+                        n_ex2 += 512ull * (unsigned long long)(2 * n2 + n1);
+                        n_eval += 512ull * (unsigned long long)(n2 + n1);
+                    } else if constexpr (ADJ) {
+                        // both terms: slots [0, n2); halo only: [kCap - n1, kCap);
+                        // a group's slots past its class hold other records or
+                        // padding, and their sums are dropped
+                        for (int c0 = 0; c0 < n2; c0 += 8) {
+                            float v[8];
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) {
+                                const SpotRec r = s_spot[c0 + k];
+                                float2 t = make_float2(0.0f, 0.0f);
+#pragma unroll
+                                for (int p = 0; p < NP; ++p) {
+                                    const float2 qq =
+                                        axis_r2(lo2(r.a), hi2(r.a), lo2(r.b), hi2(r.b), lo2(r.c),
+                                                hi2(r.c), XP[p], YP[p], GXP[p], GYP[p]);
+                                    t = __ffma2_rn(FP[p], ex2x2(__fmul2_rn(PS[p], qq)), t);
+                                    t = __ffma2_rn(FH[p], ex2x2(__fmul2_rn(HS[p], qq)), t);
+                                }
+                                v[k] = t.x + t.y;
+                            }
+                            int slot;
+                            const float sum = warp_sum8(v, lane, slot);
+                            if ((lane & 3) == 0 && c0 + slot < n2 && sum != 0.0f)
+                                atomicAdd(&sh.gsum[c0 + slot], sum);
+                        }
+                        for (int c0 = kCap - n1; c0 < kCap; c0 += 8) {
+                            float v[8];
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) {
+                                const SpotRec r = s_spot[c0 + k];
+                                float2 t = make_float2(0.0f, 0.0f);
+#pragma unroll
+                                for (int p = 0; p < NP; ++p) {
+                                    const float2 qq =
+                                        axis_r2(lo2(r.a), hi2(r.a), lo2(r.b), hi2(r.b), lo2(r.c),
+                                                hi2(r.c), XP[p], YP[p], GXP[p], GYP[p]);
+                                    t = __ffma2_rn(FH[p], ex2x2(__fmul2_rn(HS[p], qq)), t);
+                                }
+                                v[k] = t.x + t.y;
+                            }
+                            int slot;
+                            const float sum = warp_sum8(v, lane, slot);
+                            if ((lane & 3) == 0 && c0 + slot < kCap && sum != 0.0f)
+                                atomicAdd(&sh.gsum[c0 + slot], sum);
+                        }
+                        __syncthreads();
+                        // each surviving spot's tile sum to its gradient
+                        for (int c = threadIdx.x; c < n2 + n1; c += kThreads) {
+                            const int sl = c < n2 ? c : kCap - n1 + (c - n2);
+                            const float a = sh.gsum[sl];
+                            if (a != 0.0f) atomicAdd(grad + __float_as_int(s_spot[sl].d.x), a);
+                            sh.gsum[sl] = 0.0f;
+                        }
+                    } else {
+#pragma unroll 2
+                        for (int c = 0; c < n2; ++c) {
+                            const SpotRec r = s_spot[c];
+                            const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b);
+                            const float2 nty = hi2(r.b), ncs = lo2(r.c), it2 = hi2(r.c);
+                            const float2 w = lo2(r.d);
+#pragma unroll
+                            for (int p = 0; p < NP; ++p) {
+                                const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
+                                                          GXP[p], GYP[p]);
+                                AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS[p], qq)), AP[p]);
+                                AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
+                            }
+                        }
+#pragma unroll 2
+                        for (int c = kCap - n1; c < kCap; ++c) {
+                            const SpotRec r = s_spot[c];
+                            const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b);
+                            const float2 nty = hi2(r.b), ncs = lo2(r.c), it2 = hi2(r.c);
+                            const float2 w = lo2(r.d);
+#pragma unroll
+                            for (int p = 0; p < NP; ++p) {
+                                const float2 qq = axis_r2(nx, ny, tx, nty, ncs, it2, XP[p], YP[p],
+                                                          GXP[p], GYP[p]);
+                                AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+                if constexpr (!ADJ) {
+#pragma unroll
+                    for (int q = 0; q < kVpt; ++q) {
+                        if (act[q]) {
+                            const float ap = (q & 1) ? AP[q >> 1].y : AP[q >> 1].x;
+                            const float ah = (q & 1) ? AH[q >> 1].y : AH[q >> 1].x;
+                            const float ld = fmaf(pf[q], ap, hf[q] * ah);
+                            if (BEAM_OUT) neumaier(bs_s[q], bs_c[q], ld);
+                            neumaier(tot_s[q], tot_c[q], ld);
+                        }
                     }
                 }
             }
