@@ -330,7 +330,31 @@ struct SmoothSteps {
     float dm[PB_MAX_BEAMS][6][3];
     double inv_s;
     float tie;   // half-width of the band around half-integers sent to the exact path
+    // per (direction, radius): bit a set when the axis-a index of some
+    // voxel's sample can lie within `tie` of a half-integer
+    unsigned char tmask[PB_MAX_BEAMS][6][9];
 };
+
+// Which (direction, radius, axis) samples can come near a half-integer.  A
+// voxel's own index coordinate m0 is an integer up to the FP32 roundings of
+// its position (at most `err`), so its sample's index m0 + dr*dm has, up to
+// 2*err plus the rounding of that sum, the fractional part of dr*dm, the
+// same for every voxel of the beam.  Where that fraction is farther than
+// tie + 2*err + 1e-4 from 0.5, no voxel's fast index is within `tie` of a
+// half-integer; elsewhere the kernel takes the reference-order index.
+static void tie_masks(const float (*dm)[3], double tie, double err, unsigned char (*mask)[9])
+{
+    const double band = tie + 2.0 * err + 1e-4;
+    for (int dd = 0; dd < 6; ++dd)
+        for (int r = 0; r < 9; ++r) {
+            unsigned char m = 0;
+            for (int a = 0; a < 3; ++a) {
+                const double x = (double)(r + 1) * (double)dm[dd][a];
+                if (fabs((x - floor(x)) - 0.5) < band) m |= (unsigned char)(1 << a);
+            }
+            mask[dd][r] = m;
+        }
+}
 
 static void smooth_steps(const PbGrid &g, const PbBeamGeom *beams, int n_beams,
                          const SmoothDirs &d, SmoothSteps &o)
@@ -360,6 +384,7 @@ static void smooth_steps(const PbGrid &g, const PbBeamGeom *beams, int n_beams,
             for (int a = 0; a < 3; ++a)
                 o.dm[b][dd][a] = (float)((M[3 * a] * c + M[3 * a + 1] * s) * o.inv_s);
         }
+        tie_masks(o.dm[b], (double)o.tie, err, o.tmask[b]);
     }
 }
 
@@ -385,36 +410,36 @@ __device__ __forceinline__ int nearest_index(float q, float s, float inv_s)
 // linear): within about 8 roundings of the largest coordinate, divided by
 // the spacing (SmoothSteps::tie holds twice that bound, at least 2e-3).  The
 // kernel evaluates m0 + dr*dm with one FMA per axis and rounds it with an
-// FADD round-to-nearest, and only where some axis lies within `tie` of a
-// half-integer -- where the two could round differently -- does it take the
-// reference-order path.  The chosen voxels are the same.
+// FADD round-to-nearest.  The two can round differently only where the
+// value lies within `tie` of a half-integer, and which (direction, radius,
+// axis) samples can do so is known per beam (tie_masks): those axes take
+// the reference-order index, the others the fast one, with no per-sample
+// test.  The chosen voxels are the same.  (With beams along the image axes
+// the lateral step is exactly half a voxel along an axis, so every other
+// radius of two directions is flagged.)
 __device__ __forceinline__ void exact_sample(const PbBeamGeom &B, float s, float inv_s,
                                              float hx, float hy, float hz, float dr, float c,
-                                             float sn, int &ii, int &jj, int &kk)
+                                             float sn, int axes, int &ii, int &jj, int &kk)
 {
     float qx, qy, qz;
     head_to_image(B, __fadd_rn(hx, __fmul_rn(dr, c)), __fadd_rn(hy, __fmul_rn(dr, sn)), hz,
                   qx, qy, qz);
-    ii = nearest_index(__fadd_rn(qx, B.iso[0]), s, inv_s);
-    jj = nearest_index(__fadd_rn(qy, B.iso[1]), s, inv_s);
-    kk = nearest_index(__fadd_rn(qz, B.iso[2]), s, inv_s);
+    if (axes & 1) ii = nearest_index(__fadd_rn(qx, B.iso[0]), s, inv_s);
+    if (axes & 2) jj = nearest_index(__fadd_rn(qy, B.iso[1]), s, inv_s);
+    if (axes & 4) kk = nearest_index(__fadd_rn(qz, B.iso[2]), s, inv_s);
 }
 
-// Round to nearest (ties to even) for |m| < 2^22 with FP32 adds; reports
-// whether m lies within `tie` of a half-integer.
-__device__ __forceinline__ int round_fadd(float m, float tie, bool &near)
+// Round to nearest (ties to even) for |m| < 2^22 with FP32 adds.
+__device__ __forceinline__ int round_fadd(float m)
 {
-    const float magic = 12582912.0f;  // 1.5 * 2^23
-    const float t = __fadd_rn(m, magic);
-    const float r = __fsub_rn(t, magic);
-    near |= fabsf(__fsub_rn(m, r)) > 0.5f - tie;
-    return __float_as_int(t) - 0x4B400000;
+    return __float_as_int(__fadd_rn(m, 12582912.0f)) - 0x4B400000;   // 1.5 * 2^23
 }
 
 __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const PbGrid &g,
                                               const PbBeamGeom &B, const SmoothDirs &d,
                                               const double *M, const float (*dm)[3],
-                                              double inv_s_d, float tie, int i, int j, int k)
+                                              const unsigned char (*tm)[9], double inv_s_d,
+                                              int i, int j, int k)
 {
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
     const float center = R[v];
@@ -456,13 +481,15 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
         const int sy = g.nx, sz = g.nx * g.ny;
         for (int dd = 0; dd < 6; ++dd) {
             const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
-            for (float dr = 1.0f; dr <= nrf; dr = __fadd_rn(dr, 1.0f)) {
-                bool near = false;
-                int ii = round_fadd(fmaf(dr, dmx, m0x), tie, near);
-                int jj = round_fadd(fmaf(dr, dmy, m0y), tie, near);
-                int kk = round_fadd(fmaf(dr, dmz, m0z), tie, near);
-                if (near)
-                    exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], ii, jj, kk);
+            int r = 0;
+            for (float dr = 1.0f; dr <= nrf; dr = __fadd_rn(dr, 1.0f), ++r) {
+                int ii = round_fadd(fmaf(dr, dmx, m0x));
+                int jj = round_fadd(fmaf(dr, dmy, m0y));
+                int kk = round_fadd(fmaf(dr, dmz, m0z));
+                const int axes = tm[dd][r];   // the same for the whole beam
+                if (axes)
+                    exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], axes, ii, jj,
+                                 kk);
                 sum += __ldg(R + (ii + sy * jj + sz * kk));
             }
         }
@@ -470,12 +497,14 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
     }
     for (int dd = 0; dd < 6; ++dd) {
         const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
-        for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f)) {
-            bool near = false;
-            int ii = round_fadd(fmaf(dr, dmx, m0x), tie, near);
-            int jj = round_fadd(fmaf(dr, dmy, m0y), tie, near);
-            int kk = round_fadd(fmaf(dr, dmz, m0z), tie, near);
-            if (near) exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], ii, jj, kk);
+        int r = 0;
+        for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f), ++r) {
+            int ii = round_fadd(fmaf(dr, dmx, m0x));
+            int jj = round_fadd(fmaf(dr, dmy, m0y));
+            int kk = round_fadd(fmaf(dr, dmz, m0z));
+            const int axes = tm[dd][r];
+            if (axes)
+                exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], axes, ii, jj, kk);
             if (ii >= 0 && ii < g.nx && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz) {
                 sum += __ldg(R + ii + (int64_t)g.nx * (jj + (int64_t)g.ny * kk));
                 n += 1;
@@ -497,8 +526,8 @@ k_smooth(const float *__restrict__ raw, PbGrid g,
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
-    wet[b * V + v] = smooth_voxel(raw + b * V, g, bs.b[b], d, st.rot[b], st.dm[b], st.inv_s,
-                                  st.tie, i, j, k);
+    wet[b * V + v] = smooth_voxel(raw + b * V, g, bs.b[b], d, st.rot[b], st.dm[b], st.tmask[b],
+                                  st.inv_s, i, j, k);
 }
 
 // One (plan, beam) of a batched WET pass.
@@ -512,8 +541,8 @@ struct BatchWet {
     float *wet;                 // this beam's smoothed WET (V)
     double rot[9];
     float dm[6][3];
+    unsigned char tmask[6][9];
     double inv_s;
-    float tie;
     int cap;
     int bx, by, bz;             // 8x4x4 bricks per axis
     long long brick_start;      // first brick of this item in the launch
@@ -564,7 +593,7 @@ k_smooth_batch(const BatchWet *__restrict__ items, int n_items, SmoothDirs d)
     int i, j, k;
     if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
     W.wet[i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k)] =
-        smooth_voxel(W.raw, W.g, W.geom, d, W.rot, W.dm, W.inv_s, W.tie, i, j, k);
+        smooth_voxel(W.raw, W.g, W.geom, d, W.rot, W.dm, W.tmask, W.inv_s, i, j, k);
 }
 
 int ray_step_cap(const PbGrid &g)
@@ -626,8 +655,9 @@ long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbB
         for (int m = 0; m < 9; ++m) w.rot[m] = ss.rot[b][m];
         for (int dd = 0; dd < 6; ++dd)
             for (int a = 0; a < 3; ++a) w.dm[dd][a] = ss.dm[b][dd][a];
+        for (int dd = 0; dd < 6; ++dd)
+            for (int r = 0; r < 9; ++r) w.tmask[dd][r] = ss.tmask[b][dd][r];
         w.inv_s = ss.inv_s;
-        w.tie = ss.tie;
         w.cap = ray_step_cap(g);
         w.bx = bx;
         w.by = by;

@@ -149,6 +149,25 @@ def test_texture_mode_matches_reference(pkg, small, cube, curve, reference_modul
             assert max_rel(bd[b], rd[b]) <= 1e-3
 
 
+@pytest.mark.parametrize("gantry,couch", [(0.0, 0.0), (90.0, 0.0), (33.0, 20.0)])
+def test_smoothing_ties_match_reference(pkg, curve, reference_module, gantry, couch):
+    """At 2 mm with the beam along an image axis, every other radius of two
+    smoothing directions lands exactly on a half-voxel, where the chosen
+    voxel follows the reference's FP32 rounding; an oblique beam has no such
+    ties.  Texture-mode WET against the reference module at every voxel."""
+    case = pkg[2].heterogeneous(11, (gantry,), 60, shape=(48, 80, 72), spacing=2.0,
+                                n_slabs=1, n_spheres=2, semi_range=(10.0, 14.0),
+                                centre_jitter=4.0, body_inset=12.0)
+    beam = case.plan.beam_list[0]
+    beam.couch_angle = couch
+    g = case.grid
+    dp = g.prepareIMPTPlan(case.plan, 0, wet_mode="texture")
+    wet = dp.wet.cpu().numpy().reshape(g.HU.shape)
+    rlsp = np.array(np.interp(g.HU, *curve), dtype=np.single)
+    want = reference_module.proton_raytrace_cuda(_model(case.plan, beam), _vol(rlsp, g), beam, 0)
+    assert np.abs(wet - want).max() <= 1e-4
+
+
 def test_pencil_beam_pass_matches_reference_same_wet(pkg, small, curve, reference_module):
     engine = pkg[1]
     g, plan = small.grid, small.plan
