@@ -198,10 +198,10 @@ PbStatus pb_spot_geometry(const PbSpot *spots, int n_spots, float vsadx, float v
         float *o = geo_out + (size_t)PB_SPOT_GEO_FLOATS * q;
         o[0] = (float)x;
         o[1] = (float)y;
-        o[2] = (float)tx;
-        o[3] = (float)ty;
-        o[4] = (float)(x * y * (ivx - ivy));
-        o[5] = (float)(1.0 / (1.0 + tx * tx + ty * ty));
+        o[2] = (float)(1.0 / (1.0 + tx * tx + ty * ty));
+        o[3] = (float)tx;
+        o[4] = (float)ty;
+        o[5] = (float)(x * y * (ivx - ivy));
         o[6] = 0.0f;
         o[7] = 0.0f;
     }

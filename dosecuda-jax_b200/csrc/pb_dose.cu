@@ -633,8 +633,9 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                         cls[c] = 0;
                         if (si < L.n_spots) {
                             ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
-                            gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
-                            cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, gb[c].y, tb), nhs, nps);
+                            cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, ga[c].z, tb), nhs, nps);
+                            // the record's second half only for the kept spots
+                            if (cls[c]) gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
                         }
                         m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
                         m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
@@ -664,8 +665,8 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                                 MODE == kModeDose ? __ldg(mu + si) : __int_as_float(si);
                             SpotRec r;
                             r.a = make_float4(-ga[c].x, -ga[c].x, -ga[c].y, -ga[c].y);
-                            r.b = make_float4(ga[c].z, ga[c].z, -ga[c].w, -ga[c].w);
-                            r.c = make_float4(-gb[c].x, -gb[c].x, gb[c].y, gb[c].y);
+                            r.b = make_float4(ga[c].w, ga[c].w, -gb[c].x, -gb[c].x);
+                            r.c = make_float4(-gb[c].y, -gb[c].y, ga[c].z, ga[c].z);
                             r.d = make_float4(w, w, 0.0f, 0.0f);
                             s_spot[cls[c] == 2 ? pos2 : kCap - 1 - pos1] = r;
                         }

@@ -124,7 +124,9 @@ PbStatus pb_build_layers(const float *spot_list, int n_spots, const float *dvp,
                          PbLayer *layers_out, int *n_layers_out, int *perm_out);
 
 /* Per-spot geometry for the dose kernels: PB_SPOT_GEO_FLOATS floats per
- * spot (x, y, x/VSADX, y/VSADY, x*y*(1/VSADX-1/VSADY), 1/|t|^2, 0, 0). */
+ * spot (x, y, 1/|t|^2, x/VSADX, y/VSADY, x*y*(1/VSADX-1/VSADY), 0, 0) with
+ * t = (x/VSADX, y/VSADY, -1); the first four (16 bytes) are all that the
+ * per-tile spot cull reads. */
 PbStatus pb_spot_geometry(const PbSpot *spots, int n_spots, float vsadx,
                           float vsady, float *geo_out);
 

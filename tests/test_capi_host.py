@@ -106,9 +106,9 @@ def test_spot_geometry_values():
     geo = _lib.spot_geometry(spots, 1340.0, 1930.0)
     x, y = spots["x"].astype(np.float64), spots["y"].astype(np.float64)
     tx, ty = x / 1340.0, y / 1930.0
-    assert np.allclose(geo[:, 2], tx, rtol=1e-7) and np.allclose(geo[:, 3], ty, rtol=1e-7)
-    assert np.allclose(geo[:, 4], x * y * (1 / 1340.0 - 1 / 1930.0), rtol=1e-6)
-    assert np.allclose(geo[:, 5], 1.0 / (1.0 + tx * tx + ty * ty), rtol=1e-7)
+    assert np.allclose(geo[:, 3], tx, rtol=1e-7) and np.allclose(geo[:, 4], ty, rtol=1e-7)
+    assert np.allclose(geo[:, 5], x * y * (1 / 1340.0 - 1 / 1930.0), rtol=1e-6)
+    assert np.allclose(geo[:, 2], 1.0 / (1.0 + tx * tx + ty * ty), rtol=1e-7)
 
 
 def test_invalid_arguments_return_status_without_a_gpu():
