@@ -366,16 +366,38 @@ __device__ __forceinline__ float source_distance(const PbBeam &B, float X, float
     return sqrtf(__fmaf_rn(X, X, __fmaf_rn(Y, Y, __fmul_rn(dz, dz))));
 }
 
+// Asynchronous 4-byte global-to-shared copies (cp.async), committed and
+// waited for in groups.
+__device__ __forceinline__ void cp_async4(float *dst, const float *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n"
+                 :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
+}
+
+// Starts the copy of energy e's LUT row into shared memory (one commit
+// group per thread; the block waits with cp_async_wait and a barrier).
 template <int NT>
-__device__ __forceinline__ void stage_lut(const PbBeam &B, int e, float *s_dep,
-                                          float *s_sig, float *s_idd)
+__device__ __forceinline__ void stage_lut_async(const PbBeam &B, int e, float *s_dep,
+                                                float *s_sig, float *s_idd)
 {
     const size_t o = (size_t)e * B.lut_len;
     for (int x = threadIdx.x; x < B.lut_len; x += NT) {
-        s_dep[x] = __ldg(B.depths_dev + o + x);
-        s_sig[x] = __ldg(B.sigmas_dev + o + x);
-        s_idd[x] = __ldg(B.idds_dev + o + x);
+        cp_async4(s_dep + x, B.depths_dev + o + x);
+        cp_async4(s_sig + x, B.sigmas_dev + o + x);
+        cp_async4(s_idd + x, B.idds_dev + o + x);
     }
+    cp_async_commit();
 }
 
 // ------------------------------------------------------------------ forward
@@ -389,7 +411,9 @@ constexpr int kModeDose = 0, kModeCount = 1, kModeAdjoint = 2;
 // adjoint reads spots in groups of 8.
 template <int NT, int KCULL>
 struct DoseShared {
-    float dep[PB_MAX_LUT_LEN], sig[PB_MAX_LUT_LEN], idd[PB_MAX_LUT_LEN];
+    // LUT rows, double-buffered: the next kept layer's row is copied in
+    // while the current layer is processed
+    float dep[2][PB_MAX_LUT_LEN], sig[2][PB_MAX_LUT_LEN], idd[2][PB_MAX_LUT_LEN];
     SpotRec spot[NT * KCULL + 8];
     float gsum[NT * KCULL + 8];   // adjoint: per-slot gradient partials
     float red[NT / 32][kRedSlots];
@@ -459,7 +483,6 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
     constexpr int kCull = KCULL;
     constexpr int NP = kVpt / 2;  // voxel pairs per thread
     constexpr int kWarps = kThreads / 32;
-    float *s_dep = sh.dep, *s_sig = sh.sig, *s_idd = sh.idd;
     SpotRec *s_spot = sh.spot;
     float (*s_red)[kRedSlots] = sh.red;
     int (*s_wcount)[kWarps] = sh.wcount;
@@ -554,6 +577,9 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
             }
             if (keep) sh.lsel[lpos] = l0 + threadIdx.x;
             __syncthreads();
+            if (nsel > 0)
+                stage_lut_async<kThreads>(B, layers[B.layer_start + sh.lsel[0]].energy_id,
+                                          sh.dep[0], sh.sig[0], sh.idd[0]);
             for (int li = 0; li < nsel; ++li) {
                 const int l = sh.lsel[li];
                 const PbLayer L = layers[B.layer_start + l];
@@ -565,8 +591,19 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                     act[q] = valid[q] && !(w > cut);
                     if constexpr (ADJ) act[q] = act[q] && wv[q] != 0.0f;
                 }
-                stage_lut<kThreads>(B, L.energy_id, s_dep, s_sig, s_idd);
+                // the next kept layer's LUT row into the other buffer; then
+                // wait for this layer's
+                const int buf = li & 1;
+                if (li + 1 < nsel) {
+                    stage_lut_async<kThreads>(
+                        B, layers[B.layer_start + sh.lsel[li + 1]].energy_id, sh.dep[buf ^ 1],
+                        sh.sig[buf ^ 1], sh.idd[buf ^ 1]);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
                 __syncthreads();
+                const float *s_dep = sh.dep[buf], *s_sig = sh.sig[buf], *s_idd = sh.idd[buf];
                 const LayerK K = layer_consts(
                     L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, s_dep, B.lut_len);
                 float pf[kVpt], hf[kVpt];
@@ -1090,7 +1127,7 @@ struct DoseVariant {
 };
 static const DoseVariant kDoseVariants[] = {
     {128, 4, 2, "t128_v4_c2"}, {128, 4, 1, "t128_v4_c1"}, {128, 4, 4, "t128_v4_c4"},
-    {256, 2, 1, "t256_v2_c1"}, {256, 2, 2, "t256_v2_c2"},
+    {256, 2, 1, "t256_v2_c1"}, {128, 4, 3, "t128_v4_c3"},
 };
 constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
 
@@ -1126,7 +1163,7 @@ PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
     case 1: launch_dose_t<128, 4, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
     case 2: launch_dose_t<128, 4, 4>(A, tiles, wet, layers, g4, mu, dose, st); break;
     case 3: launch_dose_t<256, 2, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
-    case 4: launch_dose_t<256, 2, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 4: launch_dose_t<128, 4, 3>(A, tiles, wet, layers, g4, mu, dose, st); break;
     default: launch_dose_t<128, 4, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
     }
     return check_launch("k_dose");
@@ -1164,7 +1201,7 @@ PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items
     case 1: k_dose_batch<128, 4, 1><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     case 2: k_dose_batch<128, 4, 4><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     case 3: k_dose_batch<256, 2, 1><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 4: k_dose_batch<256, 2, 2><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 4: k_dose_batch<128, 4, 3><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     default: k_dose_batch<128, 4, 2><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     }
     return check_launch("k_dose_batch");
