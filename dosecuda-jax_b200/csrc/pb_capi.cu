@@ -231,6 +231,15 @@ PbStatus pb_texture_create(const float *rlsp_dev, const PbGrid *grid, PbTexture 
     return texture_create(rlsp_dev, *grid, tex_out, static_cast<cudaStream_t>(stream));
 }
 
+PbStatus pb_cells_create(const float *rlsp_dev, const PbGrid *grid, PbTexture *cells_out,
+                         void *stream)
+{
+    PbStatus s = check_grid(grid);
+    if (s != PB_OK) return s;
+    if (!rlsp_dev || !cells_out) return set_error(PB_ERR_INVALID, "NULL argument");
+    return texture_create(rlsp_dev, *grid, cells_out, static_cast<cudaStream_t>(stream), false);
+}
+
 PbStatus pb_texture_update(PbTexture tex, const float *rlsp_dev, void *stream)
 {
     if (!tex || !rlsp_dev) return set_error(PB_ERR_INVALID, "NULL argument");
@@ -249,15 +258,15 @@ PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
 {
     PbStatus s = check_grid(grid);
     if (s != PB_OK) return s;
-    if ((!rlsp_dev && !tex) || !beams || !raw_work_dev || !wet_dev)
+    if ((!rlsp_dev && !texture_samples(tex)) || !beams || !raw_work_dev || !wet_dev)
         return set_error(PB_ERR_INVALID, "NULL argument");
     if (tex && !texture_matches(tex, *grid))
         return set_error(PB_ERR_INVALID, "texture extent differs from the grid");
     if (n_beams <= 0 || n_beams > PB_MAX_BEAMS)
         return set_error(PB_ERR_INVALID, "n_beams must be in [1, %d] (got %d)", PB_MAX_BEAMS,
                          n_beams);
-    return launch_wet(rlsp_dev, texture_object(tex), texture_cells(tex), *grid, beams, n_beams, raw_work_dev, wet_dev,
-                      status_dev, static_cast<cudaStream_t>(stream));
+    return launch_wet(rlsp_dev, texture_object(tex), texture_cells(tex), *grid, beams, n_beams,
+                      raw_work_dev, wet_dev, status_dev, static_cast<cudaStream_t>(stream));
 }
 
 PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams, const float *wet_dev,
@@ -609,7 +618,8 @@ PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
                                  P.spot_geo_dev);
         if (s != PB_OK)
             return set_error(s, "plan %d: %s", p, pb_last_error());
-        if ((!P.rlsp_dev && !P.tex) || !P.raw_work_dev || !P.dose_dev || !P.mu_dev)
+        if ((!P.rlsp_dev && !texture_samples(P.tex)) || !P.raw_work_dev || !P.dose_dev ||
+            !P.mu_dev)
             return set_error(PB_ERR_INVALID, "plan %d: NULL buffer", p);
         if (P.tex && !texture_matches(P.tex, P.grid))
             return set_error(PB_ERR_INVALID, "plan %d: texture extent differs from the grid", p);

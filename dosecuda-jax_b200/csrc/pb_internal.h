@@ -37,7 +37,9 @@ long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbB
 PbStatus launch_wet_batch(const void *items_dev, int n_items, long long n_bricks, int *status,
                           cudaStream_t st);
 
-PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st);
+PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st,
+                        bool with_texture = true);
+bool texture_samples(uint64_t h);   // a texture (not a records-only handle)
 PbStatus texture_update(uint64_t h, const float *rlsp, cudaStream_t st);
 bool texture_matches(uint64_t h, const PbGrid &g);
 cudaTextureObject_t texture_object(uint64_t h);

@@ -66,7 +66,7 @@ extern "C" PbStatus pb_wet_noalloc(const float *rlsp_dev, PbTexture tex, const P
                                    int *status_dev, void *stream)
 {
     if (!grid) return set_error(PB_ERR_INVALID, "grid is NULL");
-    if ((!rlsp_dev && !tex) || !beams || !wet_dev)
+    if ((!rlsp_dev && !texture_samples(tex)) || !beams || !wet_dev)
         return set_error(PB_ERR_INVALID, "NULL argument");
     if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0 || !(grid->spacing > 0.0f))
         return set_error(PB_ERR_INVALID, "grid dimensions and spacing must be positive");

@@ -236,9 +236,10 @@ __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
     const int nsafe = safe_steps(g, B, inv_s, px, py, pz, ux, uy, uz, cap);
     double acc = 0.0;
     int n = 0;
-    if (TEX && rec) {
-        // runs through flat regions, the texture unit elsewhere; the sample
-        // counter is kept in FP32 (exact below 2^24)
+    if (rec) {
+        // runs through flat regions, the sampler elsewhere; the sample
+        // counter is kept in FP32 (exact below 2^24).  Exact trilinear
+        // weights on a flat cell also give exactly its value.
         const float dmax = fmaxf(fabsf(inv_s * ux), fmaxf(fabsf(inv_s * uy), fabsf(inv_s * uz))) +
                            1e-6f;
         const float inv_dmax = __frcp_rd(dmax);
@@ -258,13 +259,13 @@ __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
             } else {
                 // not flat here: the texture unit for the next few samples
                 // before looking at the records again
-                float part = fmaxf(tex3D<float>(tex, x, y, z), 0.0f);
+                float part = fmaxf(ray_sample<TEX>(rho, tex, g, x, y, z), 0.0f);
                 const float e = fminf(t + (float)kTexBurst, nsf);
                 for (t += 1.0f; t < e; t += 1.0f) {
                     const float x = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(ux, t, px), ix), 0.5f);
                     const float y = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uy, t, py), iy), 0.5f);
                     const float z = __fmaf_rn(inv_s, __fadd_rn(__fmaf_rn(uz, t, pz), iz), 0.5f);
-                    part += fmaxf(tex3D<float>(tex, x, y, z), 0.0f);
+                    part += fmaxf(ray_sample<TEX>(rho, tex, g, x, y, z), 0.0f);
                 }
                 acc += (double)part;
             }
@@ -582,7 +583,7 @@ k_raytrace_batch(const BatchWet *__restrict__ items, int n_items, int *status)
     if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
     const float r =
         W.tex ? raytrace_voxel<true>(W.rlsp, W.tex, W.rec, W.g, W.geom, i, j, k, W.cap, status)
-              : raytrace_voxel<false>(W.rlsp, 0, nullptr, W.g, W.geom, i, j, k, W.cap, status);
+              : raytrace_voxel<false>(W.rlsp, 0, W.rec, W.g, W.geom, i, j, k, W.cap, status);
     W.raw[i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k)] = r;
 }
 
@@ -620,7 +621,7 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *re
         k_raytrace<true><<<grid, block, 0, st>>>(rlsp, tex, rec, g, bs, zb, ray_step_cap(g),
                                                  raw, status);
     else
-        k_raytrace<false><<<grid, block, 0, st>>>(rlsp, tex, nullptr, g, bs, zb,
+        k_raytrace<false><<<grid, block, 0, st>>>(rlsp, tex, rec, g, bs, zb,
                                                   ray_step_cap(g), raw, status);
     PbStatus s = check_launch("k_raytrace");
     if (s != PB_OK) return s;
@@ -786,8 +787,10 @@ static PbStatus texture_fill(RlspTexture *t, const float *rlsp, cudaStream_t st)
     p.dstArray = t->arr;
     p.extent = make_cudaExtent(t->nx, t->ny, t->nz);
     p.kind = cudaMemcpyDeviceToDevice;
-    PbStatus s = check_cuda(cudaMemcpy3DAsync(&p, st), "cudaMemcpy3DAsync");
-    if (s != PB_OK) return s;
+    if (t->arr) {
+        const PbStatus s = check_cuda(cudaMemcpy3DAsync(&p, st), "cudaMemcpy3DAsync");
+        if (s != PB_OK) return s;
+    }
     const PbGrid g{t->nx, t->ny, t->nz, 1.0f};
     const int blocks = 148 * 8;
     k_cell_flat<<<blocks, 256, 0, st>>>(rlsp, g, t->value);
@@ -809,7 +812,9 @@ static void texture_free(RlspTexture *t)
     delete t;
 }
 
-PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st)
+// with_texture false: the cell records only, for exact-trilinear sampling.
+PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaStream_t st,
+                        bool with_texture)
 {
     const size_t ncell = (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
     if (ncell > (size_t)INT32_MAX)
@@ -821,13 +826,15 @@ PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaS
     t->nz = g.nz;
     cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
     cudaExtent ext = make_cudaExtent(g.nx, g.ny, g.nz);
-    PbStatus s = check_cuda(cudaMalloc3DArray(&t->arr, &ch, ext, cudaArrayDefault),
-                            "cudaMalloc3DArray");
+    PbStatus s = PB_OK;
+    if (with_texture)
+        s = check_cuda(cudaMalloc3DArray(&t->arr, &ch, ext, cudaArrayDefault),
+                       "cudaMalloc3DArray");
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->rec, sizeof(float2) * ncell), "cudaMalloc");
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->value, sizeof(float) * ncell), "cudaMalloc");
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d0, ncell), "cudaMalloc");
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d1, ncell), "cudaMalloc");
-    if (s == PB_OK) {
+    if (s == PB_OK && with_texture) {
         cudaResourceDesc rd{};
         rd.resType = cudaResourceTypeArray;
         rd.res.array.array = t->arr;
@@ -857,6 +864,11 @@ bool texture_matches(uint64_t h, const PbGrid &g)
 {
     const RlspTexture *t = reinterpret_cast<const RlspTexture *>(h);
     return t && t->nx == g.nx && t->ny == g.ny && t->nz == g.nz;
+}
+
+bool texture_samples(uint64_t h)
+{
+    return h && reinterpret_cast<const RlspTexture *>(h)->tex != 0;
 }
 
 cudaTextureObject_t texture_object(uint64_t h)

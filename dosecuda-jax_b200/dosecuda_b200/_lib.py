@@ -112,6 +112,7 @@ _SIGS = {
     "pb_spot_geometry": (_I, [_VP, _I, _F, _F, _VP]),
     "pb_rlsp_from_hu": (_I, [_VP, _I64, _VP, _VP, _I, _VP, _VP]),
     "pb_texture_create": (_I, [_VP, ctypes.POINTER(PbGrid), ctypes.POINTER(ctypes.c_uint64), _VP]),
+    "pb_cells_create": (_I, [_VP, ctypes.POINTER(PbGrid), ctypes.POINTER(ctypes.c_uint64), _VP]),
     "pb_texture_update": (_I, [ctypes.c_uint64, _VP, _VP]),
     "pb_texture_destroy": (_I, [ctypes.c_uint64]),
     "pb_wet": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),

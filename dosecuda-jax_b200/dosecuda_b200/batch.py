@@ -48,7 +48,9 @@ class BatchPlans:
             for b in range(dp.n_beams):
                 R.beams[b] = dp.beams[b]
             R.rlsp_dev = self.rlsps[p].data_ptr()
-            R.tex = dp._tex.value
+            # the handle of the plan's last WET mode: texture, or the exact
+            # mode's cell records
+            R.tex = dp._tex.value if dp.wet_mode == "texture" else dp._cells.value
             R.raw_work_dev = dp.raw_wet.data_ptr()
             R.wet_dev = dp.wet.data_ptr()
             R.layers_dev = dp.layers.data_ptr()

@@ -181,16 +181,19 @@ class DevicePlan:
         self.wet: Optional[torch.Tensor] = None
         self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._tex = ctypes.c_uint64(0)
+        self._cells = ctypes.c_uint64(0)
+        self.wet_mode = "texture"
 
     def __del__(self):
-        tex = getattr(self, "_tex", None)
-        if tex is not None and tex.value:
-            try:
-                torch.cuda.synchronize(self.device)
-                _lib.lib.pb_texture_destroy(tex)
-            except Exception:
-                pass
-            tex.value = 0
+        for name in ("_tex", "_cells"):
+            h = getattr(self, name, None)
+            if h is not None and h.value:
+                try:
+                    torch.cuda.synchronize(self.device)
+                    _lib.lib.pb_texture_destroy(h)
+                except Exception:
+                    pass
+                h.value = 0
 
     # -- spot order helpers ---------------------------------------------------
     def to_sorted(self, mu_plan: torch.Tensor) -> torch.Tensor:
@@ -206,14 +209,20 @@ class DevicePlan:
         return self.to_plan(self.mu_sorted)
 
     # -- WET ---------------------------------------------------------------------
-    def _texture(self, rlsp: torch.Tensor) -> int:
+    def _texture(self, rlsp: torch.Tensor, kind: str = "texture") -> int:
+        """The plan's texture ("texture") or records-only ("cells") handle,
+        created on first use and refilled from rlsp."""
         st = _stream(self.device)
-        if self._tex.value:
-            check(_lib.lib.pb_texture_update(self._tex, ptr(rlsp), st), "pb_texture_update")
+        h = self._tex if kind == "texture" else self._cells
+        if h.value:
+            check(_lib.lib.pb_texture_update(h, ptr(rlsp), st), "pb_texture_update")
+        elif kind == "texture":
+            check(_lib.lib.pb_texture_create(ptr(rlsp), ctypes.byref(self.grid), ctypes.byref(h),
+                                             st), "pb_texture_create")
         else:
-            check(_lib.lib.pb_texture_create(ptr(rlsp), ctypes.byref(self.grid),
-                                             ctypes.byref(self._tex), st), "pb_texture_create")
-        return self._tex.value
+            check(_lib.lib.pb_cells_create(ptr(rlsp), ctypes.byref(self.grid), ctypes.byref(h),
+                                           st), "pb_cells_create")
+        return h.value
 
     def compute_wet(self, rlsp: torch.Tensor, check_status: bool = True,
                     wet_mode: str = "texture") -> torch.Tensor:
@@ -227,7 +236,7 @@ class DevicePlan:
         if wet_mode not in ("texture", "exact"):
             raise ValueError("wet_mode must be 'texture' or 'exact'")
         rlsp = rlsp.contiguous()
-        tex = self._texture(rlsp) if wet_mode == "texture" else 0
+        tex = self._texture(rlsp, "texture" if wet_mode == "texture" else "cells")
         raw = torch.empty((self.n_beams, self.n_vox), dtype=torch.float32, device=self.device)
         wet = torch.empty_like(raw)
         self._status.zero_()
@@ -239,6 +248,7 @@ class DevicePlan:
             raise _lib.PbError(_lib.PB_ERR_RAY_CAP, "a WET ray reached its step cap")
         self.wet = wet
         self.raw_wet = raw
+        self.wet_mode = wet_mode
         return wet
 
     def set_wet(self, wet: torch.Tensor) -> None:

@@ -143,22 +143,31 @@ PbStatus pb_rlsp_from_hu(const float *hu_dev, int64_t n, const double *curve_hu,
  * coordinates (TextureClasses.cu:14-41, IMPTClasses.cu:292).  The texture
  * unit's filter weights are fixed point, so samples through it differ
  * slightly from exact trilinear interpolation; the reference's WET is
- * defined by them.  Creating one allocates a CUDA array. */
+ * defined by them.  Creating one allocates a CUDA array.  The handle also
+ * holds per-cell records (whether each 2x2x2 block of texels is flat, and
+ * how far the nearest non-flat one is) from which pb_wet adds whole runs of
+ * samples through flat regions at once. */
 typedef uint64_t PbTexture;
 
 PbStatus pb_texture_create(const float *rlsp_dev, const PbGrid *grid,
                            PbTexture *tex_out, void *stream);
-/* Refill an existing texture from a volume of the same grid. */
+/* A handle with the cell records only (no texture, no CUDA array), for
+ * exact-trilinear WET with the same runs through flat regions.  No
+ * counterpart in the reference. */
+PbStatus pb_cells_create(const float *rlsp_dev, const PbGrid *grid, PbTexture *cells_out,
+                         void *stream);
+/* Refill an existing handle (either kind) from a volume of the same grid. */
 PbStatus pb_texture_update(PbTexture tex, const float *rlsp_dev, void *stream);
 PbStatus pb_texture_destroy(PbTexture tex);
 
 /* WET (cm) of every voxel for n_beams beams: the ray trace toward the
  * source (CudaClasses.cu:180-228, accumulated in FP64) followed by the
  * lateral smoothing (IMPTClasses.cu:139-202).
- *   tex != 0: RLSP is sampled through the texture (the reference's
- *             samples); rlsp_dev is not read and may be NULL.
- *   tex == 0: RLSP is read from rlsp_dev with exact FP32 trilinear
- *             weights (border 0).
+ *   tex from pb_texture_create: RLSP is sampled through the texture (the
+ *             reference's samples); rlsp_dev is not read and may be NULL.
+ *   tex from pb_cells_create, or 0: RLSP is read from rlsp_dev with exact
+ *             FP32 trilinear weights (border 0); with the records, runs
+ *             through flat cells are added at once.
  * raw_work_dev and wet_dev hold n_beams x V floats; raw_work_dev receives
  * the unsmoothed WET.  status_dev (nullable) is one device int that is
  * OR-ed with PB_ERR_RAY_CAP if a ray reaches its step cap. */

@@ -91,6 +91,30 @@ def test_wet_exact_matches_oracle(pkg, small, curve, oracle):
         assert np.abs(wet[b] - sm).max() <= 1e-4
 
 
+@pytest.mark.parametrize("which", ["small", "full"])
+def test_exact_wet_runs_match_sample_by_sample(pkg, small, curve, which):
+    """Exact-trilinear WET with the cell records (pb_cells_create: runs
+    through flat cells) against the same pass sampling every step (handle
+    0): equal up to the FP64 summation order; a sample taken from a wrong
+    cell would show as >= 1e-2 cm."""
+    import ctypes
+    from dosecuda_b200 import _lib, engine
+    case = small if which == "small" else pkg[2].config_gradient()
+    g = case.grid
+    dp = g.prepareIMPTPlan(case.plan, 0, wet_mode="exact")
+    runs = dp.wet.clone()
+    hu = torch.from_numpy(np.ascontiguousarray(g.HU).reshape(-1)).to(DEV)
+    rlsp = engine.rlsp_from_hu(hu, *curve)
+    raw = torch.empty_like(runs)
+    each = torch.empty_like(runs)
+    _lib.check(_lib.lib.pb_wet(_lib.ptr(rlsp), 0, ctypes.byref(dp.grid),
+                               ctypes.cast(dp.geoms, ctypes.c_void_p), dp.n_beams, _lib.ptr(raw),
+                               _lib.ptr(each), None,
+                               ctypes.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)))
+    torch.cuda.synchronize(DEV)
+    assert float((runs - each).abs().max()) <= 1e-4
+
+
 def test_dose_exact_matches_oracle(pkg, small, cube, curve, oracle):
     for case in (small, cube):
         g, plan = case.grid, case.plan
