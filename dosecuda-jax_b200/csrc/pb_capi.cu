@@ -321,6 +321,23 @@ PbStatus pb_count_pairs(const PbGrid *grid, const PbBeam *beams, int n_beams,
                               static_cast<cudaStream_t>(stream));
 }
 
+PbStatus pb_dose_adjoint_positions(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                   const float *wet_dev, const PbLayer *layers_dev,
+                                   const float *spot_geo_dev, const float *mu_dev,
+                                   const float *dobj_dose_dev, float scale, float *grad_dev,
+                                   float *grad_x_dev, float *grad_y_dev, void *stream)
+{
+    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev);
+    if (s != PB_OK) return s;
+    if (!dobj_dose_dev || !grad_x_dev || !grad_y_dev)
+        return set_error(PB_ERR_INVALID, "NULL argument");
+    for (int b = 0; b < n_beams; ++b)
+        if (beams[b].n_layers && !mu_dev) return set_error(PB_ERR_INVALID, "mu is NULL");
+    return launch_adjoint_positions(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev,
+                                    mu_dev, dobj_dose_dev, scale, grad_dev, grad_x_dev,
+                                    grad_y_dev, static_cast<cudaStream_t>(stream));
+}
+
 PbStatus pb_count_evaluated(const PbGrid *grid, const PbBeam *beams, int n_beams,
                             const float *wet_dev, const PbLayer *layers_dev,
                             const float *spot_geo_dev, unsigned long long *count_dev,

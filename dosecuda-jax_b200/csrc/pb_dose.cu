@@ -405,7 +405,7 @@ __device__ __forceinline__ void stage_lut_async(const PbBeam &B, int e, float *s
 
 // What dose_tile computes: the dose, the forward's operation counts, or the
 // adjoint (gradient with respect to the spot weights).
-constexpr int kModeDose = 0, kModeCount = 1, kModeAdjoint = 2;
+constexpr int kModeDose = 0, kModeCount = 1, kModeAdjoint = 2, kModeAdjointPos = 3;
 
 // Shared memory of one tile.  The spot list has 8 slots past its end: the
 // adjoint reads spots in groups of 8.
@@ -447,6 +447,98 @@ __device__ __forceinline__ float warp_sum8(float (&v)[8], int lane, int &slot)
     return t;
 }
 
+// Spot-position derivatives of the adjoint sums.  With q = |t x ray|^2 *
+// it2 the scaled squared axis distance (axis_r2), the spot's factor at a
+// voxel is mu (Pf 2^(ps2 q) + Hf 2^(hs2 q)), so
+//   d/dxs = mu ln2 (Pf ps2 e1 + Hf hs2 e2) dq/dxs,
+// and from ax = X - xs gx, ay = Y - ys gy, cz = (xs/VSADX) Y - (ys/VSADY) X
+// - xs ys k (k = 1/VSADX - 1/VSADY), it2 = 1/(1 + xs^2/VSADX^2 + ys^2/VSADY^2):
+//   dq/dxs = 2 it2 (-ax gx + cz (Y/VSADX - ys k) - q xs/VSADX^2)
+//   dq/dys = 2 it2 (-ay gy + cz (-X/VSADY - xs k) - q ys/VSADY^2).
+// The voxel sums of wv (Pf ps2 e1 + Hf hs2 e2) ln2 times the bracket meet as
+// in the weight adjoint; the spot's factor mu * 2 * it2 is applied when they
+// go to grad_x, grad_y.  The weight gradient is formed alongside (grad may
+// be NULL).
+template <int NT, int NP, int KCAP>
+__device__ __forceinline__ void adjoint_positions(const SpotRec *s_spot, float *gsum,
+                                                  float *gsum_x, float *gsum_y, int n2, int n1,
+                                                  const PbBeam &B, const float2 *XP,
+                                                  const float2 *YP, const float2 *GXP,
+                                                  const float2 *GYP, const float2 *PS,
+                                                  const float2 *HS, const float2 *FP,
+                                                  const float2 *FH, const float2 *FPd,
+                                                  const float2 *FHd, int lane,
+                                                  const float *__restrict__ mu,
+                                                  float *__restrict__ grad,
+                                                  float *__restrict__ grad_x,
+                                                  float *__restrict__ grad_y)
+{
+    const float ivx = __fdiv_rn(1.0f, B.geom.vsadx), ivy = __fdiv_rn(1.0f, B.geom.vsady);
+    const float kap = __fsub_rn(ivx, ivy);
+    const float ivx2 = __fmul_rn(ivx, ivx), ivy2 = __fmul_rn(ivy, ivy);
+    for (int cls = 0; cls < 2; ++cls) {
+        const int lo = cls == 0 ? 0 : KCAP - n1, hi = cls == 0 ? n2 : KCAP;
+        for (int c0 = lo; c0 < hi; c0 += 8) {
+            float v[8], vx[8], vy[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const SpotRec r = s_spot[c0 + k];
+                const float xs = -r.a.x, ys = -r.a.z;
+                const float2 kx2 = f2(-__fmul_rn(xs, ivx2)), ky2 = f2(-__fmul_rn(ys, ivy2));
+                const float2 ckx = f2(-__fmul_rn(ys, kap)), cky = f2(-__fmul_rn(xs, kap));
+                float2 t = make_float2(0.0f, 0.0f), ux = t, uy = t;
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    const float2 ax = __ffma2_rn(lo2(r.a), GXP[p], XP[p]);
+                    const float2 ay = __ffma2_rn(hi2(r.a), GYP[p], YP[p]);
+                    const float2 cz = __ffma2_rn(lo2(r.b), YP[p], __ffma2_rn(hi2(r.b), XP[p],
+                                                                            lo2(r.c)));
+                    const float2 S = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(cz, cz)));
+                    const float2 qq = __fmul2_rn(S, hi2(r.c));
+                    const float2 e2 = ex2x2(__fmul2_rn(HS[p], qq));
+                    t = __ffma2_rn(FH[p], e2, t);
+                    float2 u = __fmul2_rn(FHd[p], e2);
+                    if (cls == 0) {
+                        const float2 e1 = ex2x2(__fmul2_rn(PS[p], qq));
+                        t = __ffma2_rn(FP[p], e1, t);
+                        u = __ffma2_rn(FPd[p], e1, u);
+                    }
+                    float2 bx = __ffma2_rn(cz, __ffma2_rn(YP[p], f2(ivx), ckx),
+                                           __fmul2_rn(ax, __fmul2_rn(GXP[p], f2(-1.0f))));
+                    bx = __ffma2_rn(qq, kx2, bx);
+                    float2 by = __ffma2_rn(cz, __ffma2_rn(XP[p], f2(-ivy), cky),
+                                           __fmul2_rn(ay, __fmul2_rn(GYP[p], f2(-1.0f))));
+                    by = __ffma2_rn(qq, ky2, by);
+                    ux = __ffma2_rn(u, bx, ux);
+                    uy = __ffma2_rn(u, by, uy);
+                }
+                v[k] = t.x + t.y;
+                vx[k] = ux.x + ux.y;
+                vy[k] = uy.x + uy.y;
+            }
+            int slot;
+            const float sum = warp_sum8(v, lane, slot);
+            const float sx = warp_sum8(vx, lane, slot);
+            const float sy = warp_sum8(vy, lane, slot);
+            if ((lane & 3) == 0 && c0 + slot < hi) {
+                if (sum != 0.0f) atomicAdd(&gsum[c0 + slot], sum);
+                if (sx != 0.0f) atomicAdd(&gsum_x[c0 + slot], sx);
+                if (sy != 0.0f) atomicAdd(&gsum_y[c0 + slot], sy);
+            }
+        }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < n2 + n1; c += NT) {
+        const int sl = c < n2 ? c : KCAP - n1 + (c - n2);
+        const int si = __float_as_int(s_spot[sl].d.x);
+        const float f = __fmul_rn(__fmul_rn(2.0f, s_spot[sl].c.z), __ldg(mu + si));
+        if (grad && gsum[sl] != 0.0f) atomicAdd(grad + si, gsum[sl]);
+        if (gsum_x[sl] != 0.0f) atomicAdd(grad_x + si, __fmul_rn(gsum_x[sl], f));
+        if (gsum_y[sl] != 0.0f) atomicAdd(grad_y + si, __fmul_rn(gsum_y[sl], f));
+        gsum[sl] = gsum_x[sl] = gsum_y[sl] = 0.0f;
+    }
+}
+
 // One 8x8x8 tile of one plan by one block of NT threads, VPT = 512 / NT
 // voxels per thread; spots are culled KCULL per thread per compaction round.
 //   kModeDose     the dose (BEAM_OUT: also each beam's dose)
@@ -455,6 +547,9 @@ __device__ __forceinline__ float warp_sum8(float (&v)[8], int lane, int &slot)
 //                 and to count[1] the spot-voxel evaluations the forward
 //                 issues (each surviving spot against the tile's 512 voxel
 //                 slots); no dose
+//   kModeAdjointPos  as kModeAdjoint (grad may be NULL), and also the
+//                 derivatives with respect to the spot's position at the
+//                 isocentre plane into grad_x, grad_y (see below)
 //   kModeAdjoint  grad[spot] += scale * sum over the tile's voxels of
 //                 wfield[v] * d dose[v] / d mu[spot], with the voxels where
 //                 wfield is 0 inactive.  Each thread evaluates its voxels
@@ -472,10 +567,14 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                                           DoseShared<NT, KCULL> &sh,
                                           unsigned long long *count = nullptr,
                                           const float *__restrict__ wfield = nullptr,
-                                          float *__restrict__ grad = nullptr)
+                                          float *__restrict__ grad = nullptr,
+                                          float *__restrict__ grad_x = nullptr,
+                                          float *__restrict__ grad_y = nullptr,
+                                          float *gsum_xy = nullptr)
 {
+    constexpr bool POS = MODE == kModeAdjointPos;
     constexpr bool COUNT = MODE == kModeCount;
-    constexpr bool ADJ = MODE == kModeAdjoint;
+    constexpr bool ADJ = MODE == kModeAdjoint || POS;
     unsigned long long n_ex2 = 0, n_eval = 0;
     static_assert(NT * VPT == 512, "a block covers one 8x8x8 tile");
     constexpr int kVpt = VPT;
@@ -510,6 +609,9 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
         }
         if (!__syncthreads_or(anyw)) return;
         for (int c = threadIdx.x; c < kCull * kThreads + 8; c += kThreads) sh.gsum[c] = 0.0f;
+        if constexpr (POS)
+            for (int c = threadIdx.x; c < 2 * (kCull * kThreads + 8); c += kThreads)
+                gsum_xy[c] = 0.0f;
     }
 
     for (int b = 0; b < A.n_beams; ++b) {
@@ -643,13 +745,19 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                 block_max2<kThreads>(hmax, pmax, s_red, nhs, nps);
                 nhs = -nhs;
                 nps = -nps;
-                // adjoint: the voxels' weighted prefactors as packed pairs
-                float2 FP[NP], FH[NP];
+                // adjoint: the voxels' weighted prefactors as packed pairs;
+                // for positions also times d(exponent)/dq = ln2 * ps2 (hs2)
+                float2 FP[NP], FH[NP], FPd[NP], FHd[NP];
                 if constexpr (ADJ) {
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
                         FP[p] = make_float2(wv[2 * p] * pf[2 * p], wv[2 * p + 1] * pf[2 * p + 1]);
                         FH[p] = make_float2(wv[2 * p] * hf[2 * p], wv[2 * p + 1] * hf[2 * p + 1]);
+                        if constexpr (POS) {
+                            constexpr float kLn2 = 0.6931471805599453f;
+                            FPd[p] = __fmul2_rn(__fmul2_rn(FP[p], PS[p]), f2(kLn2));
+                            FHd[p] = __fmul2_rn(__fmul2_rn(FH[p], HS[p]), f2(kLn2));
+                        }
                     }
                 }
                 float2 AP[NP], AH[NP];
@@ -712,6 +820,10 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                     if constexpr (COUNT) {
                         n_ex2 += 512ull * (unsigned long long)(2 * n2 + n1);
                         n_eval += 512ull * (unsigned long long)(n2 + n1);
+                    } else if constexpr (POS) {
+                        adjoint_positions<kThreads, NP, kCap>(
+                            s_spot, sh.gsum, gsum_xy, gsum_xy + kCap + 8, n2, n1, B, XP, YP,
+                            GXP, GYP, PS, HS, FP, FH, FPd, FHd, lane, mu, grad, grad_x, grad_y);
                     } else if constexpr (ADJ) {
                         // both terms: slots [0, n2); halo only: [kCap - n1, kCap);
                         // a group's slots past its class hold other records or
@@ -867,6 +979,21 @@ k_adjoint_tile(const __grid_constant__ PlanArgs A, const float *__restrict__ wet
     __shared__ DoseShared<128, 2> sh;
     dose_tile<128, 4, 2, false, kModeAdjoint>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr,
                                               nullptr, sh, nullptr, wfield, grad);
+}
+
+// Spot-weight and spot-position gradients: dose_tile in kModeAdjointPos.
+__global__ void __launch_bounds__(128, dose_min_blocks<128>())
+k_adjoint_pos_tile(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+                   const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
+                   const float *__restrict__ mu, const float *__restrict__ wfield,
+                   float *__restrict__ grad, float *__restrict__ grad_x,
+                   float *__restrict__ grad_y)
+{
+    __shared__ DoseShared<128, 2> sh;
+    __shared__ float gsum_xy[2 * (2 * 128 + 8)];
+    dose_tile<128, 4, 2, false, kModeAdjointPos>(A, blockIdx.x, wet, layers, geo, mu, nullptr,
+                                                 nullptr, sh, nullptr, wfield, grad, grad_x,
+                                                 grad_y, gsum_xy);
 }
 
 // SFU exp2 throughput: kEx2Chains independent chains x <- 2^(-x) per
@@ -1231,6 +1358,30 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                                                     reinterpret_cast<const float4 *>(geo), w,
                                                     grad);
     return check_launch("k_adjoint_tile");
+}
+
+PbStatus launch_adjoint_positions(const PbGrid &g, const PbBeam *beams, int n_beams,
+                                  const float *wet, const PbLayer *layers, const float *geo,
+                                  const float *mu, const float *w, float scale, float *grad,
+                                  float *grad_x, float *grad_y, cudaStream_t st)
+{
+    PlanArgs A;
+    fill_args(A, g, beams, n_beams, scale);
+    int total_spots = 0;
+    for (int b = 0; b < n_beams; ++b) {
+        const int e = beams[b].spot_start + beams[b].n_spots;
+        if (e > total_spots) total_spots = e;
+    }
+    const size_t bytes = sizeof(float) * (size_t)total_spots;
+    PbStatus s = PB_OK;
+    for (float *o : {grad, grad_x, grad_y})
+        if (o && s == PB_OK) s = check_cuda(cudaMemsetAsync(o, 0, bytes, st), "cudaMemsetAsync");
+    if (s != PB_OK) return s;
+    const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
+    k_adjoint_pos_tile<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers,
+                                                        reinterpret_cast<const float4 *>(geo), mu,
+                                                        w, grad, grad_x, grad_y);
+    return check_launch("k_adjoint_pos_tile");
 }
 
 size_t objective_work_size() { return sizeof(double) * kObjBlocks; }

@@ -76,6 +76,10 @@ PbStatus launch_objective(const float *dose, const float *presc,
                           float *resid, void *work, cudaStream_t st);
 size_t objective_work_size();
 
+PbStatus launch_adjoint_positions(const PbGrid &g, const PbBeam *beams, int n_beams,
+                                  const float *wet, const PbLayer *layers, const float *geo,
+                                  const float *mu, const float *w, float scale, float *grad,
+                                  float *grad_x, float *grad_y, cudaStream_t st);
 PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
                             const float *geo, cudaStream_t st);
 PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beams,

@@ -308,6 +308,24 @@ class DevicePlan:
                                        _stream(self.device)), "pb_dose_adjoint")
         return grad[: self.n_spots]
 
+    def adjoint_positions(self, dobj_ddose: torch.Tensor, scale: float = 1.0,
+                          mu_sorted: Optional[torch.Tensor] = None):
+        """(weight gradient, d/dx, d/dy) of sum_v dobj_ddose[v] D_v over the
+        spots in sorted order, x and y the spot position at the isocentre
+        plane (mm)."""
+        self._need_wet()
+        if dobj_ddose.dtype != torch.float32 or dobj_ddose.numel() != self.n_vox:
+            raise ValueError("dobj_ddose must be float32 with one entry per voxel")
+        mu = self.mu_sorted if mu_sorted is None else mu_sorted
+        n = max(self.n_spots, 1)
+        g, gx, gy = (torch.empty(n, dtype=torch.float32, device=self.device) for _ in range(3))
+        check(_lib.lib.pb_dose_adjoint_positions(
+            ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+            ptr(self.wet), ptr(self.layers), ptr(self.spot_geo), ptr(mu.contiguous()),
+            ptr(dobj_ddose.contiguous()), float(scale), ptr(g), ptr(gx), ptr(gy),
+            _stream(self.device)), "pb_dose_adjoint_positions")
+        return g[: self.n_spots], gx[: self.n_spots], gy[: self.n_spots]
+
     def count_pairs(self) -> int:
         """Dense spot-voxel pair count E of the reference kernel."""
         self._need_wet()

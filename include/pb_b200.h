@@ -213,6 +213,17 @@ PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams,
 PbStatus pb_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers_dev,
                          const float *spot_geo_dev, void *stream);
 
+/* pb_dose_adjoint and, beside it, the derivatives with respect to each
+ * spot's position (x, y at the isocentre plane, mm): grad_x_dev[s] =
+ * scale * sum_v dobj_dose_dev[v] * d dose[v] / d x_s, the same for y, in
+ * sorted spot order; grad_dev (nullable) receives the spot-weight gradient.
+ * Needs the spot weights (mu_dev).  No counterpart in the reference. */
+PbStatus pb_dose_adjoint_positions(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                   const float *wet_dev, const PbLayer *layers_dev,
+                                   const float *spot_geo_dev, const float *mu_dev,
+                                   const float *dobj_dose_dev, float scale, float *grad_dev,
+                                   float *grad_x_dev, float *grad_y_dev, void *stream);
+
 /* ------------------------------------------------------- measurement */
 
 /* What the forward pencil-beam sum issues, counted with its own culling

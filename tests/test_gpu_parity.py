@@ -319,6 +319,54 @@ def test_gradient_central_differences(pkg, small, oracle):
     assert abs(obj - objective(D)) <= 1e-4 * objective(D)
 
 
+def test_position_gradient_central_differences(pkg, small, oracle):
+    """d/dx and d/dy of sum_v w_v D_v with respect to the spot positions
+    (pb_dose_adjoint_positions) against FP64 central differences of the
+    oracle's single-spot doses on 40 seeded spots (h = 0.05 mm, the float
+    step measured), with the weight gradient of the same call against the
+    oracle adjoint."""
+    g, plan = small.grid, small.plan
+    dp = g.prepareIMPTPlan(plan, 0, wet_mode="exact")
+    shape = g.HU.shape
+    wet = dp.wet.cpu().numpy().reshape(dp.n_beams, *shape)
+    w = np.random.default_rng(5).normal(size=shape)
+    gw, gx, gy = dp.adjoint_positions(torch.from_numpy(w.reshape(-1).astype(np.float32)).to(DEV))
+    gx = dp.to_plan(gx).cpu().numpy()
+    gy = dp.to_plan(gy).cpu().numpy()
+    per_beam, nrow = [], []
+    for b, beam in enumerate(plan.beam_list):
+        m, ob, spots, layers = _oracle_beam(oracle, g, beam, _model(plan, beam))
+        sl = np.asarray(beam.spot_list, np.float32).reshape(-1, 4)
+        per_beam.append((m, ob, sl))
+        nrow.append(len(sl))
+    offs = np.cumsum([0] + nrow)
+    picks = np.random.default_rng(11).choice(offs[-1], size=40, replace=False)
+    fdx, fdy = [], []
+    for p in picks:
+        b = int(np.searchsorted(offs, p, side="right") - 1)
+        row = int(p - offs[b])
+        m, ob, sl = per_beam[b]
+        out = []
+        for axis in (0, 1):
+            cols = []
+            for sign in (1.0, -1.0):
+                one = sl[row:row + 1].copy()
+                one[0, axis] = np.float32(one[0, axis] + sign * 0.05)
+                spots, layers = oracle.build_layers(one, m.dvp)
+                cols.append((float(one[0, axis]),
+                             oracle.dose(wet[b], g.spacing[0], ob, m, spots, layers)))
+            (xp, dpos), (xm, dneg) = cols
+            out.append(float(np.sum(w * (dpos - dneg))) / (xp - xm))
+        fdx.append(out[0])
+        fdy.append(out[1])
+    fdx, fdy = np.array(fdx), np.array(fdy)
+    scale = max(np.abs(fdx).max(), np.abs(fdy).max())
+    assert np.abs(gx[picks] - fdx).max() <= 2e-3 * scale
+    assert np.abs(gy[picks] - fdy).max() <= 2e-3 * scale
+    g_ref = dp.adjoint(torch.from_numpy(w.reshape(-1).astype(np.float32)).to(DEV))
+    assert torch.allclose(gw, g_ref, rtol=1e-5, atol=1e-6 * float(g_ref.abs().max()))
+
+
 def test_autograd_backward_is_adjoint(pkg, small):
     from dosecuda_b200 import autograd
     g, plan = small.grid, small.plan
