@@ -49,7 +49,7 @@ L2_FLUSH_BYTES = 256 << 20
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_dose launch of the
 # default workload (seed 3, texture WET), from the ncu --set full capture
 # summarised in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md
-K_DOSE_TRAFFIC = 169_797_120 + 32_388_608
+K_DOSE_TRAFFIC = 169_035_520 + 32_191_488
 
 
 def _peaks():
