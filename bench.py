@@ -34,6 +34,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -66,7 +67,8 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(),
+                                 f"pb_bench_clocks_{os.getpid()}_{index}.csv")
 
     def __enter__(self):
         try:

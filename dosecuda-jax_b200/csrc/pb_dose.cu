@@ -276,7 +276,7 @@ __device__ __forceinline__ void block_max2(float a, float b, float (*s_red)[kRed
 }
 
 // True when no spot of layer L can pass cull_class at any voxel of the
-// tile, judged from the layer's bounds alone (before any per-voxel work).
+// tile, decided from the layer's bounds alone (before any per-voxel work).
 // A spot's cull value is (dx^2 + dy^2) * it2 * nhs; here dx, dy are taken
 // to the box of all the layer's spot axes at the tile's depths (FP32
 // products are monotone, so each spot's own dx, dy are no smaller), it2 to
