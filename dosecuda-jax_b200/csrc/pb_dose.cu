@@ -965,8 +965,8 @@ k_dose_count(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
              const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
              unsigned long long *count)
 {
-    __shared__ DoseShared<128, 2> sh;
-    dose_tile<128, 4, 2, false, kModeCount>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr,
+    __shared__ DoseShared<128, 1> sh;
+    dose_tile<128, 4, 1, false, kModeCount>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr,
                                             nullptr, sh, count);
 }
 
@@ -1253,7 +1253,7 @@ struct DoseVariant {
     const char *name;
 };
 static const DoseVariant kDoseVariants[] = {
-    {128, 4, 2, "t128_v4_c2"}, {128, 4, 1, "t128_v4_c1"}, {128, 4, 4, "t128_v4_c4"},
+    {128, 4, 1, "t128_v4_c1"}, {128, 4, 2, "t128_v4_c2"}, {128, 4, 4, "t128_v4_c4"},
     {256, 2, 1, "t256_v2_c1"}, {128, 4, 3, "t128_v4_c3"},
 };
 constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
@@ -1283,15 +1283,15 @@ PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
     if (beam_dose) {
         // per-beam output: the default shape only
-        k_dose<128, 4, 2, true><<<tiles, 128, 0, st>>>(A, wet, layers, g4, mu, dose, beam_dose);
+        k_dose<128, 4, 1, true><<<tiles, 128, 0, st>>>(A, wet, layers, g4, mu, dose, beam_dose);
         return check_launch("k_dose");
     }
     switch (variant) {
-    case 1: launch_dose_t<128, 4, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 1: launch_dose_t<128, 4, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
     case 2: launch_dose_t<128, 4, 4>(A, tiles, wet, layers, g4, mu, dose, st); break;
     case 3: launch_dose_t<256, 2, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
     case 4: launch_dose_t<128, 4, 3>(A, tiles, wet, layers, g4, mu, dose, st); break;
-    default: launch_dose_t<128, 4, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    default: launch_dose_t<128, 4, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
     }
     return check_launch("k_dose");
 }
@@ -1325,11 +1325,11 @@ PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items
     if (s != PB_OK) return s;
     const BatchDose *P = static_cast<const BatchDose *>(plans_dev);
     switch (variant) {
-    case 1: k_dose_batch<128, 4, 1><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 1: k_dose_batch<128, 4, 2><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     case 2: k_dose_batch<128, 4, 4><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     case 3: k_dose_batch<256, 2, 1><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
     case 4: k_dose_batch<128, 4, 3><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
-    default: k_dose_batch<128, 4, 2><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    default: k_dose_batch<128, 4, 1><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     }
     return check_launch("k_dose_batch");
 }

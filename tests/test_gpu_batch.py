@@ -2,7 +2,10 @@
 
 The batch runs every (plan, beam) WET in one launch and every plan's
 forward dose in one persistent launch; each voxel's arithmetic is the same
-as in the single-plan kernels, so results are compared for equality."""
+as in the single-plan kernel of the same shape, so results are compared for
+equality.  Kernel shapes that cull a different number of spots per round
+add a layer's spots in a different order when the layer has more spots
+than a round: those agree to rounding."""
 import numpy as np
 import pytest
 import torch
@@ -25,7 +28,7 @@ def test_batch_matches_single_plans(cases, wet_mode):
     from dosecuda_b200 import batch
     bp = batch.from_cases(cases, 0, wet_mode=wet_mode)
     single_wet = [dp.wet.clone() for dp in bp.plans]
-    single = [dp.forward() for dp in bp.plans]
+    single = [dp.forward_variant(bp.variant) for dp in bp.plans]
     for dp in bp.plans:
         dp.wet.zero_()
     bp.run()
@@ -37,12 +40,30 @@ def test_batch_matches_single_plans(cases, wet_mode):
         assert float(single[p].max()) > 0
 
 
-def test_forward_variants_agree(cases):
-    dp = cases[0].grid.prepareIMPTPlan(cases[0].plan, 0)
+def _round_size(name):
+    """Spots culled per round of a kernel shape named t<threads>_v<vpt>_c<k>."""
+    t, _, c = name.split("_")
+    return int(t[1:]) * int(c[1:])
+
+
+@pytest.mark.parametrize("pitch", [5.0, 1.5])
+def test_forward_variants_agree(pitch):
+    """Every kernel shape gives the default's dose: bit for bit when it culls
+    as many spots per round, to rounding otherwise (on the 1.5 mm lattice a
+    layer holds ~240 spots, more than some shapes' rounds)."""
+    from dosecuda_b200 import autotune, phantoms
+    case = phantoms.heterogeneous(7, (0.0, 135.0), 4000, shape=(40, 48, 56), spacing=3.0,
+                                  n_slabs=1, n_spheres=2, semi_range=(10.0, 16.0),
+                                  centre_jitter=5.0, body_inset=15.0, pitch=pitch)
+    dp = case.grid.prepareIMPTPlan(case.plan, 0)
     ref = dp.forward()
-    from dosecuda_b200 import autotune
-    for v in range(len(autotune.variants())):
-        assert torch.equal(dp.forward_variant(v), ref), v
+    names = autotune.variants()
+    for v, name in enumerate(names):
+        d = dp.forward_variant(v)
+        if _round_size(name) == _round_size(names[0]):
+            assert torch.equal(d, ref), name
+        else:
+            assert torch.allclose(d, ref, rtol=1e-5, atol=1e-6 * float(ref.max())), name
 
 
 def test_batch_variants_and_grids_agree(cases):
@@ -50,12 +71,17 @@ def test_batch_variants_and_grids_agree(cases):
     bp = batch.from_cases(cases, 0)
     bp.run()
     ref = [d.clone() for d in bp.doses]
+    names = autotune.variants()
     for v, bps in autotune.batch_candidates()[::3]:
         for d in bp.doses:
             d.zero_()
         bp.run(variant=v, blocks_per_sm=bps)
         for p in range(bp.n_plans):
-            assert torch.equal(bp.doses[p], ref[p]), (v, bps, p)
+            if _round_size(names[v]) == _round_size(names[bp.variant]):
+                assert torch.equal(bp.doses[p], ref[p]), (v, bps, p)
+            else:
+                assert torch.allclose(bp.doses[p], ref[p], rtol=1e-5,
+                                      atol=1e-6 * float(ref[p].max())), (v, bps, p)
 
 
 def test_batch_graph_replay_reads_new_weights(cases):
