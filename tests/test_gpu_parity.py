@@ -517,6 +517,53 @@ def test_invalid_device_raises_runtime_error(pkg, small, curve):
         mine.proton_raytrace_cuda(_model(plan, beam), _vol(rlsp, g), beam, 97)
 
 
+def _one_beam(plan, beam):
+    p = plan.__class__.__new__(plan.__class__)
+    p.__dict__.update(plan.__dict__)
+    p.beam_list = [beam]
+    p.n_beams = 1
+    return p
+
+
+def test_edge_plans_empty_and_single_spot_beams(pkg, small):
+    """A beam without spots adds nothing (its layers are empty); a beam of
+    one spot, added as the reference's addSingleSpot leaves it (a 1-D
+    spot_list), gives that spot's dose; a plan whose every beam is empty
+    gives zero dose and an empty gradient."""
+    from dosecuda_b200.plan_impt import IMPTBeam
+    g, plan = small.grid, small.plan
+    b0 = plan.beam_list[0]
+    empty = IMPTBeam(b0)
+    empty.resetSpots()
+    single = IMPTBeam(b0)
+    single.resetSpots()
+    x, y, mu, e = np.asarray(b0.spot_list, np.float32).reshape(-1, 4)[0]
+    single.addSingleSpot(x, y, mu, e)
+    assert np.asarray(single.spot_list).ndim == 1
+
+    d_ref = g.prepareIMPTPlan(_one_beam(plan, b0), 0).forward()
+    two = _one_beam(plan, b0)
+    two.beam_list = [b0, empty]
+    two.n_beams = 2
+    dp2 = g.prepareIMPTPlan(two, 0)
+    assert torch.equal(dp2.forward(), d_ref)
+
+    solo = g.prepareIMPTPlan(_one_beam(plan, single), 0)
+    full = g.prepareIMPTPlan(_one_beam(plan, b0), 0)
+    mu_rows = torch.zeros(full.n_spots, dtype=torch.float32, device=DEV)
+    mu_rows[0] = float(mu)               # plan row 0 only
+    mu1 = full.to_sorted(mu_rows)
+    assert solo.n_spots == 1
+    d1 = solo.forward()
+    assert float(d1.max()) > 0
+    assert torch.allclose(d1, full.forward(mu1), rtol=1e-6, atol=1e-7 * float(d1.max()))
+
+    none = _one_beam(plan, empty)
+    dpn = g.prepareIMPTPlan(none, 0)
+    assert dpn.n_spots == 0 and float(dpn.forward().abs().max()) == 0.0
+    assert dpn.adjoint(torch.ones(dpn.n_vox, dtype=torch.float32, device=DEV)).numel() == 0
+
+
 def test_ray_cap_status_is_zero_on_valid_geometry(pkg, small):
     dp = small.grid.prepareIMPTPlan(small.plan, 0)
     assert int(dp._status.item()) == 0
