@@ -333,7 +333,7 @@ struct SmoothSteps {
     float tie;   // half-width of the band around half-integers sent to the exact path
     // per (direction, radius): bit a set when the axis-a index of some
     // voxel's sample can lie within `tie` of a half-integer
-    unsigned char tmask[PB_MAX_BEAMS][6][9];
+    unsigned tmask[PB_MAX_BEAMS][6];   // 3 bits (x, y, z) per radius, radius 1 lowest
 };
 
 // Which (direction, radius, axis) samples can come near a half-integer.  A
@@ -343,18 +343,18 @@ struct SmoothSteps {
 // same for every voxel of the beam.  Where that fraction is farther than
 // tie + 2*err + 1e-4 from 0.5, no voxel's fast index is within `tie` of a
 // half-integer; elsewhere the kernel takes the reference-order index.
-static void tie_masks(const float (*dm)[3], double tie, double err, unsigned char (*mask)[9])
+static void tie_masks(const float (*dm)[3], double tie, double err, unsigned *mask)
 {
     const double band = tie + 2.0 * err + 1e-4;
-    for (int dd = 0; dd < 6; ++dd)
-        for (int r = 0; r < 9; ++r) {
-            unsigned char m = 0;
+    for (int dd = 0; dd < 6; ++dd) {
+        unsigned m = 0;
+        for (int r = 0; r < 9; ++r)
             for (int a = 0; a < 3; ++a) {
                 const double x = (double)(r + 1) * (double)dm[dd][a];
-                if (fabs((x - floor(x)) - 0.5) < band) m |= (unsigned char)(1 << a);
+                if (fabs((x - floor(x)) - 0.5) < band) m |= 1u << (3 * r + a);
             }
-            mask[dd][r] = m;
-        }
+        mask[dd] = m;
+    }
 }
 
 static void smooth_steps(const PbGrid &g, const PbBeamGeom *beams, int n_beams,
@@ -439,8 +439,8 @@ __device__ __forceinline__ int round_fadd(float m)
 __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const PbGrid &g,
                                               const PbBeamGeom &B, const SmoothDirs &d,
                                               const double *M, const float (*dm)[3],
-                                              const unsigned char (*tm)[9], double inv_s_d,
-                                              int i, int j, int k)
+                                              const unsigned *tm, double inv_s_d, int i, int j,
+                                              int k)
 {
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
     const float center = R[v];
@@ -480,30 +480,47 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
         (int64_t)g.nx * g.ny * g.nz < ((int64_t)1 << 31)) {
         const float nrf = lim > 9.0f ? 9.0f : __fsub_rn(ceilf(lim), 1.0f);
         const int sy = g.nx, sz = g.nx * g.ny;
+        // x and y as one packed pair; the index is formed from the rounded
+        // values' bit patterns with the three offsets of the magic constant
+        // folded into one (unsigned arithmetic: the sum wraps to the index)
+        const float magic = 12582912.0f;   // 1.5 * 2^23: round to nearest
+        const unsigned kOff = 0x4B400000u * (1u + (unsigned)sy + (unsigned)sz);
+        const float2 m0xy = make_float2(m0x, m0y);
         for (int dd = 0; dd < 6; ++dd) {
-            const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
-            int r = 0;
-            for (float dr = 1.0f; dr <= nrf; dr = __fadd_rn(dr, 1.0f), ++r) {
-                int ii = round_fadd(fmaf(dr, dmx, m0x));
-                int jj = round_fadd(fmaf(dr, dmy, m0y));
-                int kk = round_fadd(fmaf(dr, dmz, m0z));
-                const int axes = tm[dd][r];   // the same for the whole beam
-                if (axes)
+            const float2 dmxy = make_float2(dm[dd][0], dm[dd][1]);
+            const float dmz = dm[dd][2];
+            unsigned axes_r = tm[dd];   // the same for the whole beam
+            for (float dr = 1.0f; dr <= nrf; dr = __fadd_rn(dr, 1.0f), axes_r >>= 3) {
+                const float2 txy = __fadd2_rn(__ffma2_rn(make_float2(dr, dr), dmxy, m0xy),
+                                              make_float2(magic, magic));
+                const float tz = __fadd_rn(fmaf(dr, dmz, m0z), magic);
+                const int axes = axes_r & 7u;
+                unsigned idx;
+                if (axes) {
+                    int ii = __float_as_int(txy.x) - 0x4B400000;
+                    int jj = __float_as_int(txy.y) - 0x4B400000;
+                    int kk = __float_as_int(tz) - 0x4B400000;
                     exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], axes, ii, jj,
                                  kk);
-                sum += __ldg(R + (ii + sy * jj + sz * kk));
+                    idx = (unsigned)(ii + sy * jj + sz * kk);
+                } else {
+                    idx = (unsigned)__float_as_int(txy.x) +
+                          (unsigned)sy * (unsigned)__float_as_int(txy.y) +
+                          (unsigned)sz * (unsigned)__float_as_int(tz) - kOff;
+                }
+                sum += __ldg(R + idx);
             }
         }
         return __fdiv_rn(sum, __fadd_rn(__fmul_rn(6.0f, nrf), 1.0f));
     }
     for (int dd = 0; dd < 6; ++dd) {
         const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
-        int r = 0;
-        for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f), ++r) {
+        unsigned axes_r = tm[dd];
+        for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f), axes_r >>= 3) {
             int ii = round_fadd(fmaf(dr, dmx, m0x));
             int jj = round_fadd(fmaf(dr, dmy, m0y));
             int kk = round_fadd(fmaf(dr, dmz, m0z));
-            const int axes = tm[dd][r];
+            const int axes = axes_r & 7u;
             if (axes)
                 exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], axes, ii, jj, kk);
             if (ii >= 0 && ii < g.nx && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz) {
@@ -542,7 +559,7 @@ struct BatchWet {
     float *wet;                 // this beam's smoothed WET (V)
     double rot[9];
     float dm[6][3];
-    unsigned char tmask[6][9];
+    unsigned tmask[6];
     double inv_s;
     int cap;
     int bx, by, bz;             // 8x4x4 bricks per axis
@@ -657,7 +674,7 @@ long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbB
         for (int dd = 0; dd < 6; ++dd)
             for (int a = 0; a < 3; ++a) w.dm[dd][a] = ss.dm[b][dd][a];
         for (int dd = 0; dd < 6; ++dd)
-            for (int r = 0; r < 9; ++r) w.tmask[dd][r] = ss.tmask[b][dd][r];
+            w.tmask[dd] = ss.tmask[b][dd];
         w.inv_s = ss.inv_s;
         w.cap = ray_step_cap(g);
         w.bx = bx;
