@@ -19,7 +19,7 @@ import numpy as np
 import pandas as pd
 import torch
 
-from . import engine, nrrd
+from . import _lib, engine, nrrd
 from .plan import Beam, DoseGrid, Plan, Prescription, VolumeObject  # noqa: F401
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -173,6 +173,13 @@ class IMPTDoseGrid(DoseGrid):
         dp.compute_wet(rlsp.reshape(-1), wet_mode=wet_mode)
         return dp
 
+    def _beam_chunks(self, plan):
+        """The plan's beams in groups the device kernels take at once (the
+        reference loops over any number of beams)."""
+        beams = list(plan.beam_list)
+        n = _lib.PB_MAX_BEAMS
+        return [beams[i:i + n] for i in range(0, len(beams), n)]
+
     def computeIMPTPlan(self, plan, gpu_id=0, wet_mode="texture"):
         """Dose of every beam and their sum, times n_fractions
         (plan_impt.py:170-206)."""
@@ -183,27 +190,32 @@ class IMPTDoseGrid(DoseGrid):
             self.RLSP = self.RLSPFromHU(plan.machine_name, gpu_id)
             self.dose *= plan.n_fractions
             return
-        dp = self.prepareIMPTPlan(plan, gpu_id, wet_mode=wet_mode)
-        self.RLSP = self._device_rlsp.cpu().numpy().reshape(np.shape(self.HU))
-        dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
         shape = np.shape(self.HU)
-        bd_host = bd.cpu().numpy()
-        self.beam_doses = [bd_host[b].reshape(shape) for b in range(dp.n_beams)]
-        self.dose = dose.cpu().numpy().reshape(shape)
+        total = None
+        for chunk in self._beam_chunks(plan):
+            dp = self.prepareIMPTPlan(plan, gpu_id, beams=chunk, wet_mode=wet_mode)
+            dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
+            bd_host = bd.cpu().numpy()
+            self.beam_doses += [bd_host[b].reshape(shape) for b in range(dp.n_beams)]
+            total = dose if total is None else total + dose
+        self.RLSP = self._device_rlsp.cpu().numpy().reshape(shape)
+        self.dose = total.cpu().numpy().reshape(shape)
 
     def computeIMPTWET(self, plan, gpu_id=0, wet_mode="texture"):
         """Per-beam WET volumes as VolumeObjects (plan_impt.py:208-236)."""
         self._check_isotropic()
-        dp = self.prepareIMPTPlan(plan, gpu_id, wet_mode=wet_mode)
-        self.RLSP = self._device_rlsp.cpu().numpy().reshape(np.shape(self.HU))
-        wet = dp.wet.cpu().numpy()
         out = []
-        for b in range(dp.n_beams):
-            wet_object = VolumeObject()
-            wet_object.voxel_data = np.array(wet[b].reshape(np.shape(self.HU)), dtype=np.single)
-            wet_object.origin = np.array(self.origin, dtype=np.single)
-            wet_object.spacing = np.array(self.spacing, dtype=np.single)
-            out.append(wet_object)
+        for chunk in self._beam_chunks(plan):
+            dp = self.prepareIMPTPlan(plan, gpu_id, beams=chunk, wet_mode=wet_mode)
+            wet = dp.wet.cpu().numpy()
+            for b in range(dp.n_beams):
+                wet_object = VolumeObject()
+                wet_object.voxel_data = np.array(wet[b].reshape(np.shape(self.HU)),
+                                                 dtype=np.single)
+                wet_object.origin = np.array(self.origin, dtype=np.single)
+                wet_object.spacing = np.array(self.spacing, dtype=np.single)
+                out.append(wet_object)
+        self.RLSP = self._device_rlsp.cpu().numpy().reshape(np.shape(self.HU))
         return out
 
     def computeIMPTPlanFromWET(self, plan, wet_object, beam, gpu_id=0):
@@ -232,10 +244,27 @@ class IMPTDoseGrid(DoseGrid):
         beam's spot_list row order.  Returns (objective: float, gradient:
         float32 ndarray)."""
         from .autograd import plan_objective_and_grad
-        dp = self.prepareIMPTPlan(plan, gpu_id, wet_mode=wet_mode)
-        obj, grad = plan_objective_and_grad(dp, target_dose, voxel_weights,
-                                            scale=float(plan.n_fractions))
-        return obj, grad
+        chunks = self._beam_chunks(plan)
+        if len(chunks) == 1:
+            dp = self.prepareIMPTPlan(plan, gpu_id, wet_mode=wet_mode)
+            return plan_objective_and_grad(dp, target_dose, voxel_weights,
+                                           scale=float(plan.n_fractions))
+        # more beams than one launch takes: the dose is the sum over the groups,
+        # and each group's gradient comes from the residual of that sum
+        scale = float(plan.n_fractions)
+        dps = [self.prepareIMPTPlan(plan, gpu_id, beams=c, wet_mode=wet_mode) for c in chunks]
+        dev = dps[0].device
+        presc = torch.as_tensor(np.ascontiguousarray(target_dose, dtype=np.single),
+                                device=dev).reshape(-1)
+        w = torch.as_tensor(np.ascontiguousarray(voxel_weights, dtype=np.single),
+                            device=dev).reshape(-1)
+        dose = dps[0].forward(scale=scale)
+        for dp in dps[1:]:
+            dose = dose + dp.forward(scale=scale)
+        resid = torch.empty_like(dose)
+        obj = engine.objective(dose, presc, w, resid)
+        grads = [dp.to_plan(dp.adjoint(resid, scale=scale)).cpu().numpy() for dp in dps]
+        return float(obj.item()), np.concatenate(grads)
 
 
 class IMPTBeam(Beam):

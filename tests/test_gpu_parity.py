@@ -564,6 +564,41 @@ def test_edge_plans_empty_and_single_spot_beams(pkg, small):
     assert dpn.adjoint(torch.ones(dpn.n_vox, dtype=torch.float32, device=DEV)).numel() == 0
 
 
+def test_plan_with_more_beams_than_one_launch(pkg, curve):
+    """18 beams (more than the 16 a launch takes): computeIMPTPlan and
+    computeIMPTPlanGradient work in groups; every beam's dose matches the
+    same beam alone, the plan dose is their sum, and each group's gradient
+    is its adjoint of the whole plan's residual."""
+    from dosecuda_b200 import engine
+    angles = tuple(float(a) for a in range(0, 360, 20))
+    case = pkg[2].heterogeneous(9, angles, 18 * 40, shape=(32, 40, 40), spacing=4.0,
+                                n_slabs=1, n_spheres=1, semi_range=(12.0, 16.0),
+                                centre_jitter=2.0, body_inset=12.0)
+    g, plan = case.grid, case.plan
+    assert len(plan.beam_list) == 18
+    g.computeIMPTPlan(plan, 0)
+    assert len(g.beam_doses) == 18
+    total = np.sum(np.stack(g.beam_doses), axis=0, dtype=np.float64)
+    assert np.allclose(g.dose, total, rtol=1e-5, atol=1e-6 * total.max())
+    for b in (0, 17):
+        one = _one_beam(plan, plan.beam_list[b])
+        d = g.prepareIMPTPlan(one, 0).forward().cpu().numpy().reshape(g.HU.shape)
+        assert np.allclose(g.beam_doses[b], d, rtol=1e-6, atol=1e-7 * d.max())
+    presc, wts = case.objective_fields()
+    obj, grad = g.computeIMPTPlanGradient(plan, presc, wts, 0)
+    assert grad.shape == (sum(np.asarray(b.spot_list).reshape(-1, 4).shape[0]
+                              for b in plan.beam_list),)
+    dose = torch.from_numpy(g.dose.reshape(-1)).to(DEV)
+    resid = torch.empty_like(dose)
+    o_ref = float(engine.objective(dose, torch.from_numpy(presc.reshape(-1)).to(DEV),
+                                   torch.from_numpy(wts.reshape(-1)).to(DEV), resid))
+    assert abs(obj - o_ref) <= 1e-6 * o_ref
+    last = _one_beam(plan, plan.beam_list[17])
+    dp = g.prepareIMPTPlan(last, 0)
+    g17 = dp.to_plan(dp.adjoint(resid)).cpu().numpy()
+    assert np.allclose(grad[-len(g17):], g17, rtol=1e-4, atol=1e-5 * np.abs(g17).max())
+
+
 def test_ray_cap_status_is_zero_on_valid_geometry(pkg, small):
     dp = small.grid.prepareIMPTPlan(small.plan, 0)
     assert int(dp._status.item()) == 0
