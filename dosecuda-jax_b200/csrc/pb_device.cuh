@@ -25,12 +25,6 @@ struct BeamGeomSet {
     PbBeamGeom b[PB_MAX_BEAMS];
 };
 
-// cos/sin of the six smoothing directions i*pi/3, computed on the host.
-struct SmoothDirs {
-    float c[6];
-    float s[6];
-};
-
 __device__ __forceinline__ void vox_mm(const PbBeamGeom &b, float s, int i,
                                        int j, int k, float &x, float &y,
                                        float &z)

@@ -9,6 +9,9 @@
 // voxel bricks so that a warp covers an 8x4 patch whose rays have similar
 // lengths whatever the beam direction, and each row of 8 voxels is one
 // 32-byte sector.  Several beams share one launch (grid z = z-bricks x beams).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
 #include <new>
 
 #include "pb_internal.h"
@@ -323,208 +326,217 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex,
     raw[b * V + v] = raytrace_voxel<TEX>(rho, tex, rec, g, bs.b[b], i, j, k, cap, status);
 }
 
-// Linear map of the smoothing samples in index space, per beam: head ->
-// image rotation (rot, row-major, FP64 from the FP32 sines and cosines the
-// kernels use) and, per direction, the index step of 1 mm (dm).
-struct SmoothSteps {
-    double rot[PB_MAX_BEAMS][9];
-    float dm[PB_MAX_BEAMS][6][3];
-    double inv_s;
-    float tie;   // half-width of the band around half-integers sent to the exact path
-    // per (direction, radius): bit a set when the axis-a index of some
-    // voxel's sample can lie within `tie` of a half-integer
-    unsigned tmask[PB_MAX_BEAMS][6];   // 3 bits (x, y, z) per radius, radius 1 lowest
+// Per-beam table of the smoothing samples.  Sample (direction dd, radius
+// dr = r + 1 mm) of voxel (i, j, k) lies, along each axis a, at index
+// coordinate  m_a = i_a + dr * dm_a  up to the FP32 roundings of the
+// reference's sample position (the map from head to image coordinates is
+// linear and the voxel's own coordinate is an integer), where dm_a is the
+// index step of 1 mm along the direction.  Where the fractional part of
+// dr * dm_a is farther than the rounding bound from 0.5, roundf picks
+// i_a + ro[dd][r][a] for every voxel of the beam; the other (direction,
+// radius, axis) triples are flagged in tmask and take the reference-order
+// position per voxel.
+struct SmoothBeam {
+    int off[6][9];            // linear-index offset when no axis is flagged
+    float rc[6][9], rs[6][9]; // dr * cos, dr * sin in FP32 (the reference's products)
+    short ro[6][9][3];        // per-axis index offsets round(dr * dm_a); floor where flagged
+    unsigned tmask[6];        // 3 bits (x, y, z) per radius, radius 1 lowest
+    int margin[3];            // interior: margin_a <= i_a <= n_a - 1 - margin_a
+    float inv_s;              // 1 / spacing in FP32
+    int pow2;                 // the spacing is a power of two: inv_s is exact
+};
+
+struct SmoothSet {
+    SmoothBeam b[PB_MAX_BEAMS];
 };
 
 // Which (direction, radius, axis) samples can come near a half-integer.  A
-// voxel's own index coordinate m0 is an integer up to the FP32 roundings of
-// its position (at most `err`), so its sample's index m0 + dr*dm has, up to
-// 2*err plus the rounding of that sum, the fractional part of dr*dm, the
-// same for every voxel of the beam.  Where that fraction is farther than
-// tie + 2*err + 1e-4 from 0.5, no voxel's fast index is within `tie` of a
-// half-integer; elsewhere the kernel takes the reference-order index.
-static void tie_masks(const float (*dm)[3], double tie, double err, unsigned *mask)
+// voxel's reference-order index coordinate differs from the real-number
+// i_a + dr*dm_a by at most `err` (FP32 roundings of positions no larger
+// than the grid's extent plus the isocentre), so where the fractional part
+// of dr*dm_a is farther than tie + 2*err + 1e-4 from 0.5, every voxel's
+// sample rounds to i_a + round(dr*dm_a); elsewhere the kernel takes the
+// reference-order index, which is one of the two integers around it.
+// (With beams along the image axes the lateral step is exactly half a
+// voxel along an axis, so every other radius of two directions is flagged.)
+static void smooth_table(const PbGrid &g, const PbBeamGeom &B, const float *c, const float *sn,
+                         double err, double tie, SmoothBeam &T)
 {
+    memset(&T, 0, sizeof(T));
+    const double inv_s = 1.0 / (double)g.spacing;
+    int e2;
+    T.pow2 = frexp((double)g.spacing, &e2) == 0.5;
+    T.inv_s = (float)inv_s;
+    const double sg = B.singa, cg = B.cosga, st = B.sinta, ct = B.costa;
+    // head (hx, hy, hz) -> (xz, yz, zz) = (-hx, hz, hy); gantry; couch:
+    // x = (xz cg - yz sg) ct + zz st ; y = xz sg + yz cg ;
+    // z = -(xz cg - yz sg) st + zz ct.  Rows: image axis; columns: hx, hy.
+    const double M[3][2] = {{-cg * ct, st}, {-sg, 0.0}, {cg * st, ct}};
     const double band = tie + 2.0 * err + 1e-4;
+    const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
     for (int dd = 0; dd < 6; ++dd) {
+        double dm[3];
+        for (int a = 0; a < 3; ++a)
+            dm[a] = (M[a][0] * (double)c[dd] + M[a][1] * (double)sn[dd]) * inv_s;
         unsigned m = 0;
-        for (int r = 0; r < 9; ++r)
+        for (int r = 0; r < 9; ++r) {
+            const double dr = (double)(r + 1);
+            // dr is a small integer, so the FP64 product is exact and its
+            // FP32 rounding is the FP32 product
+            T.rc[dd][r] = (float)(dr * (double)c[dd]);
+            T.rs[dd][r] = (float)(dr * (double)sn[dd]);
+            int64_t off = 0;
             for (int a = 0; a < 3; ++a) {
-                const double x = (double)(r + 1) * (double)dm[dd][a];
-                if (fabs((x - floor(x)) - 0.5) < band) m |= 1u << (3 * r + a);
+                const double x = dr * dm[a];
+                const bool flag = fabs((x - floor(x)) - 0.5) < band;
+                if (flag) m |= 1u << (3 * r + a);
+                // flagged: the lower of the two candidates (exact_sample)
+                const int o = (int)(flag ? floor(x) : nearbyint(x));
+                T.ro[dd][r][a] = (short)o;
+                off += (a == 0 ? 1 : a == 1 ? sy : sz) * (int64_t)o;
+                T.margin[a] = std::max(T.margin[a], (int)ceil(fabs(x)) + 1);
             }
-        mask[dd] = m;
+            T.off[dd][r] = (int)off;   // used only when the grid has < 2^31 voxels
+        }
+        T.tmask[dd] = m;
     }
 }
 
-static void smooth_steps(const PbGrid &g, const PbBeamGeom *beams, int n_beams,
-                         const SmoothDirs &d, SmoothSteps &o)
+static void smooth_set(const PbGrid &g, const PbBeamGeom *beams, int n_beams, SmoothSet &o)
 {
-    o.inv_s = 1.0 / (double)g.spacing;
+    float c[6], sn[6];
+    smooth_dirs(c, sn);
+    const double inv_s = 1.0 / (double)g.spacing;
     // Bound on |FP32 reference-order index - real index|: about 8 roundings
     // of a coordinate no larger than `ext` mm, divided by the spacing, plus
-    // the fast path's own rounding; the band is twice that, at least 2e-3.
+    // 2e-4; the band is twice that, at least 2e-3.
     double ext = g.spacing * (double)(g.nx > g.ny ? (g.nx > g.nz ? g.nx : g.nz)
                                                   : (g.ny > g.nz ? g.ny : g.nz));
     for (int b = 0; b < n_beams; ++b)
         for (int a = 0; a < 3; ++a) ext = fmax(ext, fabs((double)beams[b].iso[a]) + ext);
-    const double err = 8.0 * ldexp(ext + 16.0, -24) * o.inv_s + 2e-4;
-    o.tie = (float)fmax(2e-3, 2.0 * err);
-    for (int b = 0; b < n_beams; ++b) {
-        const PbBeamGeom &B = beams[b];
-        const double sg = B.singa, cg = B.cosga, st = B.sinta, ct = B.costa;
-        // head (hx, hy, hz) -> (xz, yz, zz) = (-hx, hz, hy); gantry; couch
-        // x = (xz cg - yz sg) ct + zz st ; y = xz sg + yz cg ;
-        // z = -(xz cg - yz sg) st + zz ct
-        double *M = o.rot[b];
-        M[0] = -cg * ct; M[1] = st;  M[2] = -sg * ct;
-        M[3] = -sg;      M[4] = 0.0; M[5] = cg;
-        M[6] = cg * st;  M[7] = ct;  M[8] = sg * st;
-        for (int dd = 0; dd < 6; ++dd) {
-            const double c = d.c[dd], s = d.s[dd];
-            for (int a = 0; a < 3; ++a)
-                o.dm[b][dd][a] = (float)((M[3 * a] * c + M[3 * a + 1] * s) * o.inv_s);
-        }
-        tie_masks(o.dm[b], (double)o.tie, err, o.tmask[b]);
-    }
+    const double err = 8.0 * ldexp(ext + 16.0, -24) * inv_s + 2e-4;
+    const double tie = fmax(2e-3, 2.0 * err);
+    for (int b = 0; b < n_beams; ++b) smooth_table(g, beams[b], c, sn, err, tie, o.b[b]);
 }
 
-// roundf(q / s) as an int (CudaClasses.cuh:112-116).  q * (1/s) differs
-// from the correctly rounded quotient by a few ulp, which can change the
-// rounding only next to a half-integer; there the exact division is taken.
-__device__ __forceinline__ int nearest_index(float q, float s, float inv_s)
+// The correctly rounded quotient, out of line: the unrolled smoothing
+// loop calls it from many places.
+__device__ __noinline__ float div_rn(float q, float s) { return __fdiv_rn(q, s); }
+
+// roundf(q / s) (CudaClasses.cuh:112-116) for a quotient that lies within
+// half a voxel of the half-integer lo + 1/2 (a flagged sample): lo + 1 when
+// the quotient is above it, or equal to it and positive (roundf rounds
+// halves away from zero), else lo.  The quotient is the correctly rounded
+// one; with a power-of-two spacing 1/s is exact, so q * (1/s) is it.
+__device__ __forceinline__ int round_pick(float q, int lo, const SmoothBeam &T, float s)
 {
-    float m = __fmul_rn(q, inv_s);
-    const float tie = fabsf(fabsf(m - floorf(m)) - 0.5f);
-    if (tie < fmaf(fabsf(m), 1e-6f, 1e-6f)) m = __fdiv_rn(q, s);
-    return (int)roundf(m);
+    float m;
+    if (T.pow2)
+        m = __fmul_rn(q, T.inv_s);
+    else
+        m = div_rn(q, s);
+    const float h = __fadd_rn((float)lo, 0.5f);   // exact: |lo| < 2^22
+    return lo + ((m > h || (m == h && h > 0.0f)) ? 1 : 0);
+}
+
+// The flagged axes of sample (dd, r): the reference's FP32 position
+// (head point plus dr*(c, s, 0), rotated to the image frame, plus the
+// isocentre) divided by the spacing and rounded.  Only the flagged axes'
+// image coordinates are formed.  On entry ii, jj, kk hold the table's
+// positions, the lower candidate along the flagged axes.
+__device__ __forceinline__ void exact_sample(const PbBeamGeom &B, const SmoothBeam &T, float s,
+                                             float hx, float hy, float hz, int dd, int r,
+                                             int axes, int &ii, int &jj, int &kk)
+{
+    const float hxs = __fadd_rn(hx, T.rc[dd][r]), hys = __fadd_rn(hy, T.rs[dd][r]);
+    float qx, qy, qz;
+    if (axes & 1) {
+        head_to_image(B, hxs, hys, hz, qx, qy, qz);
+        ii = round_pick(__fadd_rn(qx, B.iso[0]), ii, T, s);
+    }
+    if (axes & 2) {
+        head_to_image(B, hxs, hys, hz, qx, qy, qz);
+        jj = round_pick(__fadd_rn(qy, B.iso[1]), jj, T, s);
+    }
+    if (axes & 4) {
+        head_to_image(B, hxs, hys, hz, qx, qy, qz);
+        kk = round_pick(__fadd_rn(qz, B.iso[2]), kk, T, s);
+    }
 }
 
 // Smoothed WET: mean of the voxel's raw WET and the in-grid nearest-voxel
 // samples at 1..9 mm along six BEV-lateral directions, taking radius dr
-// while dr < 10*WET(cm) (IMPTClasses.cu:166-198).
-//
-// The sample's voxel index along an axis is roundf of
-//   m(dr) = (head_to_image(h + dr*(c, s, 0)) + iso) / spacing,
-// evaluated in the reference's FP32 operation order (exact_sample below).
-// That value is close to the real-number m(dr) = m0 + dr*dm (the map is
-// linear): within about 8 roundings of the largest coordinate, divided by
-// the spacing (SmoothSteps::tie holds twice that bound, at least 2e-3).  The
-// kernel evaluates m0 + dr*dm with one FMA per axis and rounds it with an
-// FADD round-to-nearest.  The two can round differently only where the
-// value lies within `tie` of a half-integer, and which (direction, radius,
-// axis) samples can do so is known per beam (tie_masks): those axes take
-// the reference-order index, the others the fast one, with no per-sample
-// test.  The chosen voxels are the same.  (With beams along the image axes
-// the lateral step is exactly half a voxel along an axis, so every other
-// radius of two directions is flagged.)
-__device__ __forceinline__ void exact_sample(const PbBeamGeom &B, float s, float inv_s,
-                                             float hx, float hy, float hz, float dr, float c,
-                                             float sn, int axes, int &ii, int &jj, int &kk)
-{
-    float qx, qy, qz;
-    head_to_image(B, __fadd_rn(hx, __fmul_rn(dr, c)), __fadd_rn(hy, __fmul_rn(dr, sn)), hz,
-                  qx, qy, qz);
-    if (axes & 1) ii = nearest_index(__fadd_rn(qx, B.iso[0]), s, inv_s);
-    if (axes & 2) jj = nearest_index(__fadd_rn(qy, B.iso[1]), s, inv_s);
-    if (axes & 4) kk = nearest_index(__fadd_rn(qz, B.iso[2]), s, inv_s);
-}
-
-// Round to nearest (ties to even) for |m| < 2^22 with FP32 adds.
-__device__ __forceinline__ int round_fadd(float m)
-{
-    return __float_as_int(__fadd_rn(m, 12582912.0f)) - 0x4B400000;   // 1.5 * 2^23
-}
-
+// while dr < 10*WET(cm) (IMPTClasses.cu:166-198), summed in FP32 in the
+// reference's order (direction, then radius).  A sample is the voxel at
+// a fixed offset from this one (SmoothBeam), except along flagged axes,
+// where the reference's FP32 position is rounded (exact_sample); the
+// chosen voxels are the reference's.
 __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const PbGrid &g,
-                                              const PbBeamGeom &B, const SmoothDirs &d,
-                                              const double *M, const float (*dm)[3],
-                                              const unsigned *tm, double inv_s_d, int i, int j,
-                                              int k)
+                                              const PbBeamGeom &B, const SmoothBeam &T, int i,
+                                              int j, int k)
 {
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
     const float center = R[v];
-    float sum = center;
-    int n = 1;
+    const float lim = __fmul_rn(center, 10.0f);
+    if (!(1.0f < lim)) return center;
+    // radii 1..nr: dr < lim and dr < 10
+    const int nr = lim > 9.0f ? 9 : (int)ceilf(lim) - 1;
     float px, py, pz, hx, hy, hz;
     vox_mm(B, g.spacing, i, j, k, px, py, pz);
     image_to_head(B, px, py, pz, hx, hy, hz);
-    const float lim = __fmul_rn(center, 10.0f);
     const float s = g.spacing;
-    const float inv_s = __fdiv_rn(1.0f, s);
-    if (!(1.0f < lim)) return center;
-    // m0: real-number index coordinates of the voxel itself
-    const double dhx = hx, dhy = hy, dhz = hz;
-    const float m0x =
-        (float)((M[0] * dhx + M[1] * dhy + M[2] * dhz + (double)B.iso[0]) * inv_s_d);
-    const float m0y =
-        (float)((M[3] * dhx + M[4] * dhy + M[5] * dhz + (double)B.iso[1]) * inv_s_d);
-    const float m0z =
-        (float)((M[6] * dhx + M[7] * dhy + M[8] * dhz + (double)B.iso[2]) * inv_s_d);
-    // Interior voxels: every sample index (within 9*|dm| + 1 of m0, the
-    // reference-order path within one more) lies inside the grid, so the
-    // bounds tests and the sample count are dropped and the radii run to a
-    // precomputed count: the radii 1..9 with dr < lim.
-    float ex = 0.0f, ey = 0.0f, ez = 0.0f;
-#pragma unroll
-    for (int dd = 0; dd < 6; ++dd) {
-        ex = fmaxf(ex, fabsf(dm[dd][0]));
-        ey = fmaxf(ey, fabsf(dm[dd][1]));
-        ez = fmaxf(ez, fabsf(dm[dd][2]));
-    }
-    ex = fmaf(9.0f, ex, 2.0f);
-    ey = fmaf(9.0f, ey, 2.0f);
-    ez = fmaf(9.0f, ez, 2.0f);
-    if (m0x >= ex && m0x <= (float)(g.nx - 1) - ex && m0y >= ey &&
-        m0y <= (float)(g.ny - 1) - ey && m0z >= ez && m0z <= (float)(g.nz - 1) - ez &&
+    float sum = center;
+    // The radius loops run to 9 for every thread, the samples past the
+    // voxel's own count masked out: the loop counters and the table reads
+    // stay uniform across the warp, and whether a sample is flagged is a
+    // uniform branch.
+    if (i >= T.margin[0] && i <= g.nx - 1 - T.margin[0] && j >= T.margin[1] &&
+        j <= g.ny - 1 - T.margin[1] && k >= T.margin[2] && k <= g.nz - 1 - T.margin[2] &&
         (int64_t)g.nx * g.ny * g.nz < ((int64_t)1 << 31)) {
-        const float nrf = lim > 9.0f ? 9.0f : __fsub_rn(ceilf(lim), 1.0f);
-        const int sy = g.nx, sz = g.nx * g.ny;
-        // x and y as one packed pair; the index is formed from the rounded
-        // values' bit patterns with the three offsets of the magic constant
-        // folded into one (unsigned arithmetic: the sum wraps to the index)
-        const float magic = 12582912.0f;   // 1.5 * 2^23: round to nearest
-        const unsigned kOff = 0x4B400000u * (1u + (unsigned)sy + (unsigned)sz);
-        const float2 m0xy = make_float2(m0x, m0y);
+        // Every unflagged sample lies inside the grid (the margins): no
+        // bounds tests, 32-bit indexes.  A flagged sample is within one
+        // voxel of its unflagged position, so inside as well; it is tested
+        // all the same (cheap, and it keeps the reads in the grid whatever
+        // the table holds).  Radii unrolled: the table offsets are
+        // immediates, and a sample past the voxel's count is loaded (inside
+        // the grid all the same) and not added, without a branch.
+        const int vi = (int)v, sy = g.nx, sz = g.nx * g.ny;
+        int miss = 0;
         for (int dd = 0; dd < 6; ++dd) {
-            const float2 dmxy = make_float2(dm[dd][0], dm[dd][1]);
-            const float dmz = dm[dd][2];
-            unsigned axes_r = tm[dd];   // the same for the whole beam
-            for (float dr = 1.0f; dr <= nrf; dr = __fadd_rn(dr, 1.0f), axes_r >>= 3) {
-                const float2 txy = __fadd2_rn(__ffma2_rn(make_float2(dr, dr), dmxy, m0xy),
-                                              make_float2(magic, magic));
-                const float tz = __fadd_rn(fmaf(dr, dmz, m0z), magic);
-                const int axes = axes_r & 7u;
-                unsigned idx;
+            const unsigned tm = T.tmask[dd];   // the same for the whole beam
+#pragma unroll
+            for (int r = 0; r < 9; ++r) {
+                const int axes = (tm >> (3 * r)) & 7u;
+                int idx = vi + T.off[dd][r];
+                bool in = true;
                 if (axes) {
-                    int ii = __float_as_int(txy.x) - 0x4B400000;
-                    int jj = __float_as_int(txy.y) - 0x4B400000;
-                    int kk = __float_as_int(tz) - 0x4B400000;
-                    exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], axes, ii, jj,
-                                 kk);
-                    idx = (unsigned)(ii + sy * jj + sz * kk);
-                } else {
-                    idx = (unsigned)__float_as_int(txy.x) +
-                          (unsigned)sy * (unsigned)__float_as_int(txy.y) +
-                          (unsigned)sz * (unsigned)__float_as_int(tz) - kOff;
+                    int ii = i + T.ro[dd][r][0], jj = j + T.ro[dd][r][1],
+                        kk = k + T.ro[dd][r][2];
+                    exact_sample(B, T, s, hx, hy, hz, dd, r, axes, ii, jj, kk);
+                    in = (unsigned)ii < (unsigned)g.nx && (unsigned)jj < (unsigned)g.ny &&
+                         (unsigned)kk < (unsigned)g.nz;
+                    idx = in ? ii + sy * jj + sz * kk : vi;
                 }
-                sum += __ldg(R + idx);
+                const float x = __ldg(R + idx);
+                const bool take = r < nr;
+                sum = (take && in) ? __fadd_rn(sum, x) : sum;
+                miss += (take && !in) ? 1 : 0;
             }
         }
-        return __fdiv_rn(sum, __fadd_rn(__fmul_rn(6.0f, nrf), 1.0f));
+        return __fdiv_rn(sum, (float)(6 * nr + 1 - miss));
     }
+    int n = 1;
     for (int dd = 0; dd < 6; ++dd) {
-        const float dmx = dm[dd][0], dmy = dm[dd][1], dmz = dm[dd][2];
-        unsigned axes_r = tm[dd];
-        for (float dr = 1.0f; dr < lim && dr < 10.0f; dr = __fadd_rn(dr, 1.0f), axes_r >>= 3) {
-            int ii = round_fadd(fmaf(dr, dmx, m0x));
-            int jj = round_fadd(fmaf(dr, dmy, m0y));
-            int kk = round_fadd(fmaf(dr, dmz, m0z));
-            const int axes = axes_r & 7u;
-            if (axes)
-                exact_sample(B, s, inv_s, hx, hy, hz, dr, d.c[dd], d.s[dd], axes, ii, jj, kk);
-            if (ii >= 0 && ii < g.nx && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz) {
-                sum += __ldg(R + ii + (int64_t)g.nx * (jj + (int64_t)g.ny * kk));
+        unsigned tm = T.tmask[dd];
+#pragma unroll 1
+        for (int r = 0; r < 9; ++r, tm >>= 3) {
+            int ii = i + T.ro[dd][r][0], jj = j + T.ro[dd][r][1], kk = k + T.ro[dd][r][2];
+            const int axes = tm & 7u;
+            if (axes) exact_sample(B, T, s, hx, hy, hz, dd, r, axes, ii, jj, kk);
+            const bool take = r < nr && (unsigned)ii < (unsigned)g.nx &&
+                              (unsigned)jj < (unsigned)g.ny && (unsigned)kk < (unsigned)g.nz;
+            if (take) {
+                sum = __fadd_rn(sum, __ldg(R + ii + (int64_t)g.nx * (jj + (int64_t)g.ny * kk)));
                 n += 1;
             }
         }
@@ -533,9 +545,8 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
 }
 
 __global__ void __launch_bounds__(128)
-k_smooth(const float *__restrict__ raw, PbGrid g,
-         const __grid_constant__ BeamGeomSet bs, SmoothDirs d,
-         const __grid_constant__ SmoothSteps st, int zbricks, float *__restrict__ wet)
+k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGeomSet bs,
+         const __grid_constant__ SmoothSet st, int zbricks, float *__restrict__ wet)
 {
     const int b = blockIdx.z / zbricks;
     const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
@@ -544,8 +555,7 @@ k_smooth(const float *__restrict__ raw, PbGrid g,
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
-    wet[b * V + v] = smooth_voxel(raw + b * V, g, bs.b[b], d, st.rot[b], st.dm[b], st.tmask[b],
-                                  st.inv_s, i, j, k);
+    wet[b * V + v] = smooth_voxel(raw + b * V, g, bs.b[b], st.b[b], i, j, k);
 }
 
 // One (plan, beam) of a batched WET pass.
@@ -557,10 +567,7 @@ struct BatchWet {
     const float2 *rec;          // the texture's cell records (or null)
     float *raw;                 // this beam's unsmoothed WET (V)
     float *wet;                 // this beam's smoothed WET (V)
-    double rot[9];
-    float dm[6][3];
-    unsigned tmask[6];
-    double inv_s;
+    SmoothBeam sm;              // this beam's smoothing samples
     int cap;
     int bx, by, bz;             // 8x4x4 bricks per axis
     long long brick_start;      // first brick of this item in the launch
@@ -605,13 +612,21 @@ k_raytrace_batch(const BatchWet *__restrict__ items, int n_items, int *status)
 }
 
 __global__ void __launch_bounds__(128)
-k_smooth_batch(const BatchWet *__restrict__ items, int n_items, SmoothDirs d)
+k_smooth_batch(const BatchWet *__restrict__ items, int n_items)
 {
+    static_assert(sizeof(SmoothBeam) % 4 == 0, "the table is copied as words");
+    __shared__ SmoothBeam sm;
     const BatchWet &W = items[find_wet_item(items, n_items, blockIdx.x)];
+    // the block's sample table into shared memory (one item per block)
+    const int *src = reinterpret_cast<const int *>(&W.sm);
+    int *dst = reinterpret_cast<int *>(&sm);
+    for (int q = threadIdx.x; q < (int)(sizeof(SmoothBeam) / 4); q += blockDim.x)
+        dst[q] = __ldg(src + q);
+    __syncthreads();
     int i, j, k;
     if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
     W.wet[i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k)] =
-        smooth_voxel(W.raw, W.g, W.geom, d, W.rot, W.dm, W.tmask, W.inv_s, i, j, k);
+        smooth_voxel(W.raw, W.g, W.geom, sm, i, j, k);
 }
 
 int ray_step_cap(const PbGrid &g)
@@ -627,10 +642,8 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *re
 {
     BeamGeomSet bs;
     for (int b = 0; b < n_beams; ++b) bs.b[b] = beams[b];
-    SmoothDirs d;
-    smooth_dirs(d.c, d.s);
-    SmoothSteps ss;
-    smooth_steps(g, beams, n_beams, d, ss);
+    SmoothSet ss;
+    smooth_set(g, beams, n_beams, ss);
     const int zb = (g.nz + 3) / 4;
     dim3 block(8, 4, 4);
     dim3 grid((g.nx + 7) / 8, (g.ny + 3) / 4, zb * n_beams);
@@ -642,7 +655,7 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *re
                                                   ray_step_cap(g), raw, status);
     PbStatus s = check_launch("k_raytrace");
     if (s != PB_OK) return s;
-    k_smooth<<<grid, block, 0, st>>>(raw, g, bs, d, ss, zb, wet);
+    k_smooth<<<grid, block, 0, st>>>(raw, g, bs, ss, zb, wet);
     return check_launch("k_smooth");
 }
 
@@ -654,10 +667,8 @@ long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbB
                          const float2 *rec, float *raw, float *wet, long long brick_start)
 {
     BatchWet *W = static_cast<BatchWet *>(items_host) + first;
-    SmoothDirs d;
-    smooth_dirs(d.c, d.s);
-    SmoothSteps ss;
-    smooth_steps(g, beams, n_beams, d, ss);
+    SmoothSet ss;
+    smooth_set(g, beams, n_beams, ss);
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int bx = (g.nx + 7) / 8, by = (g.ny + 3) / 4, bz = (g.nz + 3) / 4;
     const long long per = (long long)bx * by * bz;
@@ -670,12 +681,7 @@ long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbB
         w.rec = rec;
         w.raw = raw + b * V;
         w.wet = wet + b * V;
-        for (int m = 0; m < 9; ++m) w.rot[m] = ss.rot[b][m];
-        for (int dd = 0; dd < 6; ++dd)
-            for (int a = 0; a < 3; ++a) w.dm[dd][a] = ss.dm[b][dd][a];
-        for (int dd = 0; dd < 6; ++dd)
-            w.tmask[dd] = ss.tmask[b][dd];
-        w.inv_s = ss.inv_s;
+        w.sm = ss.b[b];
         w.cap = ray_step_cap(g);
         w.bx = bx;
         w.by = by;
@@ -690,13 +696,11 @@ PbStatus launch_wet_batch(const void *items_dev, int n_items, long long n_bricks
 {
     if (n_bricks <= 0) return PB_OK;
     if (n_bricks > 0x7fffffffLL) return set_error(PB_ERR_INVALID, "batch too large");
-    SmoothDirs d;
-    smooth_dirs(d.c, d.s);
     const BatchWet *I = static_cast<const BatchWet *>(items_dev);
     k_raytrace_batch<<<(unsigned)n_bricks, 128, 0, st>>>(I, n_items, status);
     PbStatus s = check_launch("k_raytrace_batch");
     if (s != PB_OK) return s;
-    k_smooth_batch<<<(unsigned)n_bricks, 128, 0, st>>>(I, n_items, d);
+    k_smooth_batch<<<(unsigned)n_bricks, 128, 0, st>>>(I, n_items);
     return check_launch("k_smooth_batch");
 }
 

@@ -66,6 +66,7 @@ def load(port32: bool = False):
     lib.ob_raytrace.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp, i64, vp]
     lib.ob_raytrace.restype = i
     lib.ob_smooth.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp, i64, vp]
+    lib.ob_smooth_f32.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp]
     lib.ob_build_layers.argtypes = [vp, i, vp, i, i, vp, vp]
     lib.ob_build_layers.restype = i
     lib.ob_dose.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam),
@@ -131,6 +132,17 @@ def smooth(raw_f32, spacing, beam: OBeam, idx=None, port32=False):
     lib.ob_smooth(_p(raw), ctypes.byref(_grid(raw.shape, spacing)), ctypes.byref(beam), _p(idx),
                   0 if idx is None else len(idx), _p(out))
     return out if idx is not None else out.reshape(raw.shape)
+
+
+def smooth_f32(raw_f32, spacing, beam: OBeam):
+    """The smoothing with the reference's FP32 sum and quotient: equal bit
+    for bit to a kernel that picks the same sample voxels."""
+    lib = load()
+    raw = np.ascontiguousarray(raw_f32, np.float32)
+    out = np.zeros(raw.shape, np.float32)
+    lib.ob_smooth_f32(_p(raw), ctypes.byref(_grid(raw.shape, spacing)), ctypes.byref(beam),
+                      _p(out))
+    return out
 
 
 def build_layers(spot_list, dvp):

@@ -286,16 +286,18 @@ int ob_raytrace(const float *rho, const ob_grid *g, const ob_beam *b,
     return err;
 }
 
-/* Smoothed WET of one voxel from the raw WET volume (IMPTClasses.cu:139-202).
- * raw is the full raw-WET volume stored in FP32 (cm). */
-real ob_smooth_voxel(const float *raw, const ob_grid *g, const ob_beam *b,
-                     const float *dc, const float *ds, int i, int j, int k)
+/* The in-grid smoothing samples of one voxel in the reference's order
+ * (direction, then radius; IMPTClasses.cu:166-198), written to vals;
+ * returns how many (at most 54).  raw is the full raw-WET volume in FP32
+ * (cm). */
+static int smooth_samples(const float *raw, const ob_grid *g, const ob_beam *b,
+                          const float *dc, const float *ds, int i, int j, int k,
+                          float *vals)
 {
     float p[3], h[3];
     int64_t v = (int64_t)i + (int64_t)g->nx * (j + (int64_t)g->ny * k);
     float center = raw[v];
-    real sum = center;
-    int n = 1;
+    int n = 0;
     vox_mm(g, b, i, j, k, p);
     image_to_head_f(b, p, h);
     for (int d = 0; d < 6; d++) {
@@ -310,17 +312,27 @@ real ob_smooth_voxel(const float *raw, const ob_grid *g, const ob_beam *b,
             int jj = (int)roundf((pc[1] + b->iso[1]) / g->s);
             int kk = (int)roundf((pc[2] + b->iso[2]) / g->s);
             if (ii >= 0 && ii < g->nx && jj >= 0 && jj < g->ny && kk >= 0 &&
-                kk < g->nz) {
-                sum += raw[(int64_t)ii + (int64_t)g->nx * (jj + (int64_t)g->ny * kk)];
-                n += 1;
-            }
+                kk < g->nz)
+                vals[n++] = raw[(int64_t)ii + (int64_t)g->nx * (jj + (int64_t)g->ny * kk)];
             dr += 1.0f;
         }
     }
+    return n;
+}
+
+/* Smoothed WET of one voxel: the mean of the voxel's raw WET and its
+ * samples, summed in `real` (FP64 in the oracle). */
+real ob_smooth_voxel(const float *raw, const ob_grid *g, const ob_beam *b,
+                     const float *dc, const float *ds, int i, int j, int k)
+{
+    float vals[54];
+    const int m = smooth_samples(raw, g, b, dc, ds, i, j, k, vals);
+    real sum = raw[(int64_t)i + (int64_t)g->nx * (j + (int64_t)g->ny * k)];
+    for (int q = 0; q < m; q++) sum += vals[q];
 #ifdef PB_PORT32
-    return sum / (float)n;
+    return sum / (float)(m + 1);
 #else
-    return sum / (double)n;
+    return sum / (double)(m + 1);
 #endif
 }
 
@@ -338,6 +350,27 @@ void ob_smooth(const float *raw, const ob_grid *g, const ob_beam *b,
         int j = (int)((v / g->nx) % g->ny);
         int k = (int)(v / ((int64_t)g->nx * g->ny));
         out[q] = ob_smooth_voxel(raw, g, b, dc, ds, i, j, k);
+    }
+}
+
+/* The smoothing with the reference's own arithmetic: an FP32 sum in
+ * sample order and an FP32 quotient (IMPTClasses.cu:168-198), so that a
+ * kernel choosing the same voxels gives the same bits. */
+void ob_smooth_f32(const float *raw, const ob_grid *g, const ob_beam *b, float *out)
+{
+    float dc[6], ds[6];
+    ob_smooth_dirs(dc, ds);
+    int64_t nv = (int64_t)g->nx * g->ny * g->nz;
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < nv; v++) {
+        int i = (int)(v % g->nx);
+        int j = (int)((v / g->nx) % g->ny);
+        int k = (int)(v / ((int64_t)g->nx * g->ny));
+        float vals[54];
+        const int m = smooth_samples(raw, g, b, dc, ds, i, j, k, vals);
+        float sum = raw[v];
+        for (int q = 0; q < m; q++) sum += vals[q];
+        out[v] = sum / (float)(m + 1);
     }
 }
 

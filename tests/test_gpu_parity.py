@@ -192,6 +192,44 @@ def test_smoothing_ties_match_reference(pkg, curve, reference_module, gantry, co
     assert np.abs(wet - want).max() <= 1e-4
 
 
+@pytest.mark.parametrize("gantry,couch,spacing", [(0.0, 0.0, 2.0), (90.0, 0.0, 2.0),
+                                                 (270.0, 90.0, 2.5), (33.3, 15.0, 3.0),
+                                                 (180.0, 0.0, 1.5), (225.0, 300.0, 2.0),
+                                                 (90.0, 0.0, 3.0), (0.0, 0.0, 1.0)])
+def test_smoothing_bitwise_reference_arithmetic(pkg, oracle, gantry, couch, spacing):
+    """The smoothing alone, bit for bit: the kernel's raw WET of a noisy
+    RLSP volume (so that neighbouring voxels differ) smoothed by the oracle
+    with the reference's FP32 sum and quotient equals the kernel's smoothed
+    WET at every voxel, the grid's edges included.  A single sample taken
+    from another voxel would change the bits.  Beams along the image axes
+    put samples exactly on half-voxels (2, 3 and 1 mm; 3 mm is not a power
+    of two, so the quotient is formed by division there)."""
+    import ctypes
+    from dosecuda_b200 import _lib
+    case = pkg[2].heterogeneous(13, (gantry,), 40, shape=(37, 45, 51), spacing=spacing,
+                                n_slabs=1, n_spheres=1, semi_range=(4.0 * spacing, 5.0 * spacing),
+                                centre_jitter=3.0 * spacing, body_inset=5.0 * spacing)
+    beam = case.plan.beam_list[0]
+    beam.couch_angle = couch
+    g = case.grid
+    dp = g.prepareIMPTPlan(case.plan, 0, wet_mode="exact")
+    rng = np.random.default_rng(int(gantry * 10 + couch))
+    rlsp = torch.from_numpy(rng.uniform(0.0, 2.5, g.HU.size).astype(np.float32)).to(DEV)
+    raw = torch.empty_like(dp.wet)
+    wet = torch.empty_like(dp.wet)
+    _lib.check(_lib.lib.pb_wet(_lib.ptr(rlsp), 0, ctypes.byref(dp.grid),
+                               ctypes.cast(dp.geoms, ctypes.c_void_p), dp.n_beams, _lib.ptr(raw),
+                               _lib.ptr(wet), None,
+                               ctypes.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)))
+    torch.cuda.synchronize(DEV)
+    _, ob, _, _ = _oracle_beam(oracle, g, beam, _model(case.plan, beam))
+    raw_np = raw.cpu().numpy().reshape(g.HU.shape)
+    want = oracle.smooth_f32(raw_np, g.spacing[0], ob)
+    got = wet.cpu().numpy().reshape(g.HU.shape)
+    assert (raw_np * 10.0 > 9.0).mean() > 0.5   # most voxels take all nine radii
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 def test_pencil_beam_pass_matches_reference_same_wet(pkg, small, curve, reference_module):
     engine = pkg[1]
     g, plan = small.grid, small.plan

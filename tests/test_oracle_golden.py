@@ -68,6 +68,20 @@ def test_oracle_wet_and_dose_match_reference(path, plan, oracle):
         assert np.abs(got - ref).max() <= 5e-3 * ref.max()
 
 
+def test_oracle_fp32_smoothing_agrees_with_fp64(plan, oracle):
+    """The FP32-sum smoothing (the reference's arithmetic, used for the
+    kernels' bitwise check) and the FP64-sum smoothing take the same samples:
+    they differ by the sum's rounding only."""
+    z = np.load(FILES[0])
+    rng = np.random.default_rng(5)
+    raw = rng.uniform(0.0, 3.0, z["hu"].shape).astype(np.float32)
+    for b, m, ob, spots, layers in _beams(z, plan, oracle):
+        f64 = oracle.smooth(raw, z["spacing"][0], ob)
+        f32 = oracle.smooth_f32(raw, z["spacing"][0], ob)
+        assert f32.dtype == np.float32
+        assert np.abs(f32 - f64).max() <= 2e-6 * np.abs(f64).max()
+
+
 def test_rlsp_is_numpy_interp_of_the_machine_curve(plan, oracle):
     z = np.load(FILES[0])
     from dosecuda_b200.plan_impt import _hu_curve
