@@ -333,13 +333,16 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex,
 // linear and the voxel's own coordinate is an integer), where dm_a is the
 // index step of 1 mm along the direction.  Where the fractional part of
 // dr * dm_a is farther than the rounding bound from 0.5, roundf picks
-// i_a + ro[dd][r][a] for every voxel of the beam; the other (direction,
-// radius, axis) triples are flagged in tmask and take the reference-order
-// position per voxel.
+// i_a + ro for every voxel of the beam; the other (direction, radius,
+// axis) triples are flagged in tmask and take the reference-order position
+// per voxel, which is i_a + ro or i_a + ro + 1 with ro = floor(dr * dm_a).
+// The table holds ro + 1/2 (hh), the half-integer the flagged position is
+// compared with.
 struct SmoothBeam {
     int off[6][9];            // linear-index offset when no axis is flagged
     float rc[6][9], rs[6][9]; // dr * cos, dr * sin in FP32 (the reference's products)
-    short ro[6][9][3];        // per-axis index offsets round(dr * dm_a); floor where flagged
+    float hh[6][9][3];        // per-axis index offset ro + 1/2: ro = round(dr * dm_a),
+                              // floor where flagged
     unsigned tmask[6];        // 3 bits (x, y, z) per radius, radius 1 lowest
     int margin[3];            // interior: margin_a <= i_a <= n_a - 1 - margin_a
     float inv_s;              // 1 / spacing in FP32
@@ -390,9 +393,9 @@ static void smooth_table(const PbGrid &g, const PbBeamGeom &B, const float *c, c
                 const double x = dr * dm[a];
                 const bool flag = fabs((x - floor(x)) - 0.5) < band;
                 if (flag) m |= 1u << (3 * r + a);
-                // flagged: the lower of the two candidates (exact_sample)
+                // flagged: the lower of the two candidates (exact_steps)
                 const int o = (int)(flag ? floor(x) : nearbyint(x));
-                T.ro[dd][r][a] = (short)o;
+                T.hh[dd][r][a] = (float)o + 0.5f;
                 off += (a == 0 ? 1 : a == 1 ? sy : sz) * (int64_t)o;
                 T.margin[a] = std::max(T.margin[a], (int)ceil(fabs(x)) + 1);
             }
@@ -423,44 +426,45 @@ static void smooth_set(const PbGrid &g, const PbBeamGeom *beams, int n_beams, Sm
 // loop calls it from many places.
 __device__ __noinline__ float div_rn(float q, float s) { return __fdiv_rn(q, s); }
 
-// roundf(q / s) (CudaClasses.cuh:112-116) for a quotient that lies within
-// half a voxel of the half-integer lo + 1/2 (a flagged sample): lo + 1 when
-// the quotient is above it, or equal to it and positive (roundf rounds
-// halves away from zero), else lo.  The quotient is the correctly rounded
-// one; with a power-of-two spacing 1/s is exact, so q * (1/s) is it.
-__device__ __forceinline__ int round_pick(float q, int lo, const SmoothBeam &T, float s)
+// roundf(q / s) (CudaClasses.cuh:112-116) minus lo, for a flagged sample
+// whose quotient lies within half a voxel of h = lo + 1/2: 1 when the
+// quotient is above h, or equal to it and positive (roundf rounds halves
+// away from zero), else 0.  The quotient is the correctly rounded one;
+// with a power-of-two spacing 1/s is exact, so q * (1/s) is it.
+template <bool POW2>
+__device__ __forceinline__ int round_up(float q, float h, float s, float inv_s)
 {
-    float m;
-    if (T.pow2)
-        m = __fmul_rn(q, T.inv_s);
-    else
-        m = div_rn(q, s);
-    const float h = __fadd_rn((float)lo, 0.5f);   // exact: |lo| < 2^22
-    return lo + ((m > h || (m == h && h > 0.0f)) ? 1 : 0);
+    const float m = POW2 ? __fmul_rn(q, inv_s) : div_rn(q, s);
+    return (m > h || (m == h && h > 0.0f)) ? 1 : 0;
 }
 
-// The flagged axes of sample (dd, r): the reference's FP32 position
+// Sample (dd, r) along the flagged axes: the reference's FP32 position
 // (head point plus dr*(c, s, 0), rotated to the image frame, plus the
-// isocentre) divided by the spacing and rounded.  Only the flagged axes'
-// image coordinates are formed.  On entry ii, jj, kk hold the table's
-// positions, the lower candidate along the flagged axes.
-__device__ __forceinline__ void exact_sample(const PbBeamGeom &B, const SmoothBeam &T, float s,
-                                             float hx, float hy, float hz, int dd, int r,
-                                             int axes, int &ii, int &jj, int &kk)
+// isocentre) divided by the spacing and rounded, as 0/1 steps from the
+// table's lower candidates; fi, fj, fk are the voxel's indexes as floats.
+// Only the flagged axes' image coordinates are formed.
+template <bool POW2>
+__device__ __forceinline__ void exact_steps(const PbBeamGeom &B, const SmoothBeam &T, float s,
+                                            float hx, float hy, float hz, float fi, float fj,
+                                            float fk, int dd, int r, int axes, int &ui, int &uj,
+                                            int &uk)
 {
     const float hxs = __fadd_rn(hx, T.rc[dd][r]), hys = __fadd_rn(hy, T.rs[dd][r]);
     float qx, qy, qz;
     if (axes & 1) {
         head_to_image(B, hxs, hys, hz, qx, qy, qz);
-        ii = round_pick(__fadd_rn(qx, B.iso[0]), ii, T, s);
+        ui = round_up<POW2>(__fadd_rn(qx, B.iso[0]), __fadd_rn(fi, T.hh[dd][r][0]), s,
+                            T.inv_s);
     }
     if (axes & 2) {
         head_to_image(B, hxs, hys, hz, qx, qy, qz);
-        jj = round_pick(__fadd_rn(qy, B.iso[1]), jj, T, s);
+        uj = round_up<POW2>(__fadd_rn(qy, B.iso[1]), __fadd_rn(fj, T.hh[dd][r][1]), s,
+                            T.inv_s);
     }
     if (axes & 4) {
         head_to_image(B, hxs, hys, hz, qx, qy, qz);
-        kk = round_pick(__fadd_rn(qz, B.iso[2]), kk, T, s);
+        uk = round_up<POW2>(__fadd_rn(qz, B.iso[2]), __fadd_rn(fk, T.hh[dd][r][2]), s,
+                            T.inv_s);
     }
 }
 
@@ -469,10 +473,12 @@ __device__ __forceinline__ void exact_sample(const PbBeamGeom &B, const SmoothBe
 // while dr < 10*WET(cm) (IMPTClasses.cu:166-198), summed in FP32 in the
 // reference's order (direction, then radius).  A sample is the voxel at
 // a fixed offset from this one (SmoothBeam), except along flagged axes,
-// where the reference's FP32 position is rounded (exact_sample); the
-// chosen voxels are the reference's.
+// where the reference's FP32 position is rounded (exact_steps); the
+// chosen voxels are the reference's.  POW2: the grid spacing is a power
+// of two.
+template <bool POW2>
 __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const PbGrid &g,
-                                              const PbBeamGeom &B, const SmoothBeam &T, int i,
+                                              const PbBeamGeom &Bp, const SmoothBeam &T, int i,
                                               int j, int k)
 {
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
@@ -481,10 +487,12 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
     if (!(1.0f < lim)) return center;
     // radii 1..nr: dr < lim and dr < 10
     const int nr = lim > 9.0f ? 9 : (int)ceilf(lim) - 1;
+    const PbBeamGeom B = Bp;   // the rotation and isocentre in registers
     float px, py, pz, hx, hy, hz;
     vox_mm(B, g.spacing, i, j, k, px, py, pz);
     image_to_head(B, px, py, pz, hx, hy, hz);
     const float s = g.spacing;
+    const float fi = (float)i, fj = (float)j, fk = (float)k;
     float sum = center;
     // The radius loops run to 9 for every thread, the samples past the
     // voxel's own count masked out: the loop counters and the table reads
@@ -493,46 +501,45 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
     if (i >= T.margin[0] && i <= g.nx - 1 - T.margin[0] && j >= T.margin[1] &&
         j <= g.ny - 1 - T.margin[1] && k >= T.margin[2] && k <= g.nz - 1 - T.margin[2] &&
         (int64_t)g.nx * g.ny * g.nz < ((int64_t)1 << 31)) {
-        // Every unflagged sample lies inside the grid (the margins): no
-        // bounds tests, 32-bit indexes.  A flagged sample is within one
-        // voxel of its unflagged position, so inside as well; it is tested
-        // all the same (cheap, and it keeps the reads in the grid whatever
-        // the table holds).  Radii unrolled: the table offsets are
-        // immediates, and a sample past the voxel's count is loaded (inside
-        // the grid all the same) and not added, without a branch.
+        // Interior: both candidates of every sample lie inside the grid
+        // (the margins), so there are no bounds tests and the indexes are
+        // 32-bit.  Radii unrolled: the table offsets are immediates, and a
+        // sample past the voxel's count is loaded and not added, without a
+        // branch.
         const int vi = (int)v, sy = g.nx, sz = g.nx * g.ny;
-        int miss = 0;
         for (int dd = 0; dd < 6; ++dd) {
             const unsigned tm = T.tmask[dd];   // the same for the whole beam
 #pragma unroll
             for (int r = 0; r < 9; ++r) {
                 const int axes = (tm >> (3 * r)) & 7u;
                 int idx = vi + T.off[dd][r];
-                bool in = true;
                 if (axes) {
-                    int ii = i + T.ro[dd][r][0], jj = j + T.ro[dd][r][1],
-                        kk = k + T.ro[dd][r][2];
-                    exact_sample(B, T, s, hx, hy, hz, dd, r, axes, ii, jj, kk);
-                    in = (unsigned)ii < (unsigned)g.nx && (unsigned)jj < (unsigned)g.ny &&
-                         (unsigned)kk < (unsigned)g.nz;
-                    idx = in ? ii + sy * jj + sz * kk : vi;
+                    int ui = 0, uj = 0, uk = 0;
+                    exact_steps<POW2>(B, T, s, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj,
+                                      uk);
+                    idx += ui + sy * uj + sz * uk;
                 }
                 const float x = __ldg(R + idx);
-                const bool take = r < nr;
-                sum = (take && in) ? __fadd_rn(sum, x) : sum;
-                miss += (take && !in) ? 1 : 0;
+                sum = r < nr ? __fadd_rn(sum, x) : sum;
             }
         }
-        return __fdiv_rn(sum, (float)(6 * nr + 1 - miss));
+        return __fdiv_rn(sum, (float)(6 * nr + 1));
     }
     int n = 1;
     for (int dd = 0; dd < 6; ++dd) {
         unsigned tm = T.tmask[dd];
 #pragma unroll 1
         for (int r = 0; r < 9; ++r, tm >>= 3) {
-            int ii = i + T.ro[dd][r][0], jj = j + T.ro[dd][r][1], kk = k + T.ro[dd][r][2];
+            int ii = i + __float2int_rd(T.hh[dd][r][0]), jj = j + __float2int_rd(T.hh[dd][r][1]),
+                kk = k + __float2int_rd(T.hh[dd][r][2]);
             const int axes = tm & 7u;
-            if (axes) exact_sample(B, T, s, hx, hy, hz, dd, r, axes, ii, jj, kk);
+            if (axes) {
+                int ui = 0, uj = 0, uk = 0;
+                exact_steps<POW2>(B, T, s, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj, uk);
+                ii += ui;
+                jj += uj;
+                kk += uk;
+            }
             const bool take = r < nr && (unsigned)ii < (unsigned)g.nx &&
                               (unsigned)jj < (unsigned)g.ny && (unsigned)kk < (unsigned)g.nz;
             if (take) {
@@ -544,6 +551,7 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
     return __fdiv_rn(sum, (float)n);
 }
 
+template <bool POW2>
 __global__ void __launch_bounds__(128)
 k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGeomSet bs,
          const __grid_constant__ SmoothSet st, int zbricks, float *__restrict__ wet)
@@ -555,7 +563,7 @@ k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGe
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
-    wet[b * V + v] = smooth_voxel(raw + b * V, g, bs.b[b], st.b[b], i, j, k);
+    wet[b * V + v] = smooth_voxel<POW2>(raw + b * V, g, bs.b[b], st.b[b], i, j, k);
 }
 
 // One (plan, beam) of a batched WET pass.
@@ -625,8 +633,9 @@ k_smooth_batch(const BatchWet *__restrict__ items, int n_items)
     __syncthreads();
     int i, j, k;
     if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
-    W.wet[i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k)] =
-        smooth_voxel(W.raw, W.g, W.geom, sm, i, j, k);
+    float *out = W.wet + i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k);
+    *out = sm.pow2 ? smooth_voxel<true>(W.raw, W.g, W.geom, sm, i, j, k)
+                   : smooth_voxel<false>(W.raw, W.g, W.geom, sm, i, j, k);
 }
 
 int ray_step_cap(const PbGrid &g)
@@ -655,7 +664,10 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *re
                                                   ray_step_cap(g), raw, status);
     PbStatus s = check_launch("k_raytrace");
     if (s != PB_OK) return s;
-    k_smooth<<<grid, block, 0, st>>>(raw, g, bs, ss, zb, wet);
+    if (ss.b[0].pow2)
+        k_smooth<true><<<grid, block, 0, st>>>(raw, g, bs, ss, zb, wet);
+    else
+        k_smooth<false><<<grid, block, 0, st>>>(raw, g, bs, ss, zb, wet);
     return check_launch("k_smooth");
 }
 
