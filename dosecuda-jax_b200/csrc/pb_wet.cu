@@ -503,13 +503,13 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
         (int64_t)g.nx * g.ny * g.nz < ((int64_t)1 << 31)) {
         // Interior: both candidates of every sample lie inside the grid
         // (the margins), so there are no bounds tests and the indexes are
-        // 32-bit.  Radii unrolled: the table offsets are immediates, and a
-        // sample past the voxel's count is loaded and not added, without a
-        // branch.
+        // 32-bit.  A sample past the voxel's count is loaded and not added,
+        // without a branch.  Radii unrolled by three: fully unrolled, the
+        // loop no longer fits the instruction cache.
         const int vi = (int)v, sy = g.nx, sz = g.nx * g.ny;
         for (int dd = 0; dd < 6; ++dd) {
             const unsigned tm = T.tmask[dd];   // the same for the whole beam
-#pragma unroll
+#pragma unroll 3
             for (int r = 0; r < 9; ++r) {
                 const int axes = (tm >> (3 * r)) & 7u;
                 int idx = vi + T.off[dd][r];
