@@ -79,11 +79,29 @@ class Clocks:
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # the sampler takes a moment to start: wait (at most 5 s) for its
+        # first row, so that the rows written from here on fall inside the
+        # timed region that follows
+        self.skip = 0
+        if self.proc is not None:
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.proc.poll() is None:
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.01)
+            self.skip = self._rows_now()
         return self
+
+    def _rows_now(self) -> int:
+        try:
+            self.f.flush()
+            return len([r for r in open(self.path).read().splitlines() if r.strip()])
+        except Exception:
+            return 0
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -98,6 +116,9 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         try:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r]
+            # rows written during the timed region (the one before it when
+            # the region was shorter than the sampling period)
+            rows = rows[self.skip:] or rows[-1:]
             sm = [float(r[0]) for r in rows]
             mx = float(rows[0][1])
             reasons = sorted({names[i] for r in rows for i in range(4)
