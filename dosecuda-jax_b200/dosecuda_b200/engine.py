@@ -380,3 +380,85 @@ def objective(dose: torch.Tensor, presc: torch.Tensor, weight: torch.Tensor,
                                 ptr(weight.contiguous()), n, ptr(obj), ptr(resid), ptr(work),
                                 _stream(dev)), "pb_objective")
     return obj
+
+
+class HostGradientStep:
+    """Objective and spot-weight gradient of a plan from pinned host
+    buffers, the whole round trip of one optimiser step: the HU volume,
+    prescription, voxel weights and spot weights go up, and the dose,
+    gradient and objective come back.
+
+    The copies off the critical path overlap the kernels:
+    * the HU volume goes up first, alone, since the WET needs all of it;
+    * the prescription and voxel weights follow on a copy stream while the
+      WET and dose are computed (they are first read by the objective);
+    * the dose comes back on the copy stream while the adjoint runs.
+    The step ends, on the caller's current stream, once every copy has
+    landed, so the next step may reuse every buffer.  Device buffers are
+    allocated once, here.
+    """
+
+    def __init__(self, dp: DevicePlan, curve_hu: np.ndarray, curve_rlsp: np.ndarray,
+                 wet_mode: str = "texture", scale: float = 1.0):
+        self.dp = dp
+        self.curve = (curve_hu, curve_rlsp)
+        self.wet_mode = wet_mode
+        self.scale = float(scale)
+        dev = dp.device
+        V = dp.n_vox
+        f32 = dict(dtype=torch.float32, device=dev)
+        self.hu = torch.empty(V, **f32)
+        self.presc = torch.empty(V, **f32)
+        self.weights = torch.empty(V, **f32)
+        self.mu_plan = torch.empty(max(dp.n_spots, 1), **f32)
+        self.rlsp = torch.empty(V, **f32)
+        self.dose = torch.empty(V, **f32)
+        self.resid = torch.empty(V, **f32)
+        self.grad_sorted = torch.empty(max(dp.n_spots, 1), **f32)
+        self.obj = torch.empty(1, dtype=torch.float64, device=dev)
+        self.copy_stream = torch.cuda.Stream(dev)
+        self._ev = {k: torch.cuda.Event() for k in ("hu", "inputs", "dose", "out")}
+
+    def __call__(self, hu_h: torch.Tensor, presc_h: torch.Tensor, weights_h: torch.Tensor,
+                 mu_plan_h: torch.Tensor, dose_out: torch.Tensor, grad_out: torch.Tensor,
+                 obj_out: torch.Tensor) -> None:
+        """Enqueue one step on the current stream.  Host tensors are pinned
+        float32 (obj_out float64), V / n_spots elements, spot weights and the
+        gradient in plan row order.  Nothing is synchronised: read the
+        outputs after synchronising the current stream."""
+        dp = self.dp
+        n = dp.n_spots
+        for name, t, m in (("hu", hu_h, dp.n_vox), ("prescription", presc_h, dp.n_vox),
+                           ("voxel weights", weights_h, dp.n_vox), ("dose_out", dose_out, dp.n_vox),
+                           ("spot weights", mu_plan_h, n), ("grad_out", grad_out, n)):
+            if t.numel() != m or t.dtype != torch.float32 or t.device.type != "cpu":
+                raise ValueError(f"{name} must be a host float32 tensor of {m} elements")
+        if obj_out.numel() != 1 or obj_out.dtype != torch.float64 or obj_out.device.type != "cpu":
+            raise ValueError("obj_out must be a host float64 tensor of one element")
+        main = torch.cuda.current_stream(dp.device)
+        cs, ev = self.copy_stream, self._ev
+        # the copy stream may overwrite the inputs once the previous step's
+        # kernels (queued on `main`) are done with them
+        cs.wait_stream(main)
+        self.hu.copy_(hu_h, non_blocking=True)
+        ev["hu"].record(main)
+        self.mu_plan[:n].copy_(mu_plan_h, non_blocking=True)
+        with torch.cuda.stream(cs):
+            cs.wait_event(ev["hu"])
+            self.presc.copy_(presc_h, non_blocking=True)
+            self.weights.copy_(weights_h, non_blocking=True)
+            ev["inputs"].record(cs)
+        rlsp_from_hu(self.hu, *self.curve, out=self.rlsp)
+        dp.compute_wet(self.rlsp, check_status=False, wet_mode=self.wet_mode)
+        dp.forward(dp.to_sorted(self.mu_plan[:n]), scale=self.scale, out=self.dose)
+        ev["dose"].record(main)
+        main.wait_event(ev["inputs"])
+        objective(self.dose, self.presc, self.weights, self.resid, out=self.obj)
+        with torch.cuda.stream(cs):
+            cs.wait_event(ev["dose"])
+            dose_out.copy_(self.dose, non_blocking=True)
+            ev["out"].record(cs)
+        dp.adjoint(self.resid, scale=self.scale, out=self.grad_sorted[:n])
+        grad_out.copy_(dp.to_plan(self.grad_sorted[:n]), non_blocking=True)
+        obj_out.copy_(self.obj, non_blocking=True)
+        main.wait_event(ev["out"])
