@@ -756,7 +756,7 @@ k_cell_flat(const float *__restrict__ rho, PbGrid g, float *__restrict__ value)
 // kRunCap: axis 0 starts from the flat flags, axes 1 and 2 combine the
 // previous pass with max(|offset|, d).
 template <int AXIS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_cell_dist(PbGrid g, const float *__restrict__ value, const unsigned char *__restrict__ din,
             unsigned char *__restrict__ dout)
 {
@@ -768,22 +768,24 @@ k_cell_dist(PbGrid g, const float *__restrict__ value, const unsigned char *__re
          c += (int64_t)gridDim.x * blockDim.x) {
         const int pos = AXIS == 0 ? (int)(c % cx)
                                   : (AXIS == 1 ? (int)((c / cx) % cy) : (int)(c / ((int64_t)cx * cy)));
+        // every tap, unrolled and without branches, so that all the loads
+        // are in flight at once (a tap with |k| >= best cannot lower best,
+        // so taking it changes nothing)
         int best = kRunCap;
+#pragma unroll
         for (int k = -kRunCap; k <= kRunCap; ++k) {
             const int q = pos + k;
             const int ak = k < 0 ? -k : k;
-            if (ak >= best) continue;
-            int d;
-            if (q < 0 || q >= len) {
-                d = 0;
-            } else if (AXIS == 0) {
-                const float v = __ldg(value + c + k);
-                d = (v == v) ? kRunCap : 0;
-            } else {
-                d = __ldg(din + c + k * stride);
+            int d = 0;
+            if (q >= 0 && q < len) {
+                if (AXIS == 0) {
+                    const float v = __ldg(value + c + k);
+                    d = (v == v) ? kRunCap : 0;
+                } else {
+                    d = __ldg(din + c + k * stride);
+                }
             }
-            const int m = ak > d ? ak : d;
-            if (m < best) best = m;
+            best = min(best, max(ak, d));
         }
         dout[c] = (unsigned char)best;
     }
