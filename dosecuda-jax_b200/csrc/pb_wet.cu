@@ -310,10 +310,11 @@ __device__ __forceinline__ float raytrace_voxel(const float *__restrict__ rho,
     return __double2float_rn(fma(0.1, acc, -0.05));
 }
 
-// 12 resident blocks per SM (40 registers): more warps to cover the
-// dependent record loads; measured faster than the unbounded 48 registers.
+// Texture sampling: 12 resident blocks per SM (40 registers), more warps to
+// cover the dependent record loads; measured faster than the unbounded 48
+// registers.  The exact-trilinear version spills at 40 and is left unbounded.
 template <bool TEX>
-__global__ void __launch_bounds__(128, 12)
+__global__ void __launch_bounds__(128, TEX ? 12 : 1)
 k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex,
            const float2 *__restrict__ rec, PbGrid g, const __grid_constant__ BeamGeomSet bs,
            int zbricks, int cap, float *__restrict__ raw, int *status)
@@ -553,8 +554,11 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
     return __fdiv_rn(sum, (float)n);
 }
 
+// 12 resident blocks per SM (40 registers) with a power-of-two spacing,
+// measured faster; with the division call the kernel spills at 40 and is
+// left unbounded.
 template <bool POW2>
-__global__ void __launch_bounds__(128, 12)
+__global__ void __launch_bounds__(128, POW2 ? 12 : 1)
 k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGeomSet bs,
          const __grid_constant__ SmoothSet st, int zbricks, float *__restrict__ wet)
 {
