@@ -336,11 +336,11 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex,
 // linear and the voxel's own coordinate is an integer), where dm_a is the
 // index step of 1 mm along the direction.  Where the fractional part of
 // dr * dm_a is farther than the rounding bound from 0.5, roundf picks
-// i_a + ro for every voxel of the beam; the other (direction, radius,
-// axis) triples are flagged in tmask and take the reference-order position
-// per voxel, which is i_a + ro or i_a + ro + 1 with ro = floor(dr * dm_a).
-// The table holds ro + 1/2 (hh), the half-integer the flagged position is
-// compared with.
+// i_a + ro, ro = round(dr * dm_a), for every voxel of the beam.  The other
+// (direction, radius, axis) triples are flagged in tmask and take the
+// reference-order position per voxel, which is i_a + ro or i_a + ro + 1
+// with ro = floor(dr * dm_a) there.  The table holds ro + 1/2 (hh): for a
+// flagged triple, the half-integer the position is compared with.
 struct SmoothBeam {
     int off[6][9];            // linear-index offset when no axis is flagged
     float rc[6][9], rs[6][9]; // dr * cos, dr * sin in FP32 (the reference's products)
