@@ -269,6 +269,22 @@ PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
                       raw_work_dev, wet_dev, status_dev, static_cast<cudaStream_t>(stream));
 }
 
+PbStatus pb_smooth_table(const PbGrid *grid, const PbBeamGeom *beams, int n_beams, int beam,
+                         int *off, float *hh, unsigned *tmask, int *margin)
+{
+    PbStatus s = check_grid(grid);
+    if (s != PB_OK) return s;
+    if (!beams || !off || !hh || !tmask || !margin)
+        return set_error(PB_ERR_INVALID, "NULL argument");
+    if (n_beams <= 0 || n_beams > PB_MAX_BEAMS)
+        return set_error(PB_ERR_INVALID, "n_beams must be in [1, %d] (got %d)", PB_MAX_BEAMS,
+                         n_beams);
+    if (beam < 0 || beam >= n_beams)
+        return set_error(PB_ERR_INVALID, "beam %d is not in [0, %d)", beam, n_beams);
+    smooth_table_host(*grid, beams, n_beams, beam, off, hh, tmask, margin);
+    return PB_OK;
+}
+
 PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams, const float *wet_dev,
                  const PbLayer *layers_dev, const float *spot_geo_dev, const float *mu_dev,
                  float scale, float *dose_dev, float *beam_dose_dev, void *stream)

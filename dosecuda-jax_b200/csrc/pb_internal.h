@@ -30,6 +30,11 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *re
                     float *wet, int *status, cudaStream_t st);
 
 // Batched WET pass (pb_wet.cu): one record per (plan, beam).
+// The smoothing sample table of one beam (pb_wet.cu), as the WET launch
+// builds it: off[6][9], hh[6][9][3], tmask[6], margin[3].
+void smooth_table_host(const PbGrid &g, const PbBeamGeom *beams, int n_beams, int beam,
+                       int *off, float *hh, unsigned *tmask, int *margin);
+
 size_t batch_wet_size();
 long long fill_batch_wet(void *items_host, int first, const PbGrid &g, const PbBeamGeom *beams,
                          int n_beams, const float *rlsp, cudaTextureObject_t tex,

@@ -677,6 +677,18 @@ PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *re
     return check_launch("k_smooth");
 }
 
+void smooth_table_host(const PbGrid &g, const PbBeamGeom *beams, int n_beams, int beam,
+                       int *off, float *hh, unsigned *tmask, int *margin)
+{
+    SmoothSet ss;
+    smooth_set(g, beams, n_beams, ss);
+    const SmoothBeam &T = ss.b[beam];
+    memcpy(off, T.off, sizeof(T.off));
+    memcpy(hh, T.hh, sizeof(T.hh));
+    memcpy(tmask, T.tmask, sizeof(T.tmask));
+    memcpy(margin, T.margin, sizeof(T.margin));
+}
+
 size_t batch_wet_size() { return sizeof(BatchWet); }
 
 // Fills the batch records of one plan's beams; returns the bricks they use.

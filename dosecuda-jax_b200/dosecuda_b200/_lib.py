@@ -117,6 +117,7 @@ _SIGS = {
     "pb_texture_destroy": (_I, [ctypes.c_uint64]),
     "pb_wet": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),
     "pb_wet_noalloc": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP]),
+    "pb_smooth_table": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _I, _VP, _VP, _VP, _VP]),
     "pb_dose": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP, _VP, _VP]),
     "pb_dose_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP,
                              _VP]),
@@ -188,6 +189,22 @@ def beam_setup(gantry_deg: float, couch_deg: float, vsadx: float, vsady: float,
     check(lib.pb_beam_setup(float(gantry_deg), float(couch_deg), float(vsadx), float(vsady),
                             ptr(iso), ptr(origin), ctypes.byref(g)), "pb_beam_setup")
     return g
+
+
+def smooth_table(shape, spacing: float, geoms, beam: int = 0):
+    """The smoothing sample table of one beam, as the WET pass builds it:
+    (off [6, 9], hh [6, 9, 3], tmask [6], margin [3]); see pb_smooth_table."""
+    nz, ny, nx = shape
+    grid = PbGrid(int(nx), int(ny), int(nz), float(spacing))
+    arr = (PbBeamGeom * len(geoms))(*geoms)
+    off = np.zeros((6, 9), np.int32)
+    hh = np.zeros((6, 9, 3), np.float32)
+    tmask = np.zeros(6, np.uint32)
+    margin = np.zeros(3, np.int32)
+    check(lib.pb_smooth_table(ctypes.byref(grid), ctypes.cast(arr, ctypes.c_void_p), len(geoms),
+                              int(beam), ptr(off), ptr(hh), ptr(tmask), ptr(margin)),
+          "pb_smooth_table")
+    return off, hh, tmask, margin
 
 
 def build_layers(spot_list: np.ndarray, dvp: np.ndarray):

@@ -192,6 +192,19 @@ PbStatus pb_wet_noalloc(const float *rlsp_dev, PbTexture tex, const PbGrid *grid
                         const PbBeamGeom *beams, int n_beams, float *wet_dev,
                         int *status_dev, void *stream);
 
+/* The lateral-smoothing sample table that pb_wet builds for beam `beam` of
+ * the n_beams given, on the host (no GPU needed).  No counterpart in the
+ * reference: it exposes how the smoothing (IMPTClasses.cu:166-198) picks
+ * its samples, for tests and inspection.  For direction d (angle d*pi/3)
+ * and radius r+1 mm, sample (d, r) of voxel (i, j, k) is, along axis a,
+ * at index i_a + floor(hh[(d*9 + r)*3 + a]), or one more where bit 3r+a of
+ * tmask[d] is set (a half-voxel tie, decided per voxel in the reference's
+ * FP32 order); off[d*9 + r] is the linear offset of the unflagged position.
+ * Voxels with margin[a] <= i_a <= n_a - 1 - margin[a] have every candidate
+ * inside the grid.  Sizes: off 54, hh 162, tmask 6, margin 3. */
+PbStatus pb_smooth_table(const PbGrid *grid, const PbBeamGeom *beams, int n_beams, int beam,
+                         int *off, float *hh, unsigned *tmask, int *margin);
+
 /* Forward pencil-beam dose of a plan (IMPTClasses.cu:204-271) for all of
  * its beams in one launch.  wet_dev: n_beams x V (cm).  layers_dev: all
  * layers, beam-major.  spot_geo_dev: PB_SPOT_GEO_FLOATS per spot, mu_dev:

@@ -67,6 +67,7 @@ def load(port32: bool = False):
     lib.ob_raytrace.restype = i
     lib.ob_smooth.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp, i64, vp]
     lib.ob_smooth_f32.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp]
+    lib.ob_smooth_choices.argtypes = [ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp]
     lib.ob_build_layers.argtypes = [vp, i, vp, i, i, vp, vp]
     lib.ob_build_layers.restype = i
     lib.ob_dose.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam),
@@ -142,6 +143,15 @@ def smooth_f32(raw_f32, spacing, beam: OBeam):
     out = np.zeros(raw.shape, np.float32)
     lib.ob_smooth_f32(_p(raw), ctypes.byref(_grid(raw.shape, spacing)), ctypes.byref(beam),
                       _p(out))
+    return out
+
+
+def smooth_choices(shape, spacing, beam: OBeam):
+    """Index (i, j, k) the reference picks for every smoothing sample of
+    every voxel: int32 [nz, ny, nx, 6 directions, 9 radii, 3 axes]."""
+    lib = load()
+    out = np.zeros(tuple(shape) + (6, 9, 3), np.int32)
+    lib.ob_smooth_choices(ctypes.byref(_grid(shape, spacing)), ctypes.byref(beam), _p(out))
     return out
 
 

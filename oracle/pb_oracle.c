@@ -353,6 +353,41 @@ void ob_smooth(const float *raw, const ob_grid *g, const ob_beam *b,
     }
 }
 
+/* The voxel index (i, j, k) that the reference's FP32 arithmetic picks for
+ * every smoothing sample of every voxel, whether or not the sample is in
+ * the grid or within the voxel's radius limit: out[((v*6 + d)*9 + r)*3 + a]
+ * for direction d, radius r+1 mm, axis a (IMPTClasses.cu:178-186). */
+void ob_smooth_choices(const ob_grid *g, const ob_beam *b, int32_t *out)
+{
+    float dc[6], ds[6];
+    ob_smooth_dirs(dc, ds);
+    int64_t nv = (int64_t)g->nx * g->ny * g->nz;
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < nv; v++) {
+        int i = (int)(v % g->nx);
+        int j = (int)((v / g->nx) % g->ny);
+        int k = (int)(v / ((int64_t)g->nx * g->ny));
+        float p[3], h[3];
+        vox_mm(g, b, i, j, k, p);
+        image_to_head_f(b, p, h);
+        for (int d = 0; d < 6; d++) {
+            float dr = 1.0f;
+            for (int r = 0; r < 9; r++) {
+                float hc[3], pc[3];
+                hc[0] = h[0] + dr * dc[d];
+                hc[1] = h[1] + dr * ds[d];
+                hc[2] = h[2];
+                head_to_image_f(b, hc, pc);
+                int32_t *o = out + ((v * 6 + d) * 9 + r) * 3;
+                o[0] = (int32_t)roundf((pc[0] + b->iso[0]) / g->s);
+                o[1] = (int32_t)roundf((pc[1] + b->iso[1]) / g->s);
+                o[2] = (int32_t)roundf((pc[2] + b->iso[2]) / g->s);
+                dr += 1.0f;
+            }
+        }
+    }
+}
+
 /* The smoothing with the reference's own arithmetic: an FP32 sum in
  * sample order and an FP32 quotient (IMPTClasses.cu:168-198), so that a
  * kernel choosing the same voxels gives the same bits. */

@@ -136,3 +136,63 @@ def test_invalid_arguments_return_status_without_a_gpu():
     assert L.pb_proton_raytrace_host(0, 1340.0, 1930.0, _lib.ptr(buf), _lib.ptr(dims),
                                      ctypes.c_float(2.0), _lib.ptr(buf), _lib.ptr(buf), 0.0, 0.0,
                                      _lib.ptr(buf)) == _lib.PB_ERR_INVALID
+
+
+def _smoothing_cases(n):
+    rng = np.random.default_rng(17)
+    spacings = [1.0, 1.5, 2.0, 2.5, 3.0, 0.9765625, 1.171875, 2.34375, 1.2]
+    for c in range(n):
+        gantry = [0.0, 90.0, 180.0, 270.0][c % 4] if c % 2 == 0 else float(rng.uniform(0, 360))
+        couch = [0.0, 90.0, 270.0, float(rng.uniform(-90, 90))][(c // 2) % 4]
+        s = spacings[c % len(spacings)]
+        shape = tuple(int(x) for x in rng.integers(8, 22, 3))
+        iso = rng.uniform(-100, 100, 3).astype(np.float32)
+        origin = (-(np.array(shape[::-1]) * s) / 2 + rng.uniform(-20, 20, 3)).astype(np.float32)
+        yield gantry, couch, s, shape, iso, origin
+
+
+def test_smoothing_table_holds_the_reference_samples(oracle):
+    """The WET pass's smoothing table (pb_smooth_table) against the voxels
+    the reference's FP32 arithmetic picks (oracle), for every sample of
+    every voxel, over 180 beams: axis-aligned and oblique gantries, couch
+    rotations, 9 spacings (powers of two and not), random isocentres.  An
+    unflagged sample is exactly the table's voxel; a flagged one (a
+    half-voxel tie) is that voxel or the next; the linear offsets agree with
+    the per-axis ones; inside the margins every candidate is in the grid."""
+    from dosecuda_b200 import _lib
+    n_flag = 0
+    for gantry, couch, s, shape, iso, origin in _smoothing_cases(180):
+        geom = _lib.beam_setup(gantry, couch, 1340.0, 1930.0, iso, origin)
+        ob = oracle.beam_setup(gantry, couch, 1340.0, 1930.0, iso, origin)
+        off, hh, tmask, margin = _lib.smooth_table(shape, s, [geom], 0)
+        ro = np.floor(hh).astype(np.int64)
+        assert np.array_equal(hh, ro + 0.5)
+        nz, ny, nx = shape
+        assert np.array_equal(off, ro[..., 0] + nx * ro[..., 1] + nx * ny * ro[..., 2])
+        bit = 3 * np.arange(9)[:, None] + np.arange(3)[None, :]
+        flag = ((tmask[:, None, None] >> bit[None]) & 1).astype(bool)      # [6, 9, 3]
+        n_flag += int(flag.sum())
+        got = oracle.smooth_choices(shape, s, ob).astype(np.int64)        # [z, y, x, 6, 9, 3]
+        k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        own = np.stack([i, j, k], -1)[:, :, :, None, None, :]
+        step = got - (own + ro)
+        assert np.all(step[..., ~flag] == 0), (gantry, couch, s)
+        assert np.all((step[..., flag] == 0) | (step[..., flag] == 1)), (gantry, couch, s)
+        n = np.array([nx, ny, nz])
+        lo_ok = own[..., 0, 0, :] - margin >= 0
+        hi_ok = own[..., 0, 0, :] + margin <= n - 1
+        inner = np.all(lo_ok & hi_ok, -1)
+        if inner.any():
+            cand_lo = (own + ro)[inner]
+            cand_hi = cand_lo + flag
+            assert cand_lo.min() >= 0 and np.all(cand_hi <= n - 1)
+    assert n_flag > 0   # the axis-aligned beams do have ties
+
+
+def test_smoothing_table_rejects_bad_arguments():
+    from dosecuda_b200 import _lib
+    geom = _lib.beam_setup(0.0, 0.0, 1340.0, 1930.0, [0, 0, 0], [0, 0, 0])
+    with pytest.raises(_lib.PbError):
+        _lib.smooth_table((10, 10, 10), 2.0, [geom], 1)
+    with pytest.raises(_lib.PbError):
+        _lib.smooth_table((10, 0, 10), 2.0, [geom], 0)
