@@ -878,7 +878,9 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                             sh.gsum[sl] = 0.0f;
                         }
                     } else {
-#pragma unroll 2
+                        // unrolled by 8: more independent exp2 chains in
+                        // flight (measured: 8.57 -> 8.29 ms against 2)
+#pragma unroll 8
                         for (int c = 0; c < n2; ++c) {
                             const SpotRec r = s_spot[c];
                             const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b);
@@ -892,7 +894,7 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
                                 AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], qq)), AH[p]);
                             }
                         }
-#pragma unroll 2
+#pragma unroll 8
                         for (int c = kCap - n1; c < kCap; ++c) {
                             const SpotRec r = s_spot[c];
                             const float2 nx = lo2(r.a), ny = hi2(r.a), tx = lo2(r.b);
