@@ -946,11 +946,18 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
 #ifndef PB_DOSE_MIN_BLOCKS
 #define PB_DOSE_MIN_BLOCKS 5
 #endif
-// Resident blocks per SM the forward kernels are compiled for.
-template <int NT> constexpr int dose_min_blocks() { return NT == 128 ? PB_DOSE_MIN_BLOCKS : 3; }
+// Resident blocks per SM the kernels are compiled for (their register
+// budget).  Shapes of 128 threads that cull one round of 128 spots (the
+// forward's default) take one more block: measured 8.28 -> 8.19 ms.  The
+// adjoint (two rounds) stays at PB_DOSE_MIN_BLOCKS: one more made it
+// slower (9.16 -> 9.23 ms).
+template <int NT, int KCULL = 2> constexpr int dose_min_blocks()
+{
+    return NT == 128 ? PB_DOSE_MIN_BLOCKS + (KCULL == 1 ? 1 : 0) : 3;
+}
 
 template <int NT, int VPT, int KCULL, bool BEAM_OUT>
-__global__ void __launch_bounds__(NT, dose_min_blocks<NT>())
+__global__ void __launch_bounds__(NT, dose_min_blocks<NT, KCULL>())
 k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
        const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
        const float *__restrict__ mu, float *__restrict__ dose,
@@ -962,7 +969,7 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 
 // The forward's SFU exponentials and spot-voxel evaluations, counted with
 // its own decisions (dose_tile with COUNT); shape of pb_dose's kernel.
-__global__ void __launch_bounds__(128, dose_min_blocks<128>())
+__global__ void __launch_bounds__(128, dose_min_blocks<128, 1>())
 k_dose_count(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
              const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
              unsigned long long *count)
@@ -1034,7 +1041,7 @@ struct BatchDose {
 // one queue until it is empty.  Plans are stored in decreasing order of
 // estimated cost per tile so that the expensive tiles start first.
 template <int NT, int VPT, int KCULL>
-__global__ void __launch_bounds__(NT, dose_min_blocks<NT>())
+__global__ void __launch_bounds__(NT, dose_min_blocks<NT, KCULL>())
 k_dose_batch(const BatchDose *__restrict__ plans, int n_plans, long long n_items,
              unsigned long long *counter)
 {

@@ -106,12 +106,24 @@ def tune_plan(dp, reps: int = 3, use_cache: bool = True) -> int:
     return v
 
 
+def rounds_of(name: str) -> int:
+    """Rounds of spots a kernel shape culls at once (t<threads>_v<vpt>_c<k>)."""
+    return int(name.split("_")[2][1:])
+
+
+def max_blocks_per_sm(name: str) -> int:
+    """Resident blocks per SM a kernel shape is compiled for: 6 for 128
+    threads with one round, 5 for other 128-thread shapes, 3 for 256."""
+    if threads_of(name) != 128:
+        return 3
+    return 6 if rounds_of(name) == 1 else 5
+
+
 def batch_candidates():
     """(variant, blocks per SM) pairs the batch launch accepts."""
     out = []
     for v, name in enumerate(variants()):
-        top = 5 if threads_of(name) == 128 else 3
-        for bps in range(2, top + 1):
+        for bps in range(2, max_blocks_per_sm(name) + 1):
             out.append((v, bps))
     return out
 

@@ -16,7 +16,11 @@ def test_variants_and_batch_candidates():
     cands = autotune.batch_candidates()
     for v, bps in cands:
         assert 0 <= v < len(names)
-        assert 2 <= bps <= (5 if autotune.threads_of(names[v]) == 128 else 3)
+        assert 2 <= bps <= autotune.max_blocks_per_sm(names[v])
+    assert autotune.max_blocks_per_sm("t128_v4_c1") == 6
+    assert autotune.max_blocks_per_sm("t128_v4_c2") == 5
+    assert autotune.max_blocks_per_sm("t256_v2_c1") == 3
+    assert (0, 6) in cands
 
 
 def test_cache_roundtrip(tmp_path, monkeypatch):
