@@ -167,8 +167,10 @@ __device__ __forceinline__ float ray_sample(const float *__restrict__ rho,
 // 0.1 * sum(max(RLSP, 0)).  The sum is carried in FP64 (FP32 partials of 8
 // samples).  A ray that exceeds the grid-diagonal step cap stops and raises
 // PB_ERR_RAY_CAP in *status.  The leading samples that are certainly inside
-// the grid (safe_steps) are taken 8 at a time without the in-grid test, so
-// that several texture fetches are in flight per thread.
+// the grid (safe_steps) go without the in-grid test: with cell records, as
+// runs through flat cells (flat_run) and bursts of kTexBurst fetches
+// elsewhere; without them, 8 fetches at a time.  Either way several
+// fetches are in flight per thread.
 //
 // TEX = true samples RLSP through a border-0, linearly filtered 3-D texture
 // and forms the ray direction with rnorm3df, as the reference does
