@@ -139,6 +139,9 @@ def test_invalid_arguments_return_status_without_a_gpu():
 
 
 def _smoothing_cases(n):
+    """Beams over small grids; every third case puts the grid and the
+    isocentre far from the coordinate origin (hundreds of mm), where the
+    FP32 positions round more coarsely."""
     rng = np.random.default_rng(17)
     spacings = [1.0, 1.5, 2.0, 2.5, 3.0, 0.9765625, 1.171875, 2.34375, 1.2]
     for c in range(n):
@@ -146,8 +149,12 @@ def _smoothing_cases(n):
         couch = [0.0, 90.0, 270.0, float(rng.uniform(-90, 90))][(c // 2) % 4]
         s = spacings[c % len(spacings)]
         shape = tuple(int(x) for x in rng.integers(8, 22, 3))
-        iso = rng.uniform(-100, 100, 3).astype(np.float32)
-        origin = (-(np.array(shape[::-1]) * s) / 2 + rng.uniform(-20, 20, 3)).astype(np.float32)
+        if c % 3 == 2:
+            iso = rng.uniform(-400, 400, 3).astype(np.float32)
+            origin = rng.uniform(-700, 700, 3).astype(np.float32)
+        else:
+            iso = rng.uniform(-100, 100, 3).astype(np.float32)
+            origin = (-(np.array(shape[::-1]) * s) / 2 + rng.uniform(-20, 20, 3)).astype(np.float32)
         yield gantry, couch, s, shape, iso, origin
 
 
@@ -155,7 +162,8 @@ def test_smoothing_table_holds_the_reference_samples(oracle):
     """The WET pass's smoothing table (pb_smooth_table) against the voxels
     the reference's FP32 arithmetic picks (oracle), for every sample of
     every voxel, over 180 beams: axis-aligned and oblique gantries, couch
-    rotations, 9 spacings (powers of two and not), random isocentres.  An
+    rotations, 9 spacings (powers of two and not), random isocentres, a
+    third of them hundreds of mm from the origin.  An
     unflagged sample is exactly the table's voxel; a flagged one (a
     half-voxel tie) is that voxel or the next; the linear offsets agree with
     the per-axis ones; inside the margins every candidate is in the grid."""
