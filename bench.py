@@ -7,23 +7,36 @@ target, 4 beams (0/90/180/270 deg) with ~20,000 spots on 5 mm lattices, and
 the quadratic objective sum_v w_v (D_v - P_v)^2 (P = 60 in the target, 0
 outside; w = 1 / 0.1).  Synthetic, seeded data (no clinical CT exists here).
 
-One step = one plan evaluation with its spot-weight gradient:
-    HU -> RLSP -> WET of 4 beams -> forward dose -> FP64 objective + residual
-    -> adjoint (d objective / d spot weight)
-The plain forward (HU -> RLSP -> WET -> dose) is timed beside it.
+Modes (the same in both arms, so that their lines compare like for like):
+  forward  (default) one step = one plan's dose from its CT:
+           HU -> RLSP -> WET of 4 beams -> dose.  The reference has this
+           path and nothing more, so this is the step both arms time.
+  grad     one step = dose + spot-weight gradient:
+           HU -> RLSP -> WET -> dose -> FP64 objective + residual -> adjoint.
+           The reference has no gradient: its arm prints "unavailable".
+The forward line carries the dose + gradient timing too (`dose_grad`).
 
 metric  spot-voxel evals/s = E / t_step, where E is the reference kernel's
         dense pair count sum_beams sum_layers |{v: 10 WET <= 1.1 R80}| x spots
         (the same E for every implementation, so culling counts as speed).
 
+`value` is timed with the inputs already in HBM.  `e2e` is the same step
+through the public host API: in forward mode IMPTDoseGrid.computeIMPTPlan
+(host HU in; host dose, per-beam doses and RLSP out, as the reference's
+computeIMPTPlan returns them), in grad mode the library's host-buffer
+optimiser step.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+                    [--mode forward|grad] [--workload plan|batch|optimize]
 
 N > 1 runs N independent replicas (one plan per GPU, seeds differ), launched
 with torch.distributed.run; the reported value is the sum over ranks of the
 work divided by the slowest rank's time.  --impl reference times the
 reference's own CUDA module (dose_kernels built from its sources for sm_100a
-into oracle/_ref) through its host-buffer API on the same workload; it has
-no gradient, so its step is the plain forward.
+into oracle/_ref) through its host-buffer API on the same workload, driven
+by a restatement of its computeIMPTPlan loop; that process loads no library
+of this package (it builds the workload from the package's host-side plan
+classes, which do not load libpb_b200.so).
 """
 from __future__ import annotations
 
@@ -47,10 +60,11 @@ for _p in (os.path.join(ROOT, "dosecuda-jax_b200"), ROOT):
 METRIC = "IMPT dose+grad ms/plan (20k spots, 256²×160) vs plain fwd; spot-voxel evals/s"
 UNIT = "spot-voxel evals/s"
 L2_FLUSH_BYTES = 256 << 20
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_dose launch of the
-# default workload (seed 3, texture WET), from the ncu --set full capture
-# summarised in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md
-K_DOSE_TRAFFIC = 169_035_520 + 32_191_488
+L2_NOTE = "flushed (256 MiB write) between timed iterations"
+# dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu captures of
+# this workload (seed 3, texture WET) on the kernels as built now; the command
+# and the figures are in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md
+NCU_TRAFFIC = {"k_dose": None, "k_adjoint_tile": None}
 
 
 def _peaks():
@@ -149,21 +163,74 @@ def _sum_over_ranks(x: float, world: int, device) -> float:
     return replicas.sum_over_ranks(x, world, device)
 
 
+# ---------------------------------------------------------------- workload
+
+def plan_case(seed: int):
+    """The benchmarked plan (seeded), built from host-side classes only."""
+    from dosecuda_b200 import phantoms
+    return phantoms.config_gradient(seed=seed)
+
+
+def beam_model(plan, beam):
+    """The beam's model, looked up by its range-shifter label as the
+    reference's computeIMPTPlan does (plan_impt.py:187-192)."""
+    labels = list(plan.dicom_rangeshifter_label.astype(str))
+    return plan.beam_models[labels.index(beam.dicom_rangeshifter_label)]
+
+
+def spot_count(plan) -> int:
+    return int(sum(np.asarray(b.spot_list).reshape(-1, 4).shape[0] for b in plan.beam_list))
+
+
+def plan_config(case, mode: str) -> dict:
+    """The `config` object both arms print for the plan workload."""
+    g, plan = case.grid, case.plan
+    nz, ny, nx = g.HU.shape
+    steps = {"forward": "HU -> RLSP -> WET -> dose",
+             "grad": "HU -> RLSP -> WET -> dose -> objective -> adjoint"}[mode]
+    return {"workload": f"heterogeneous {nx}x{ny}x{nz} @{g.spacing[0]:g}mm, "
+                        f"{len(plan.beam_list)} beams, {spot_count(plan)} spots, "
+                        f"{mode} ({steps})",
+            "voxels": int(nx * ny * nz), "beams": len(plan.beam_list),
+            "spots": spot_count(plan), "mode": mode, "l2": L2_NOTE}
+
+
+def reference_copy_bytes(case) -> tuple:
+    """Bytes the reference's host API moves per plan: for each beam,
+    proton_raytrace_cuda copies the RLSP volume up (its texture) and the
+    smoothed WET back; proton_spot_cuda copies RLSP, WET, layers, spots,
+    divergence parameters and the three LUTs up and the dose back
+    (IMPTClasses.cu:274-340)."""
+    g, plan = case.grid, case.plan
+    V = int(np.prod(g.HU.shape))
+    h2d = d2h = 0
+    for beam in plan.beam_list:
+        m = beam_model(plan, beam)
+        sl = np.asarray(beam.spot_list).reshape(-1, 4)
+        n_layers = len(np.unique(sl[:, 3]))
+        n_e, lut_len = np.shape(m.lut_depths)
+        h2d += 4 * V                                    # raytrace: RLSP texture
+        d2h += 4 * V                                    # raytrace: WET
+        h2d += 8 * V + 20 * n_layers + 16 * len(sl)     # spot: RLSP, WET, layers, spots
+        h2d += 4 * n_e * (np.shape(m.divergence_params)[1] + 3 * lut_len)
+        d2h += 4 * V                                    # spot: dose
+    return h2d, d2h
+
+
 # ------------------------------------------------------------------ mine
 
 def run_mine(args, world, rank, local):
     import torch
 
-    from dosecuda_b200 import engine, phantoms
+    from dosecuda_b200 import engine
     from dosecuda_b200.plan_impt import _hu_curve
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    case = phantoms.config_gradient(seed=args.seed + rank)
+    case = plan_case(args.seed + rank)
     g, plan = case.grid, case.plan
     curve = _hu_curve(plan.machine_name)
-    shape = g.HU.shape
-    V = int(np.prod(shape))
+    V = int(np.prod(g.HU.shape))
 
     dp = g.prepareIMPTPlan(plan, local, wet_mode=args.wet_mode)
     E = dp.count_pairs()
@@ -214,13 +281,16 @@ def run_mine(args, world, rank, local):
                                                                             resid)), record)
         timed("adjoint", lambda: dp.adjoint(resid, out=grad_sorted), record)
 
-    # end to end: the library's host-buffer step (inputs up from pinned host
-    # memory, dose / gradient / objective back), copies overlapped with the
-    # kernels where they are off the critical path
+    # end to end through the public host API
     host_step = engine.HostGradientStep(dp, *curve, wet_mode=args.wet_mode)
 
-    def e2e_step():
+    def e2e_grad():
         host_step(hu_h, presc_h, wts_h, mu_h, dose_out, grad_out, obj_out)
+
+    def e2e_forward():
+        # the reference's call: host HU in; host dose, per-beam doses and
+        # RLSP out (spot sort, layer build, texture creation included)
+        g.computeIMPTPlan(plan, local, wet_mode=args.wet_mode)
 
     def run_timed(fn, k):
         times = []
@@ -236,104 +306,152 @@ def run_mine(args, world, rank, local):
             times.append(a.elapsed_time(b))
         return times
 
+    head = forward if args.mode == "forward" else step
+    e2e_fn = e2e_forward if args.mode == "forward" else e2e_grad
     for _ in range(args.warmup):
         step()
         forward()
-        e2e_step()
+        e2e_fn()
     torch.cuda.synchronize(dev)
 
     with Clocks(local) as clk:
-        t_step = run_timed(lambda: step(record=True), args.steps)
-    t_fwd = run_timed(forward, args.steps)
-    t_e2e = run_timed(e2e_step, args.steps)
+        t_head = run_timed(head, args.steps)
+    t_fwd = t_head if args.mode == "forward" else run_timed(forward, args.steps)
+    t_step = run_timed(lambda: step(record=True), args.steps)
+    t_e2e = run_timed(e2e_fn, args.steps)
     torch.cuda.synchronize(dev)
     kms = {k: (sum(a.elapsed_time(b) for a, b in v) / len(v)) if v else None
            for k, v in kt.items()}
 
-    ms_step = _max_over_ranks(sum(t_step) / len(t_step), world, dev)
+    ms_head = _max_over_ranks(sum(t_head) / len(t_head), world, dev)
     ms_fwd = _max_over_ranks(sum(t_fwd) / len(t_fwd), world, dev)
+    ms_step = _max_over_ranks(sum(t_step) / len(t_step), world, dev)
     ms_e2e = _max_over_ranks(sum(t_e2e) / len(t_e2e), world, dev)
     E_all = _sum_over_ranks(float(E), world, dev)
-    h2d = 4 * (hu.numel() + presc.numel() + wts.numel() + mu_plan.numel())
-    d2h = 4 * (dose.numel() + n_spots) + 8
+    if args.mode == "forward":
+        # computeIMPTPlan: the HU volume and the spot lists up; dose, every
+        # beam's dose and the RLSP volume back
+        h2d = 4 * V + 16 * n_spots
+        d2h = 4 * V * (2 + dp.n_beams)
+    else:
+        h2d = 4 * (hu.numel() + presc.numel() + wts.numel() + mu_plan.numel())
+        d2h = 4 * (dose.numel() + n_spots) + 8
 
-    peaks, peak_kind = _peaks()
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
-    # dominant kernel: the forward pencil-beam kernel (k_dose, one launch per step)
-    bytes_dose = 4 * V * (dp.n_beams + 1) + 36 * n_spots + \
-        sum(t.dvp.numel() + 3 * t.depths.numel() for t in dp.tables) * 4
-    achieved = bytes_dose / (kms["dose"] * 1e-3) / 1e9
-    # SFU roofline of the same kernel: the exp2 operations one launch issues
-    # (counted with its own culling decisions) over its time, against the
-    # exp2 throughput measured on this GPU now
-    n_ex2, n_eval = dp.count_evaluated()
-    ex2_peak = engine.measure_ex2_rate(dev)
-    ex2_achieved = n_ex2 / (kms["dose"] * 1e-3)
-    # DRAM traffic of one k_dose launch from the ncu capture of this workload
-    traffic = K_DOSE_TRAFFIC if (args.seed == 3 and args.wet_mode == "texture") else None
     line = {
         "metric": METRIC,
-        "value": E_all / (ms_step * 1e-3),
+        "value": E_all / (ms_head * 1e-3),
         "unit": UNIT,
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms_step,
+        "ms_per_step": ms_head,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 (FP64 WET integration and objective)",
         "data": "synthetic (seeded phantom and spot plan)",
-        "config": {"workload": "heterogeneous 256x256x160 @2mm, 4 beams, "
-                               f"{n_spots} spots, quadratic objective (dose+grad)",
-                   "voxels": V, "beams": dp.n_beams, "spots": n_spots,
-                   "dense_pairs_E": E, "wet_mode": args.wet_mode,
-                   "l2": "flushed (256 MiB write) between timed iterations",
-                   "parallelism": f"replicas x{world}"},
+        "config": plan_config(case, args.mode),
+        "dense_pairs_E": E,
+        "wet_mode": args.wet_mode,
+        "parallelism": f"replicas x{world}",
         "fwd_ms_per_plan": ms_fwd,
-        "dose_grad_over_fwd": ms_step / ms_fwd,
+        "dose_grad": {"ms_per_plan": ms_step, "value": E_all / (ms_step * 1e-3), "unit": UNIT,
+                      "over_fwd": ms_step / ms_fwd},
         "kernel_ms": kms,
         "e2e": {"value": E_all / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        # per step: HU->RLSP, [texture mode: five cell-record passes], ray trace,
-        # smoothing, pencil-beam sum, objective (two), adjoint
-        "gpu_launches": (12 if args.wet_mode == "texture" else 7) * args.steps,
-        "roofline": {"kernel": "k_dose (forward pencil-beam sum)", "bound": "hbm",
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": f"of {peak_kind}",
-                     "algorithmic_bytes_per_launch": bytes_dose, "traffic": traffic},
-        "compute_roofline": {"kernel": "k_dose", "bound": "sfu (exp2)",
-                             "achieved": ex2_achieved, "peak": ex2_peak, "unit": "exp2/s",
-                             "frac": ex2_achieved / ex2_peak,
-                             "peak_kind": "measured now on this GPU (pb_measure_ex2_rate)",
-                             "exp2_per_launch": n_ex2,
-                             "spot_voxel_evaluations_per_launch": n_eval,
-                             "dense_pairs_E": E},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "call": "IMPTDoseGrid.computeIMPTPlan" if args.mode == "forward"
+                else "engine.HostGradientStep"},
+        # per forward step: HU->RLSP, [texture mode: five cell-record passes],
+        # ray trace, smoothing, pencil-beam sum; the grad step adds the
+        # objective (two) and the adjoint
+        "gpu_launches": ((9 if args.wet_mode == "texture" else 4) +
+                         (3 if args.mode == "grad" else 0)) * args.steps,
         "clocks": clk.summary(),
     }
+    line.update(rooflines(dp, kms, V, E, dev))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case, dp, E)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
+def rooflines(dp, kms, V, E, dev) -> dict:
+    """Roofline lines of every kernel group over 1 ms in the step.
+
+    HBM: algorithmic bytes per launch (each input read once, each output
+    written once) over the launch's average CUDA-event time, against the
+    measured copy bandwidth.  SFU: the exp2 operations the launch issues,
+    counted with its own culling decisions, against the exp2 rate measured
+    on this GPU now (the pencil-beam sums are exp2/FMA-issue bound, not
+    traffic bound)."""
+    from dosecuda_b200 import engine
+    peaks, peak_kind = _peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    B, S = dp.n_beams, dp.n_spots
+    lut = sum(t.dvp.numel() + 3 * t.depths.numel() for t in dp.tables) * 4
+    ex2_peak = engine.measure_ex2_rate(dev)
+
+    def hbm_line(kernel, nbytes, ms, traffic=None):
+        a = nbytes / (ms * 1e-3) / 1e9
+        return {"kernel": kernel, "bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
+                "frac": a / hbm, "peak_kind": f"of {peak_kind}",
+                "algorithmic_bytes_per_launch": nbytes, "traffic": traffic}
+
+    def sfu_line(kernel, n_ex2, n_eval, ms):
+        a = n_ex2 / (ms * 1e-3)
+        return {"kernel": kernel, "bound": "sfu (exp2)", "achieved": a, "peak": ex2_peak,
+                "unit": "exp2/s", "frac": a / ex2_peak,
+                "peak_kind": "measured now on this GPU (pb_measure_ex2_rate)",
+                "exp2_per_launch": n_ex2, "spot_voxel_evaluations_per_launch": n_eval,
+                "dense_pairs_E": E}
+
+    # k_dose: WET of every beam read, dose written, per spot 32 B of geometry
+    # and its weight, the LUT rows
+    bytes_dose = 4 * V * (B + 1) + 36 * S + lut
+    n_ex2, n_eval = dp.count_evaluated()
+    out = {"roofline": hbm_line("k_dose (forward pencil-beam sum)", bytes_dose, kms["dose"],
+                                NCU_TRAFFIC["k_dose"]),
+           "compute_roofline": sfu_line("k_dose", n_ex2, n_eval, kms["dose"])}
+    lines = {}
+    if kms.get("adjoint"):
+        # k_adjoint_tile: WET of every beam and dObj/dD read, per spot 32 B of
+        # geometry and its gradient written, the LUT rows
+        bytes_adj = 4 * V * (B + 1) + 36 * S + lut
+        lines["adjoint"] = [hbm_line("k_adjoint_tile", bytes_adj, kms["adjoint"],
+                                     NCU_TRAFFIC["k_adjoint_tile"])]
+        counts = getattr(dp, "count_evaluated_adjoint", None)
+        if counts is not None and getattr(dp, "_last_adjoint_field", None) is not None:
+            a_ex2, a_eval = counts(dp._last_adjoint_field)
+            lines["adjoint"].append(sfu_line("k_adjoint_tile", a_ex2, a_eval, kms["adjoint"]))
+    if kms.get("wet"):
+        # WET pass: RLSP read once (texture fill and cell records), raw WET
+        # written and read back by the smoothing, smoothed WET written
+        lines["wet"] = [hbm_line("WET (cell records + k_raytrace + k_smooth)",
+                                 4 * V * (1 + 3 * B), kms["wet"])]
+    if kms.get("rlsp"):
+        lines["rlsp"] = [hbm_line("k_rlsp", 8 * V, kms["rlsp"])]
+    out["kernel_rooflines"] = lines
+    return out
+
+
 def cpu_baseline(case, dp, E_full):
     """FP32 OpenMP port of the reference algorithm (oracle/libport32.so) on a
     bounded sample: ray trace and pencil-beam dose of all 4 beams at the
     voxels of the axial slice through the target centre."""
+    from dosecuda_b200.plan_impt import _hu_curve
     from oracle import oracle as O
     g, plan = case.grid, case.plan
     shape = g.HU.shape
     nz, ny, nx = shape
     kc = int(np.argmax(case.target.sum(axis=(1, 2))))
     idx = (np.arange(ny * nx, dtype=np.int64) + kc * ny * nx)
-    rlsp = O.rlsp_from_hu(g.HU, *__import__("dosecuda_b200.plan_impt", fromlist=["x"])._hu_curve(
-        plan.machine_name))
+    rlsp = O.rlsp_from_hu(g.HU, *_hu_curve(plan.machine_name))
     wet = dp.wet.cpu().numpy()
     pairs = 0
     t0 = time.perf_counter()
     for b, beam in enumerate(plan.beam_list):
-        m = O.Model(plan.beam_models[0])
+        m = O.Model(beam_model(plan, beam))
         ob = O.beam_setup(beam.gantry_angle, beam.couch_angle, m.vsadx, m.vsady, beam.iso,
                           g.origin, port32=True)
         spots, layers = O.build_layers(beam.spot_list, m.dvp)
@@ -399,7 +517,7 @@ def run_batch(args, world, rank, local):
                    "dense_pairs_E": E, "wet_mode": args.wet_mode,
                    "variant": autotune.variants()[variant], "blocks_per_sm": bps,
                    "plans_per_s": bp.n_plans * world / (ms * 1e-3),
-                   "l2": "flushed (256 MiB write) between timed iterations"},
+                   "l2": L2_NOTE},
         "gpu_launches": 4 * args.steps,
         "clocks": clk.summary(),
     }
@@ -486,7 +604,7 @@ def _oracle_check(case, dp, opt, n_random=600):
         sl = np.asarray(beam.spot_list, np.float32).reshape(-1, 4).copy()
         sl[:, 2] = mu[row: row + len(sl)]
         row += len(sl)
-        m = O.Model(plan.beam_models[0])
+        m = O.Model(beam_model(plan, beam))
         ob = O.beam_setup(beam.gantry_angle, beam.couch_angle, m.vsadx, m.vsady, beam.iso,
                           g.origin)
         spots, layers = O.build_layers(sl, m.dvp)
@@ -500,28 +618,52 @@ def _oracle_check(case, dp, opt, n_random=600):
 
 # -------------------------------------------------------------- reference
 
-def run_reference(args, world, rank, local):
-    if rank != 0:
-        return
-    import torch
+def _unavailable(why: str) -> None:
+    print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
 
-    from dosecuda_b200 import phantoms
-    from dosecuda_b200.plan import VolumeObject
-    from dosecuda_b200.plan_impt import _hu_curve
-    from oracle import oracle as O
+
+def load_reference_module():
+    """The reference's dose_kernels module built from its sources into
+    oracle/_ref, or None."""
     paths = glob.glob(os.path.join(ROOT, "oracle", "_ref", "dose_kernels*.so"))
     if not paths:
-        print(json.dumps({"impl": "reference", "unavailable":
-                          "oracle/_ref/dose_kernels was not built (needs the reference sources)"}))
-        return
+        return None
     import importlib.machinery
     import importlib.util
     loader = importlib.machinery.ExtensionFileLoader("dose_kernels", paths[0])
     spec = importlib.util.spec_from_file_location("dose_kernels", paths[0], loader=loader)
     ref = importlib.util.module_from_spec(spec)
     loader.exec_module(ref)
+    return ref
 
-    case = phantoms.config_gradient(seed=args.seed)
+
+def run_reference(args, world, rank, local):
+    """The reference's CUDA module on this GPU, driven as its
+    computeIMPTPlan drives it (plan_impt.py:170-206): host numpy HU -> RLSP,
+    then per beam proton_raytrace_cuda and proton_spot_cuda (each with its
+    own device allocation and host copies), the beam doses summed on the
+    host and scaled by n_fractions.  Nothing of this package's device code
+    is loaded in this process."""
+    if rank != 0:
+        return
+    if args.workload != "plan":
+        _unavailable(f"the reference has no {args.workload} mode (one beam of one plan per call)")
+        return
+    if args.mode != "forward":
+        _unavailable("the reference has no gradient: only its forward dose can be timed")
+        return
+    ref = load_reference_module()
+    if ref is None:
+        _unavailable("oracle/_ref/dose_kernels was not built (needs the reference sources)")
+        return
+    import torch
+
+    from dosecuda_b200.plan import VolumeObject
+    from dosecuda_b200.plan_impt import _hu_curve
+    from oracle import oracle as O
+
+    torch.cuda.set_device(local)
+    case = plan_case(args.seed)
     g, plan = case.grid, case.plan
     curve = _hu_curve(plan.machine_name)
 
@@ -537,47 +679,60 @@ def run_reference(args, world, rank, local):
     wets = []
 
     def step():
-        # computeIMPTPlan's loop (plan_impt.py:170-206) on the reference module
         rlsp = np.array(np.interp(g.HU, *curve), dtype=np.single)
         dose = np.zeros(g.HU.shape, dtype=np.single)
+        beam_doses = []
         wets.clear()
         for beam in plan.beam_list:
-            w = ref.proton_raytrace_cuda(plan.beam_models[0], vol(rlsp), beam, local)
+            model = beam_model(plan, beam)
+            w = ref.proton_raytrace_cuda(model, vol(rlsp), beam, local)
             wets.append(w)
-            dose += ref.proton_spot_cuda(plan.beam_models[0], vol(rlsp), vol(w), beam, local)
+            d = ref.proton_spot_cuda(model, vol(rlsp), vol(w), beam, local)
+            beam_doses.append(d * plan.n_fractions)
+            dose += d
         dose *= plan.n_fractions
         return dose
 
+    dev = torch.device("cuda", local)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
     for _ in range(args.warmup):
         step()
     E = 0
     for b, beam in enumerate(plan.beam_list):
-        _, layers = O.build_layers(beam.spot_list, plan.beam_models[0].divergence_params)
+        _, layers = O.build_layers(beam.spot_list, beam_model(plan, beam).divergence_params)
         E += O.count_pairs(wets[b], layers)
     times = []
     with Clocks(local) as clk:
         for _ in range(args.steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            step()
-            torch.cuda.synchronize()
-            times.append((time.perf_counter() - t0) * 1e3)
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()           # synchronous: returns after the dose copy
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            times.append(a.elapsed_time(b))
     ms = sum(times) / len(times)
     value = E / (ms * 1e-3)
+    h2d, d2h = reference_copy_bytes(case)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "heterogeneous 256x256x160 @2mm, 4 beams, "
-                               f"{sum(len(b.spot_list) for b in plan.beam_list)} spots "
-                               "(plain forward: the reference has no gradient)",
-                   "dense_pairs_E": E},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": plan_config(case, args.mode),
+        "dense_pairs_E": E,
+        "parallelism": "one process (rank 0)",
+        "e2e": {"value": value, "unit": UNIT, "ms_per_step": ms, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "call": "computeIMPTPlan loop over dose_kernels"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": "the whole workload; the reference's path is CUDA: its "
-                                   "dose_kernels module built from its sources for sm_100a, "
-                                   "driven from one host thread through its host-buffer API "
-                                   "(host numpy HU->RLSP, per-beam device allocation and copies)"},
+                         "runs_on": "gpu",
+                         "sample": "the whole workload, every step.  The reference's path is "
+                                   "CUDA: this is its dose_kernels module on this B200, driven "
+                                   "from one host thread through its host-buffer API (host numpy "
+                                   "HU->RLSP, per-beam device allocation and copies); its JAX "
+                                   "CPU path cannot run here (no jax)"},
         "clocks": clk.summary(),
     }), flush=True)
 
@@ -588,10 +743,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    ap.add_argument("--mode", choices=["forward", "grad"], default="forward")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--wet-mode", choices=["texture", "exact"], default="texture")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["gradient", "batch", "optimize"], default="gradient")
+    ap.add_argument("--workload", choices=["plan", "batch", "optimize"], default="plan")
     ap.add_argument("--opt-iters", type=int, default=50)
     ap.add_argument("--batch-plans", type=int, default=32)
     args = ap.parse_args()

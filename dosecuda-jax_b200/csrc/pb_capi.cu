@@ -101,6 +101,21 @@ static PbStatus check_beams(const PbGrid *g, const PbBeam *beams, int n_beams,
     return PB_OK;
 }
 
+PbStatus check_wet_args(const float *rlsp_dev, uint64_t tex, const PbGrid *grid,
+                        const PbBeamGeom *beams, int n_beams, const float *wet_dev)
+{
+    PbStatus s = check_grid(grid);
+    if (s != PB_OK) return s;
+    if ((!rlsp_dev && !texture_samples(tex)) || !beams || !wet_dev)
+        return set_error(PB_ERR_INVALID, "NULL argument");
+    if (tex && !texture_matches(tex, *grid))
+        return set_error(PB_ERR_INVALID, "texture extent differs from the grid");
+    if (n_beams <= 0 || n_beams > PB_MAX_BEAMS)
+        return set_error(PB_ERR_INVALID, "n_beams must be in [1, %d] (got %d)", PB_MAX_BEAMS,
+                         n_beams);
+    return PB_OK;
+}
+
 }  // namespace pb
 
 using namespace pb;
@@ -256,15 +271,9 @@ PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
                 const PbBeamGeom *beams, int n_beams, float *raw_work_dev, float *wet_dev,
                 int *status_dev, void *stream)
 {
-    PbStatus s = check_grid(grid);
+    PbStatus s = check_wet_args(rlsp_dev, tex, grid, beams, n_beams, wet_dev);
     if (s != PB_OK) return s;
-    if ((!rlsp_dev && !texture_samples(tex)) || !beams || !raw_work_dev || !wet_dev)
-        return set_error(PB_ERR_INVALID, "NULL argument");
-    if (tex && !texture_matches(tex, *grid))
-        return set_error(PB_ERR_INVALID, "texture extent differs from the grid");
-    if (n_beams <= 0 || n_beams > PB_MAX_BEAMS)
-        return set_error(PB_ERR_INVALID, "n_beams must be in [1, %d] (got %d)", PB_MAX_BEAMS,
-                         n_beams);
+    if (!raw_work_dev) return set_error(PB_ERR_INVALID, "NULL argument");
     return launch_wet(rlsp_dev, texture_object(tex), texture_cells(tex), *grid, beams, n_beams,
                       raw_work_dev, wet_dev, status_dev, static_cast<cudaStream_t>(stream));
 }

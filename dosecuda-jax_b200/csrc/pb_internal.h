@@ -25,6 +25,11 @@ int ray_step_cap(const PbGrid &g);
 PbStatus launch_rlsp(const float *hu, int64_t n, const double *xh,
                      const double *yh, int m, float *out, cudaStream_t st);
 
+// The argument checks of the WET entry points (pb_wet, pb_wet_noalloc):
+// grid, input (RLSP pointer or texture), beams and output.
+PbStatus check_wet_args(const float *rlsp_dev, uint64_t tex, const PbGrid *grid,
+                        const PbBeamGeom *beams, int n_beams, const float *wet_dev);
+
 PbStatus launch_wet(const float *rlsp, cudaTextureObject_t tex, const float2 *rec,
                     const PbGrid &g, const PbBeamGeom *beams, int n_beams, float *raw,
                     float *wet, int *status, cudaStream_t st);

@@ -19,10 +19,14 @@
 // reads (the ray trace writes the raw WET of every voxel of every beam
 // before the smoothing reads any), so nothing needs clearing between calls.
 //
-// Host code cannot use the array's name as a device address: on the first
-// call on a device the entry point asks the runtime for the array's address
-// on that device (cudaGetSymbolAddress, with that device current) and keeps
-// it; make that first call before any stream capture.
+// Host code cannot use the array's name as a device address.  The entry
+// point asks the runtime for the array's address in the current context
+// (cudaGetSymbolAddress, with the device current) on its first call in that
+// context, and keeps it for that context: one set-up per device, repeated
+// only if the device's context is re-created (after cudaDeviceReset, say).
+// Make that first call before any stream capture.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "pb_internal.h"
@@ -33,10 +37,28 @@ static __device__ __align__(256) float g_noalloc_raw_wet[PB_NOALLOC_MAX_WET_FLOA
 
 constexpr int kNoallocDevices = 64;
 static std::mutex g_noalloc_mu;
+static CUcontext g_noalloc_ctx[kNoallocDevices];
 static float *g_noalloc_addr[kNoallocDevices];
 
-// Device address of the work array on the current device (set up once per
-// device).
+using CtxGetCurrent = CUresult (*)(CUcontext *);
+
+// The driver's cuCtxGetCurrent, found through the runtime (the library does
+// not link libcuda itself).
+static CtxGetCurrent ctx_get_current()
+{
+    static CtxGetCurrent fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault,
+                                             &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetCurrent>(p);
+    }();
+    return fn;
+}
+
+// Device address of the work array in the current device's context.
 static PbStatus noalloc_scratch(float **out)
 {
     int dev = -1;
@@ -45,13 +67,21 @@ static PbStatus noalloc_scratch(float **out)
     if (dev < 0 || dev >= kNoallocDevices)
         return set_error(PB_ERR_UNSUPPORTED, "device ordinal %d is beyond %d", dev,
                          kNoallocDevices);
+    // cudaFree(0) makes the device's primary context current (no allocation)
+    s = check_cuda(cudaFree(nullptr), "cudaFree(0) (context set-up)");
+    if (s != PB_OK) return s;
+    CtxGetCurrent get = ctx_get_current();
+    CUcontext ctx = nullptr;
+    if (!get || get(&ctx) != CUDA_SUCCESS || !ctx)
+        return set_error(PB_ERR_CUDA, "pb_wet_noalloc: no current CUDA context");
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev] || g_noalloc_ctx[dev] != ctx) {
         void *p = nullptr;
         s = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_raw_wet),
                        "cudaGetSymbolAddress(work array)");
         if (s != PB_OK) return s;
         g_noalloc_addr[dev] = static_cast<float *>(p);
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = g_noalloc_addr[dev];
     return PB_OK;
@@ -65,24 +95,17 @@ extern "C" PbStatus pb_wet_noalloc(const float *rlsp_dev, PbTexture tex, const P
                                    const PbBeamGeom *beams, int n_beams, float *wet_dev,
                                    int *status_dev, void *stream)
 {
-    if (!grid) return set_error(PB_ERR_INVALID, "grid is NULL");
-    if ((!rlsp_dev && !texture_samples(tex)) || !beams || !wet_dev)
-        return set_error(PB_ERR_INVALID, "NULL argument");
-    if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0 || !(grid->spacing > 0.0f))
-        return set_error(PB_ERR_INVALID, "grid dimensions and spacing must be positive");
-    if (n_beams <= 0 || n_beams > PB_MAX_BEAMS)
-        return set_error(PB_ERR_INVALID, "n_beams must be in [1, %d] (got %d)", PB_MAX_BEAMS,
-                         n_beams);
+    // the same inputs as pb_wet accepts, less its work buffer
+    PbStatus s = check_wet_args(rlsp_dev, tex, grid, beams, n_beams, wet_dev);
+    if (s != PB_OK) return s;
     const double need = (double)n_beams * grid->nx * grid->ny * grid->nz;
     if (need > (double)PB_NOALLOC_MAX_WET_FLOATS)
         return set_error(PB_ERR_INVALID,
                          "pb_wet_noalloc: n_beams x voxels = %.0f exceeds its fixed work "
                          "space of %u floats; use pb_wet with a caller-provided buffer",
                          need, (unsigned)PB_NOALLOC_MAX_WET_FLOATS);
-    if (tex && !texture_matches(tex, *grid))
-        return set_error(PB_ERR_INVALID, "texture extent differs from the grid");
     float *raw = nullptr;
-    PbStatus s = noalloc_scratch(&raw);
+    s = noalloc_scratch(&raw);
     if (s != PB_OK) return s;
     return launch_wet(rlsp_dev, texture_object(tex), texture_cells(tex), *grid, beams, n_beams,
                       raw, wet_dev, status_dev, static_cast<cudaStream_t>(stream));

@@ -19,10 +19,19 @@ import numpy as np
 import pandas as pd
 import torch
 
-from . import _lib, engine, nrrd
+from . import nrrd
 from .plan import Beam, DoseGrid, Plan, Prescription, VolumeObject  # noqa: F401
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
+
+
+def _engine():
+    """The device engine.  Imported on first use, so that the plan classes,
+    beam models and lookup tables can be built without loading
+    libpb_b200.so; every dose computation goes through here and raises
+    ImportError when the library is missing (there is no CPU path)."""
+    from . import engine
+    return engine
 
 
 def resource_filename(rel_path: str) -> str:
@@ -129,7 +138,7 @@ class IMPTDoseGrid(DoseGrid):
         self._device_rlsp = None
 
     def _device(self, gpu_id):
-        return engine.require_cuda(torch.device("cuda", int(gpu_id)))
+        return _engine().require_cuda(torch.device("cuda", int(gpu_id)))
 
     def _check_isotropic(self):
         if self.spacing[0] != self.spacing[1] or self.spacing[0] != self.spacing[2]:
@@ -139,7 +148,7 @@ class IMPTDoseGrid(DoseGrid):
     def _rlsp_device(self, machine_name, device):
         hu = torch.from_numpy(np.ascontiguousarray(self.HU, dtype=np.single)).to(device)
         xh, yh = _hu_curve(machine_name)
-        rlsp = engine.rlsp_from_hu(hu, xh, yh)
+        rlsp = _engine().rlsp_from_hu(hu, xh, yh)
         self._device_rlsp = rlsp
         return rlsp
 
@@ -153,7 +162,7 @@ class IMPTDoseGrid(DoseGrid):
         specs = []
         for beam in beams:
             model = _beam_model(plan, beam)
-            specs.append(engine.BeamSpec(beam.gantry_angle, beam.couch_angle,
+            specs.append(_engine().BeamSpec(beam.gantry_angle, beam.couch_angle,
                                          np.asarray(beam.iso, dtype=np.single),
                                          _spot_array(beam), model))
         return specs
@@ -167,7 +176,7 @@ class IMPTDoseGrid(DoseGrid):
         device = self._device(gpu_id)
         rlsp = self._rlsp_device(plan.machine_name, device)
         beams = plan.beam_list if beams is None else beams
-        dp = engine.DevicePlan(np.shape(self.HU), float(self.spacing[0]),
+        dp = _engine().DevicePlan(np.shape(self.HU), float(self.spacing[0]),
                                np.asarray(self.origin, dtype=np.single),
                                self._specs(plan, beams), device)
         dp.compute_wet(rlsp.reshape(-1), wet_mode=wet_mode)
@@ -177,7 +186,7 @@ class IMPTDoseGrid(DoseGrid):
         """The plan's beams in groups the device kernels take at once (the
         reference loops over any number of beams)."""
         beams = list(plan.beam_list)
-        n = _lib.PB_MAX_BEAMS
+        n = _engine()._lib.PB_MAX_BEAMS
         return [beams[i:i + n] for i in range(0, len(beams), n)]
 
     def computeIMPTPlan(self, plan, gpu_id=0, wet_mode="texture"):
@@ -224,7 +233,7 @@ class IMPTDoseGrid(DoseGrid):
         self._check_isotropic()
         device = self._device(gpu_id)
         wet = np.asarray(wet_object.voxel_data, dtype=np.single)
-        dp = engine.DevicePlan(wet.shape, float(self.spacing[0]),
+        dp = _engine().DevicePlan(wet.shape, float(self.spacing[0]),
                                np.asarray(self.origin, dtype=np.single),
                                self._specs(plan, [beam]), device)
         dp.set_wet(torch.from_numpy(np.ascontiguousarray(wet)).to(device))
@@ -262,7 +271,7 @@ class IMPTDoseGrid(DoseGrid):
         for dp in dps[1:]:
             dose = dose + dp.forward(scale=scale)
         resid = torch.empty_like(dose)
-        obj = engine.objective(dose, presc, w, resid)
+        obj = _engine().objective(dose, presc, w, resid)
         grads = [dp.to_plan(dp.adjoint(resid, scale=scale)).cpu().numpy() for dp in dps]
         return float(obj.item()), np.concatenate(grads)
 

@@ -252,7 +252,8 @@ def test_dose_kernels_dropin_matches_reference(pkg, small, curve, reference_modu
         w_ref = reference_module.proton_raytrace_cuda(model, _vol(rlsp, g), beam, 0)
         w_mine = mine.proton_raytrace_cuda(model, _vol(rlsp, g), beam, 0)
         assert w_mine.dtype == np.float32 and w_mine.shape == w_ref.shape
-        assert np.quantile(np.abs(w_mine - w_ref), 0.999) <= 1e-4
+        # every voxel, as the other texture-mode tests (ties included)
+        assert np.abs(w_mine - w_ref).max() <= 1e-4
         d_ref = reference_module.proton_spot_cuda(model, _vol(rlsp, g), _vol(w_ref, g), beam, 0)
         d_mine = mine.proton_spot_cuda(model, _vol(rlsp, g), _vol(w_ref, g), beam, 0)
         assert max_rel(d_mine, d_ref) <= 2e-4
