@@ -4,15 +4,43 @@ Same classes, attribute names and defaults as the reference so that code
 written against ``DoseCUDA.plan`` runs unchanged:
   VolumeObject (plan.py:6-11), Prescription (:14-19), DoseGrid (:22-232),
   Beam (:235-243), Plan (:246-268).
-NRRD volume I/O is served by the package's own reader/writer; DICOM CT/dose
-I/O and SimpleITK resampling need pydicom/SimpleITK and raise
-NotImplementedError with that reason.
+NRRD and NIfTI volume I/O is served by the package's own readers/writers.
+The RT Dose writer (writeDoseDCM) edits a reference RT Dose dataset: one
+read through pydicom from a path, or any dataset object already read (the
+same attributes and save_as).  DICOM CT reading and SimpleITK resampling
+need pydicom/SimpleITK and raise NotImplementedError with that reason.
 """
 from __future__ import annotations
 
+import copy
+import uuid
+
 import numpy as np
 
-from . import nrrd
+from . import nifti, nrrd
+
+
+def generate_uid() -> str:
+    """A new DICOM UID: pydicom's generator when pydicom is installed, else
+    the UUID-derived form 2.25.<128-bit integer> of DICOM PS3.5 B.2."""
+    try:
+        from pydicom.uid import generate_uid as gen
+        return str(gen())
+    except ImportError:
+        return "2.25.%d" % uuid.uuid4().int
+
+
+def _dataset(ref):
+    """A dataset to edit: read from a path with pydicom (force=True, as the
+    reference does), or a deep copy of a dataset object already read."""
+    if isinstance(ref, (str, bytes)) or hasattr(ref, "__fspath__"):
+        try:
+            import pydicom
+        except ImportError as e:
+            raise ImportError("reading a DICOM file needs pydicom; pass a dataset already "
+                              "read instead") from e
+        return pydicom.dcmread(ref, force=True)
+    return copy.deepcopy(ref)
 
 
 class VolumeObject:
@@ -83,7 +111,31 @@ class DoseGrid:
     # -- output -------------------------------------------------------------
     def writeDoseDCM(self, dose_path, ref_dose_path, dose_type="EFFECTIVE",
                      individual_beams=False):
-        raise NotImplementedError("writeDoseDCM writes DICOM through pydicom")
+        """The plan dose (or each beam's) as RT Dose files built on a
+        reference RT Dose (plan.py:133-171): its SeriesDescription + "_DoseCUDA",
+        DoseSummationType PLAN (BEAM per beam), DoseType, a new referenced
+        plan UID, pixel data dose * 500 * RBE as uint16 with DoseGridScaling
+        0.002.  ref_dose_path is a file (read with pydicom) or a dataset
+        already read, copied for every output file.  The pixel data is
+        stored as the array's little-endian bytes."""
+        if not dose_path.endswith(".dcm"):
+            raise Exception("Dose path must have .dcm extension")
+        rbe = _rbe(dose_type)
+        if individual_beams:
+            outs = [(dose_path.replace(".dcm", "_beam%02i.dcm" % (i + 1)), d, "BEAM")
+                    for i, d in enumerate(self.beam_doses)]
+        else:
+            outs = [(dose_path, self.dose, "PLAN")]
+        for path, dose, summation in outs:
+            ref_dose = _dataset(ref_dose_path)
+            ref_dose.SeriesDescription = ref_dose.SeriesDescription + "_DoseCUDA"
+            ref_dose.DoseSummationType = summation
+            ref_dose.DoseType = dose_type
+            ref_dose.ReferencedRTPlanSequence[0].ReferencedSOPInstanceUID = generate_uid()
+            dose_dcm = np.array(np.asarray(dose) * 500.0 * rbe, dtype=np.uint16)
+            ref_dose.PixelData = dose_dcm.astype("<u2").tobytes()
+            ref_dose.DoseGridScaling = 0.002
+            ref_dose.save_as(path)
 
     def writeDoseNRRD(self, dose_path, individual_beams=False, dose_type="EFFECTIVE"):
         """Write the plan dose (or each beam's) times RBE (plan.py:173-199)."""
@@ -105,7 +157,10 @@ class DoseGrid:
         nrrd.write(ct_path, np.asarray(self.HU), self.origin, self.spacing)
 
     def writeCTNIFTI(self, ct_path):
-        raise NotImplementedError("writeCTNIFTI writes NIfTI through SimpleITK")
+        """The CT (HU) as gzip-compressed NIfTI-1 (plan.py:214-224)."""
+        if not ct_path.endswith(".nii.gz"):
+            raise Exception("CT path must have .nii.gz extension")
+        nifti.write(ct_path, np.asarray(self.HU), self.origin, self.spacing)
 
     # -- phantoms -----------------------------------------------------------
     def createCubePhantom(self, size=[138, 138, 138], spacing=3.0):

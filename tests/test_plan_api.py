@@ -249,3 +249,104 @@ def test_read_plan_dicom_file_needs_pydicom(plan, tmp_path):
         pytest.skip("pydicom is installed")
     with pytest.raises(ImportError, match="pydicom"):
         plan.readPlanDicom(str(tmp_path / "plan.dcm"))
+
+
+class _FakeItem:
+    pass
+
+
+class _FakeRTDose:
+    """Stands in for a pydicom RT Dose dataset: the attributes writeDoseDCM
+    edits, and save_as recording what would be written."""
+
+    saved = []
+
+    def __init__(self):
+        self.SeriesDescription = "TPS dose"
+        self.DoseSummationType = "PLAN"
+        self.DoseType = "PHYSICAL"
+        self.DoseGridScaling = 1.0
+        self.PixelData = b""
+        item = _FakeItem()
+        item.ReferencedSOPInstanceUID = "1.2.3"
+        self.ReferencedRTPlanSequence = [item]
+
+    def save_as(self, path):
+        _FakeRTDose.saved.append((path, dict(self.__dict__)))
+
+
+def test_write_dose_dcm_edits_a_reference_dataset(tmp_path):
+    """writeDoseDCM (plan.py:133-171) on a dataset object: the plan dose and
+    per-beam doses as uint16 of dose * 500 * RBE with DoseGridScaling 0.002,
+    a new referenced plan UID per file, the reference dataset untouched."""
+    from dosecuda_b200.plan import DoseGrid
+    g = DoseGrid()
+    rng = np.random.default_rng(0)
+    g.dose = rng.uniform(0.0, 60.0, (3, 4, 5)).astype(np.float32)
+    g.beam_doses = [g.dose * 0.25, g.dose * 0.75]
+    ref = _FakeRTDose()
+    _FakeRTDose.saved.clear()
+    with pytest.raises(Exception, match="dcm extension"):
+        g.writeDoseDCM(str(tmp_path / "d.nrrd"), ref)
+    with pytest.raises(Exception, match="Unknown dose type"):
+        g.writeDoseDCM(str(tmp_path / "d.dcm"), ref, dose_type="RBE")
+    g.writeDoseDCM(str(tmp_path / "d.dcm"), ref)
+    g.writeDoseDCM(str(tmp_path / "d.dcm"), ref, dose_type="PHYSICAL", individual_beams=True)
+    paths = [p for p, _ in _FakeRTDose.saved]
+    assert paths == [str(tmp_path / n) for n in ("d.dcm", "d_beam01.dcm", "d_beam02.dcm")]
+    plan_ds, b1, b2 = (d for _, d in _FakeRTDose.saved)
+    assert plan_ds["SeriesDescription"] == "TPS dose_DoseCUDA"
+    assert plan_ds["DoseSummationType"] == "PLAN" and plan_ds["DoseType"] == "EFFECTIVE"
+    assert b1["DoseSummationType"] == "BEAM" and b1["DoseType"] == "PHYSICAL"
+    assert plan_ds["DoseGridScaling"] == 0.002
+    px = np.frombuffer(plan_ds["PixelData"], "<u2").reshape(g.dose.shape)
+    assert np.array_equal(px, np.array(g.dose * 500.0 * 1.1, dtype=np.uint16))
+    px2 = np.frombuffer(b2["PixelData"], "<u2").reshape(g.dose.shape)
+    assert np.array_equal(px2, np.array(g.beam_doses[1] * 500.0 * 1.0, dtype=np.uint16))
+    uids = {d["ReferencedRTPlanSequence"][0].ReferencedSOPInstanceUID for d in (plan_ds, b1, b2)}
+    import re
+    # valid DICOM UIDs: dotted numbers, at most 64 characters
+    assert len(uids) == 3 and all(re.fullmatch(r"[0-9]+(\.[0-9]+)+", u) and len(u) <= 64
+                                  for u in uids)
+    # the reference dataset itself is not modified
+    assert ref.SeriesDescription == "TPS dose" and ref.PixelData == b""
+    assert ref.ReferencedRTPlanSequence[0].ReferencedSOPInstanceUID == "1.2.3"
+
+
+def test_write_dose_dcm_from_a_file_needs_pydicom(tmp_path):
+    from dosecuda_b200.plan import DoseGrid
+    try:
+        import pydicom  # noqa: F401
+        pytest.skip("pydicom is installed")
+    except ImportError:
+        pass
+    g = DoseGrid()
+    g.dose = np.zeros((2, 2, 2), np.float32)
+    with pytest.raises(ImportError, match="pydicom"):
+        g.writeDoseDCM(str(tmp_path / "d.dcm"), str(tmp_path / "ref.dcm"))
+
+
+def test_write_ct_nifti_roundtrip(tmp_path):
+    """writeCTNIFTI (plan.py:214-224): NIfTI-1, gzip, LPS stored as RAS as an
+    ITK writer stores it; read back equal."""
+    import gzip
+    import struct
+
+    from dosecuda_b200 import nifti
+    from dosecuda_b200.plan import DoseGrid
+    g = DoseGrid()
+    g.HU = np.random.default_rng(1).uniform(-1000, 2000, (4, 5, 6)).astype(np.float32)
+    g.origin = np.array([-10.0, 20.0, -30.5])
+    g.spacing = np.array([1.5, 1.5, 2.0])
+    with pytest.raises(Exception, match="nii.gz"):
+        g.writeCTNIFTI(str(tmp_path / "ct.nii"))
+    path = str(tmp_path / "ct.nii.gz")
+    g.writeCTNIFTI(path)
+    vol, origin, spacing = nifti.read(path)
+    assert np.array_equal(vol, g.HU)
+    assert np.allclose(origin, g.origin) and np.allclose(spacing, g.spacing)
+    raw = gzip.decompress(open(path, "rb").read())
+    assert struct.unpack_from("<8h", raw, 40)[:4] == (3, 6, 5, 4)
+    assert struct.unpack_from("<hh", raw, 70) == (16, 32)
+    assert struct.unpack_from("<4f", raw, 280) == (-1.5, 0.0, 0.0, 10.0)
+    assert struct.unpack_from("<3f", raw, 256) == (0.0, 0.0, 1.0)
