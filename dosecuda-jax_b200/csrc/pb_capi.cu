@@ -321,6 +321,21 @@ PbStatus pb_dose_adjoint(const PbGrid *grid, const PbBeam *beams, int n_beams,
                           dobj_dose_dev, scale, grad_dev, static_cast<cudaStream_t>(stream));
 }
 
+PbStatus pb_dose_adjoint_variant(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                 const float *wet_dev, const PbLayer *layers_dev,
+                                 const float *spot_geo_dev, const float *dobj_dose_dev,
+                                 float scale, float *grad_dev, int variant, void *stream)
+{
+    if (variant < 0 || variant >= dose_variant_count())
+        return set_error(PB_ERR_INVALID, "variant must be in [0, %d)", dose_variant_count());
+    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev);
+    if (s != PB_OK) return s;
+    if (!dobj_dose_dev || !grad_dev) return set_error(PB_ERR_INVALID, "NULL argument");
+    return launch_adjoint(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev,
+                          dobj_dose_dev, scale, grad_dev, static_cast<cudaStream_t>(stream),
+                          variant);
+}
+
 size_t pb_objective_work_size(void) { return objective_work_size(); }
 
 PbStatus pb_objective(const float *dose_dev, const float *presc_dev, const float *weight_dev,
@@ -626,6 +641,8 @@ static size_t batch_dose_offset(int n_plans)
 extern "C" {
 
 int pb_dose_variant_count(void) { return dose_variant_count(); }
+
+int pb_dose_variant_default(void) { return dose_variant_default(); }
 
 const char *pb_dose_variant_name(int variant) { return dose_variant_name(variant); }
 

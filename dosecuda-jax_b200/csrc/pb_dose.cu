@@ -93,7 +93,15 @@ struct LayerK {
     float r3sq, c_lin;       // (R80 + 3)^2, 1.61e-9 (R80 + 3)^2
 };
 
-__device__ __forceinline__ LayerK layer_consts(float r80, const float *cabc, const float *s_dep,
+// A LUT row: a plain pointer (shared memory) or RowG, a row in global
+// memory read through the read-only data cache.
+struct RowG {
+    const float *p;
+    __device__ __forceinline__ float operator[](int i) const { return __ldg(p + i); }
+};
+
+template <class Row>
+__device__ __forceinline__ LayerK layer_consts(float r80, const float *cabc, const Row &s_dep,
                                                int lut_len)
 {
     LayerK K;
@@ -128,9 +136,10 @@ __device__ __forceinline__ LayerK layer_consts(float r80, const float *cabc, con
 // Every operation is an explicitly rounded intrinsic, so that no
 // instantiation of the tile code contracts them differently: all kernel
 // shapes give the same bits.
+template <class Row>
 __device__ __forceinline__ void layer_params(float wet_mm, float dist, const LayerK &K,
-                                             const float *s_dep, const float *s_sig,
-                                             const float *s_idd, int lut_len, float &pf,
+                                             const Row &s_dep, const Row &s_sig,
+                                             const Row &s_idd, int lut_len, float &pf,
                                              float &hf, float &ps2, float &hs2)
 {
     const float gs = ceilf(__fmul_rn(__fsub_rn(wet_mm, K.d0), K.inv_step));
@@ -943,6 +952,477 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
     }
 }
 
+// ------------------------------------------------------------ line tiles
+//
+// The forward, its operation count and the spot-weight adjoint also exist
+// on tiles of 8 x TY x TZ voxels, one block of TY*TZ threads per tile, each
+// thread owning one line of kLine = 8 voxels along x.  Along a line the
+// voxels' head-frame coordinates, and the divergence factors, are affine in
+// the voxel's offset q' = q - 3.5 from the line's centre, so the three
+// components of t x ray (axis_r2) are affine in q' and the scaled squared
+// axis distance of a spot is a quadratic
+//     it2 |t x ray|^2 = S0 + B1 q' + C2 q'^2 .
+// Per spot the block's compaction stores the spot's line-independent part
+// (C2 and 2 it2 times the per-voxel step of each component, from the
+// beam's constant step along x); each thread then forms S0 and B1 for its
+// own line from the components at the line's centre (11 operations) and
+// evaluates every voxel with two fused multiply-adds.  The per-voxel work
+// is the exponent (one multiply), the SFU's ex2 and the accumulation, so
+// the spot loops are bound by the SFU's exp2 rate rather than shared with
+// the FMA pipe.  The LUT rows are read through the read-only data cache
+// (no staging barrier).  Decisions (layer selection, the per-layer range
+// cut, the spot cull) are those of the 8^3 tiles above.
+//
+// Shapes (template TY, TZ, KCULL): tiles of 8x8x8 (64 threads), 8x8x4 and
+// 8x4x8 (32 threads), 8x16x8 and 8x8x16 (128 threads); KCULL spots culled
+// per thread per compaction round.  Shapes that differ in tile or round size
+// cull differently, or add a layer's spots in another order, and agree to
+// rounding.
+
+constexpr int kLine = 8;
+
+// Line-tile record of one surviving spot: (-x, -y, x/VSADX, -y/VSADY),
+// (-x y (1/VSADX - 1/VSADY), it2, C2, weight or index), and 2 it2 times the
+// step of each component of t x ray per voxel along x (the last float unused).
+struct LineSpot {
+    float4 a, b, c;
+};
+
+template <int NT, int KCULL>
+struct LineShared {
+    static constexpr int kWarps = NT / 32;
+    LineSpot spot[NT * KCULL + 8];
+    float gsum[NT * KCULL + 8];      // adjoint: per-slot gradient partials
+    float w[kLine][NT];              // the beam's 10*WET per voxel (INF: not valid)
+    float d[kLine][NT];              // distance to the source per voxel
+    float red[kWarps][kRedSlots];
+    int wcount[KCULL][kWarps];
+    int wcount_h[KCULL][kWarps];
+    int lcount[kWarps];
+    int lsel[NT];
+};
+
+// Offset q - 3.5 of a line's voxel from the line's centre (exact in FP32).
+__device__ __forceinline__ constexpr float line_off(int q) { return (float)q - 3.5f; }
+
+// Per-thread part of a spot's quadratic on this thread's line: S0 and B1
+// from the spot's axis components at the line's centre.
+__device__ __forceinline__ void line_spot(const LineSpot &r, float Xc, float Yc, float gxc,
+                                          float gyc, float &S0, float &B1)
+{
+    const float ax = __fmaf_rn(r.a.x, gxc, Xc);
+    const float ay = __fmaf_rn(r.a.y, gyc, Yc);
+    const float az = __fmaf_rn(r.a.z, Yc, __fmaf_rn(r.a.w, Xc, r.b.x));
+    S0 = __fmul_rn(r.b.y, __fmaf_rn(ax, ax, __fmaf_rn(ay, ay, __fmul_rn(az, az))));
+    B1 = __fmaf_rn(ax, r.c.x, __fmaf_rn(ay, r.c.y, __fmul_rn(az, r.c.z)));
+}
+
+template <int TY, int TZ, int KCULL, bool BEAM_OUT, int MODE = kModeDose>
+__device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int tz,
+                                          const float *__restrict__ wet,
+                                          const PbLayer *__restrict__ layers,
+                                          const float4 *__restrict__ geo,
+                                          const float *__restrict__ mu,
+                                          float *__restrict__ dose,
+                                          float *__restrict__ beam_dose,
+                                          LineShared<TY * TZ, KCULL> &sh,
+                                          unsigned long long *count = nullptr,
+                                          const float *__restrict__ wfield = nullptr,
+                                          float *__restrict__ grad = nullptr)
+{
+    constexpr int NT = TY * TZ;
+    constexpr int kWarps = NT / 32;
+    constexpr bool COUNT = MODE == kModeCount;
+    constexpr bool ADJ = MODE == kModeAdjoint;
+    static_assert(NT % 32 == 0, "whole warps");
+    static_assert(MODE == kModeDose || MODE == kModeCount || MODE == kModeAdjoint,
+                  "line tiles: dose, count or weight adjoint");
+    constexpr int kCap = NT * KCULL;
+    const int t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5;
+
+    // this thread's line: voxels (i0 + q, j, k), q < nvalid
+    const int i0 = tx * kLine, j = ty * TY + t % TY, k = tz * TZ + t / TY;
+    const int nvalid = (j < A.g.ny && k < A.g.nz) ? min(kLine, A.g.nx - i0) : 0;
+    const int64_t vbase = i0 + (int64_t)A.g.nx * (j + (int64_t)A.g.ny * k);
+    const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
+    unsigned long long n_ex2 = 0, n_eval = 0;
+
+    float tot_s[kLine], tot_c[kLine];
+#pragma unroll
+    for (int q = 0; q < kLine; ++q) tot_s[q] = tot_c[q] = 0.0f;
+    float wv[kLine];   // adjoint: scale * dObj/dD per voxel
+    if constexpr (ADJ) {
+        bool anyw = false;
+#pragma unroll
+        for (int q = 0; q < kLine; ++q) {
+            wv[q] = q < nvalid ? __ldg(wfield + vbase + q) * A.scale : 0.0f;
+            anyw |= (wv[q] != 0.0f);
+        }
+        if (!__syncthreads_or(anyw)) return;
+        for (int c = t; c < kCap + 8; c += NT) sh.gsum[c] = 0.0f;
+    }
+
+    for (int b = 0; b < A.n_beams; ++b) {
+        const PbBeam &B = A.beams[b];
+        // line geometry: head-frame centre and step per voxel along x
+        float dX, dY, dZ;
+        image_to_head(B.geom, A.g.spacing, 0.0f, 0.0f, dX, dY, dZ);
+        const float dgx = -__fdiv_rn(dZ, B.geom.vsadx), dgy = -__fdiv_rn(dZ, B.geom.vsady);
+        float Xc, Yc, Zc;
+        {
+            float px, py, pz, X0, Y0, Z0;
+            vox_mm(B.geom, A.g.spacing, i0, j, k, px, py, pz);
+            image_to_head(B.geom, px, py, pz, X0, Y0, Z0);
+            Xc = __fmaf_rn(3.5f, dX, X0);
+            Yc = __fmaf_rn(3.5f, dY, Y0);
+            Zc = __fmaf_rn(3.5f, dZ, Z0);
+        }
+        const float gxc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsadx));
+        const float gyc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsady));
+        TileBounds tb;
+        {
+            // the beam's depth and source distance per voxel into shared
+            // memory; the tile's box over its valid voxels
+            float v[11] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
+                           INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY};
+#pragma unroll
+            for (int q = 0; q < kLine; ++q) {
+                const float o = line_off(q);
+                float w = INFINITY, dd = 0.0f;
+                if (q < nvalid) {
+                    const float X = __fmaf_rn(o, dX, Xc), Y = __fmaf_rn(o, dY, Yc);
+                    const float Z = __fmaf_rn(o, dZ, Zc);
+                    w = __fmul_rn(__ldg(wet + b * V + vbase + q), 10.0f);
+                    dd = source_distance(B, X, Y, Z);
+                    const float GX = __fmaf_rn(o, dgx, gxc), GY = __fmaf_rn(o, dgy, gyc);
+                    v[0] = fminf(v[0], X);  v[1] = fmaxf(v[1], X);
+                    v[2] = fminf(v[2], Y);  v[3] = fmaxf(v[3], Y);
+                    v[4] = fminf(v[4], GX); v[5] = fmaxf(v[5], GX);
+                    v[6] = fminf(v[6], GY); v[7] = fmaxf(v[7], GY);
+                    v[8] = fminf(v[8], dd); v[9] = fmaxf(v[9], dd);
+                    // the least depth over voxels that can be active; a NaN
+                    // depth is never skipped
+                    if (!ADJ || wv[q] != 0.0f) v[10] = fminf(v[10], w == w ? w : -INFINITY);
+                }
+                sh.w[q][t] = w;
+                sh.d[q][t] = dd;
+            }
+#pragma unroll
+            for (int m = 0; m < 11; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
+            if (lane == 0) {
+#pragma unroll
+                for (int m = 0; m < 11; ++m) sh.red[warp][m] = v[m];
+            }
+            __syncthreads();
+            float r[11];
+#pragma unroll
+            for (int m = 0; m < 11; ++m) r[m] = sh.red[0][m];
+            for (int w = 1; w < kWarps; ++w) {
+#pragma unroll
+                for (int m = 0; m < 11; ++m)
+                    r[m] = (m & 1) ? fmaxf(r[m], sh.red[w][m]) : fminf(r[m], sh.red[w][m]);
+            }
+            tb.x0 = r[0]; tb.x1 = r[1]; tb.y0 = r[2]; tb.y1 = r[3];
+            tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
+            tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10];
+        }
+        float bs_s[kLine], bs_c[kLine];
+#pragma unroll
+        for (int q = 0; q < kLine; ++q) bs_s[q] = bs_c[q] = 0.0f;
+
+        for (int l0 = 0; l0 < B.n_layers; l0 += NT) {
+            __syncthreads();   // the previous chunk's list and the bounds have been read
+            bool keep = false;
+            {
+                const int l = l0 + t;
+                if (l < B.n_layers) {
+                    const PbLayer L = layers[B.layer_start + l];
+                    const float cut = __fmul_rn(1.1f, L.r80);
+                    keep = L.n_spots > 0 && tb.w0 <= cut && !layer_skip(L, tb, B, cut);
+                }
+            }
+            const unsigned lm = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) sh.lcount[warp] = __popc(lm);
+            __syncthreads();
+            int nsel = 0, lpos = 0;
+            for (int w = 0; w < kWarps; ++w) {
+                if (w == warp) lpos = nsel + __popc(lm & ((1u << lane) - 1u));
+                nsel += sh.lcount[w];
+            }
+            if (keep) sh.lsel[lpos] = l0 + t;
+            __syncthreads();
+            for (int li = 0; li < nsel; ++li) {
+                // every kept layer has spots, so each runs at least one
+                // compaction round, whose barriers separate this layer's
+                // block_max2 from the next one's
+                const PbLayer L = layers[B.layer_start + sh.lsel[li]];
+                const float cut = __fmul_rn(1.1f, L.r80);
+                const size_t ro = (size_t)L.energy_id * B.lut_len;
+                const RowG dep{B.depths_dev + ro}, sig{B.sigmas_dev + ro}, idd{B.idds_dev + ro};
+                const LayerK K =
+                    layer_consts(L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, dep,
+                                 B.lut_len);
+                float pf[kLine], hf[kLine], PS[kLine], HS[kLine];
+                bool act[kLine];
+                float hmax = -INFINITY, pmax = -INFINITY;
+                // every voxel's parameters without branching (inactive
+                // voxels take a harmless depth and are masked afterwards)
+#pragma unroll
+                for (int q = 0; q < kLine; ++q) {
+                    const float w = sh.w[q][t];
+                    act[q] = !(w > cut) && q < nvalid;
+                    if constexpr (ADJ) act[q] = act[q] && wv[q] != 0.0f;
+                    float ps2, hs2;
+                    layer_params(act[q] ? w : 0.0f, sh.d[q][t], K, dep, sig, idd, B.lut_len,
+                                 pf[q], hf[q], ps2, hs2);
+                    if (act[q]) {
+                        hmax = fmaxf(hmax, hs2);
+                        pmax = fmaxf(pmax, ps2);
+                    } else {
+                        pf[q] = hf[q] = ps2 = hs2 = 0.0f;
+                    }
+                    PS[q] = ps2;
+                    HS[q] = hs2;
+                }
+                float nhs, nps;
+                block_max2<NT>(hmax, pmax, sh.red, nhs, nps);
+                nhs = -nhs;
+                nps = -nps;
+                // forward: per-voxel sums; adjoint: weighted prefactors
+                float AP[kLine], AH[kLine];
+#pragma unroll
+                for (int q = 0; q < kLine; ++q) {
+                    if constexpr (ADJ) {
+                        AP[q] = __fmul_rn(wv[q], pf[q]);
+                        AH[q] = __fmul_rn(wv[q], hf[q]);
+                    } else {
+                        AP[q] = AH[q] = 0.0f;
+                    }
+                }
+
+                const int s0 = B.spot_start + L.spot_start;
+                for (int base = 0; base < L.n_spots; base += kCap) {
+                    int cls[KCULL];
+                    float4 ga[KCULL], gb[KCULL];
+                    unsigned m2[KCULL], m1[KCULL];
+#pragma unroll
+                    for (int c = 0; c < KCULL; ++c) {
+                        const int si = base + c * NT + t;
+                        cls[c] = 0;
+                        if (si < L.n_spots) {
+                            ga[c] = __ldg(geo + 2 * (int64_t)(s0 + si));
+                            cls[c] = cull_class(cull_r2(ga[c].x, ga[c].y, ga[c].z, tb), nhs, nps);
+                            if (cls[c]) gb[c] = __ldg(geo + 2 * (int64_t)(s0 + si) + 1);
+                        }
+                        m2[c] = __ballot_sync(0xffffffffu, cls[c] == 2);
+                        m1[c] = __ballot_sync(0xffffffffu, cls[c] == 1);
+                        if (lane == 0) {
+                            sh.wcount[c][warp] = __popc(m2[c]);
+                            sh.wcount_h[c][warp] = __popc(m1[c]);
+                        }
+                    }
+                    __syncthreads();
+                    int n2 = 0, n1 = 0;
+                    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+                    for (int c = 0; c < KCULL; ++c) {
+                        int pos2 = 0, pos1 = 0;
+                        for (int w = 0; w < kWarps; ++w) {
+                            if (w == warp) {
+                                pos2 = n2 + __popc(m2[c] & below);
+                                pos1 = n1 + __popc(m1[c] & below);
+                            }
+                            n2 += sh.wcount[c][w];
+                            n1 += sh.wcount_h[c][w];
+                        }
+                        if (cls[c]) {
+                            const int si = s0 + base + c * NT + t;
+                            // the dose keeps the spot's weight, the adjoint its index
+                            const float wgt =
+                                MODE == kModeDose ? __ldg(mu + si) : __int_as_float(si);
+                            const float nx = -ga[c].x, ny = -ga[c].y, txs = ga[c].w;
+                            const float nty = -gb[c].x, it2 = ga[c].z;
+                            // the spot's step of each component per voxel along x
+                            const float sx = __fmaf_rn(nx, dgx, dX);
+                            const float sy = __fmaf_rn(ny, dgy, dY);
+                            const float sz = __fmaf_rn(txs, dY, __fmul_rn(nty, dX));
+                            const float c2 = __fmul_rn(
+                                it2, __fmaf_rn(sx, sx, __fmaf_rn(sy, sy, __fmul_rn(sz, sz))));
+                            const float k2 = __fmul_rn(2.0f, it2);
+                            LineSpot r;
+                            r.a = make_float4(nx, ny, txs, nty);
+                            r.b = make_float4(-gb[c].y, it2, c2, wgt);
+                            r.c = make_float4(__fmul_rn(k2, sx), __fmul_rn(k2, sy),
+                                              __fmul_rn(k2, sz), 0.0f);
+                            sh.spot[cls[c] == 2 ? pos2 : kCap - 1 - pos1] = r;
+                        }
+                    }
+                    __syncthreads();
+                    if constexpr (COUNT) {
+                        n_ex2 += (unsigned long long)(kLine * NT) * (2 * n2 + n1);
+                        n_eval += (unsigned long long)(kLine * NT) * (n2 + n1);
+                    } else if constexpr (ADJ) {
+                        // both terms: slots [0, n2); halo only: [kCap - n1, kCap);
+                        // a group's slots past its class hold other records or
+                        // padding, and their sums are dropped
+                        for (int two = 1; two >= 0; --two) {
+                            const int lo = two ? 0 : kCap - n1, hi = two ? n2 : kCap;
+                            for (int c0 = lo; c0 < hi; c0 += 8) {
+                                float v[8];
+#pragma unroll
+                                for (int u = 0; u < 8; ++u) {
+                                    const LineSpot r = sh.spot[c0 + u];
+                                    float S0, B1;
+                                    line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
+                                    float acc = 0.0f;
+#pragma unroll
+                                    for (int q = 0; q < kLine; ++q) {
+                                        const float o = line_off(q);
+                                        const float S = __fmaf_rn(__fmaf_rn(r.b.z, o, B1), o, S0);
+                                        acc = __fmaf_rn(AH[q], ex2(__fmul_rn(HS[q], S)), acc);
+                                        if (two)
+                                            acc = __fmaf_rn(AP[q], ex2(__fmul_rn(PS[q], S)), acc);
+                                    }
+                                    v[u] = acc;
+                                }
+                                int slot;
+                                const float sum = warp_sum8(v, lane, slot);
+                                if ((lane & 3) == 0 && c0 + slot < hi && sum != 0.0f)
+                                    atomicAdd(&sh.gsum[c0 + slot], sum);
+                            }
+                        }
+                        __syncthreads();
+                        // each surviving spot's tile sum to its gradient
+                        for (int c = t; c < n2 + n1; c += NT) {
+                            const int sl = c < n2 ? c : kCap - n1 + (c - n2);
+                            const float a = sh.gsum[sl];
+                            if (a != 0.0f) atomicAdd(grad + __float_as_int(sh.spot[sl].b.w), a);
+                            sh.gsum[sl] = 0.0f;
+                        }
+                    } else {
+                        // both terms
+#pragma unroll 2
+                        for (int c = 0; c < n2; ++c) {
+                            const LineSpot r = sh.spot[c];
+                            float S0, B1;
+                            line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
+#pragma unroll
+                            for (int q = 0; q < kLine; ++q) {
+                                const float o = line_off(q);
+                                const float S = __fmaf_rn(__fmaf_rn(r.b.z, o, B1), o, S0);
+                                AP[q] = __fmaf_rn(r.b.w, ex2(__fmul_rn(PS[q], S)), AP[q]);
+                                AH[q] = __fmaf_rn(r.b.w, ex2(__fmul_rn(HS[q], S)), AH[q]);
+                            }
+                        }
+                        // halo only
+#pragma unroll 2
+                        for (int c = kCap - n1; c < kCap; ++c) {
+                            const LineSpot r = sh.spot[c];
+                            float S0, B1;
+                            line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
+#pragma unroll
+                            for (int q = 0; q < kLine; ++q) {
+                                const float o = line_off(q);
+                                const float S = __fmaf_rn(__fmaf_rn(r.b.z, o, B1), o, S0);
+                                AH[q] = __fmaf_rn(r.b.w, ex2(__fmul_rn(HS[q], S)), AH[q]);
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+                if constexpr (MODE == kModeDose) {
+#pragma unroll
+                    for (int q = 0; q < kLine; ++q) {
+                        if (act[q]) {
+                            const float ld = fmaf(pf[q], AP[q], hf[q] * AH[q]);
+                            if (BEAM_OUT) neumaier(bs_s[q], bs_c[q], ld);
+                            neumaier(tot_s[q], tot_c[q], ld);
+                        }
+                    }
+                }
+            }
+        }
+        if (BEAM_OUT) {
+#pragma unroll
+            for (int q = 0; q < kLine; ++q)
+                if (q < nvalid) beam_dose[b * V + vbase + q] = (bs_s[q] + bs_c[q]) * A.scale;
+        }
+        __syncthreads();  // sh.w, sh.d and sh.red are rewritten by the next beam
+    }
+    if constexpr (COUNT) {
+        if (t == 0) {
+            atomicAdd(count, n_ex2);
+            atomicAdd(count + 1, n_eval);
+        }
+    } else if constexpr (MODE == kModeDose) {
+#pragma unroll
+        for (int q = 0; q < kLine; ++q)
+            if (q < nvalid) dose[vbase + q] = (tot_s[q] + tot_c[q]) * A.scale;
+    }
+}
+
+// Resident blocks per SM the line-tile kernels are compiled for (their
+// register budget): 16 of 32 threads, 8 of 64, 4 of 128.
+template <int NT> constexpr int line_min_blocks()
+{
+    return NT == 32 ? 16 : (NT == 64 ? 8 : 4);
+}
+
+// Tile coordinates of a linear block index over the grid's 8 x TY x TZ tiles.
+template <int TY, int TZ>
+__device__ __forceinline__ void line_tile_coords(const PbGrid &g, long long tile, int &tx,
+                                                 int &ty, int &tz)
+{
+    const int nx8 = (g.nx + kLine - 1) / kLine, nty = (g.ny + TY - 1) / TY;
+    tx = (int)(tile % nx8);
+    tile /= nx8;
+    ty = (int)(tile % nty);
+    tz = (int)(tile / nty);
+}
+
+template <int TY, int TZ, int KCULL, bool BEAM_OUT>
+__global__ void __launch_bounds__(TY * TZ, line_min_blocks<TY * TZ>())
+k_dose_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+            const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
+            const float *__restrict__ mu, float *__restrict__ dose,
+            float *__restrict__ beam_dose)
+{
+    __shared__ LineShared<TY * TZ, KCULL> sh;
+    int tx, ty, tz;
+    line_tile_coords<TY, TZ>(A.g, blockIdx.x, tx, ty, tz);
+    line_tile<TY, TZ, KCULL, BEAM_OUT>(A, tx, ty, tz, wet, layers, geo, mu, dose, beam_dose, sh);
+}
+
+// Line-tile shape of the default forward, its count and its adjoint.
+constexpr int kLineTY = 8, kLineTZ = 8, kLineCull = 4;
+
+__global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ>())
+k_dose_count_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+                  const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
+                  unsigned long long *count)
+{
+    __shared__ LineShared<kLineTY * kLineTZ, kLineCull> sh;
+    int tx, ty, tz;
+    line_tile_coords<kLineTY, kLineTZ>(A.g, blockIdx.x, tx, ty, tz);
+    line_tile<kLineTY, kLineTZ, kLineCull, false, kModeCount>(A, tx, ty, tz, wet, layers, geo,
+                                                              nullptr, nullptr, nullptr, sh,
+                                                              count);
+}
+
+__global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ>())
+k_adjoint_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+               const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
+               const float *__restrict__ wfield, float *__restrict__ grad)
+{
+    __shared__ LineShared<kLineTY * kLineTZ, kLineCull> sh;
+    int tx, ty, tz;
+    line_tile_coords<kLineTY, kLineTZ>(A.g, blockIdx.x, tx, ty, tz);
+    line_tile<kLineTY, kLineTZ, kLineCull, false, kModeAdjoint>(A, tx, ty, tz, wet, layers, geo,
+                                                                nullptr, nullptr, nullptr, sh,
+                                                                nullptr, wfield, grad);
+}
+
 #ifndef PB_DOSE_MIN_BLOCKS
 #define PB_DOSE_MIN_BLOCKS 5
 #endif
@@ -1062,6 +1542,42 @@ k_dose_batch(const BatchDose *__restrict__ plans, int n_plans, long long n_items
         dose_tile<NT, VPT, KCULL, false>(D.A, (int)(it - D.tile_start), D.wet, D.layers, D.geo,
                                          D.mu, D.dose, nullptr, sh);
         __syncthreads();
+    }
+}
+
+// The persistent batch on line tiles: the same queue of 8x8x8 units, each
+// done as (8/TY) x (8/TZ) tiles of the kernel's shape.
+template <int TY, int TZ, int KCULL>
+__global__ void __launch_bounds__(TY * TZ, line_min_blocks<TY * TZ>())
+k_dose_batch_line(const BatchDose *__restrict__ plans, int n_plans, long long n_items,
+                  unsigned long long *counter)
+{
+    static_assert(8 % TY == 0 && 8 % TZ == 0, "batch units are 8x8x8 voxels");
+    __shared__ LineShared<TY * TZ, KCULL> sh;
+    __shared__ long long s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(counter, 1ULL);
+        __syncthreads();
+        const long long it = s_item;
+        __syncthreads();
+        if (it >= n_items) break;
+        int lo = 0, hi = n_plans - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (plans[mid].tile_start <= it) lo = mid; else hi = mid - 1;
+        }
+        const BatchDose &D = plans[lo];
+        long long u = it - D.tile_start;
+        const int ux = (int)(u % D.A.tiles_x);
+        u /= D.A.tiles_x;
+        const int uy = (int)(u % D.A.tiles_y), uz = (int)(u / D.A.tiles_y);
+        for (int sz = 0; sz < 8 / TZ; ++sz)
+            for (int sy = 0; sy < 8 / TY; ++sy) {
+                line_tile<TY, TZ, KCULL, false>(D.A, ux, uy * (8 / TY) + sy, uz * (8 / TZ) + sz,
+                                                D.wet, D.layers, D.geo, D.mu, D.dose, nullptr,
+                                                sh);
+                __syncthreads();
+            }
     }
 }
 
@@ -1255,22 +1771,52 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
     for (int b = 0; b < n_beams; ++b) A.beams[b] = beams[b];
 }
 
-// Forward kernel variants the autotuner chooses from: block threads x voxels
-// per thread over the 8x8x8 tile, and spots culled per thread per round.
+// Forward kernel variants the autotuner chooses from.  Two families:
+//   t<threads>_v<voxels per thread>_c<k>  8x8x8 tiles, each thread a set of
+//       voxels evaluated one by one (dose_tile);
+//   l8x<TY>x<TZ>_c<k>  8 x TY x TZ tiles, each thread a line of 8 voxels
+//       along x evaluated as a quadratic (line_tile);
+// k = spots each thread culls per compaction round.  `batch` marks the
+// shapes the persistent batch kernel takes (tiles dividing 8x8x8 units).
 struct DoseVariant {
-    int nt, vpt, kcull;
+    int line, ty, tz, nt, kcull;
+    bool batch;
     const char *name;
 };
 static const DoseVariant kDoseVariants[] = {
-    {128, 4, 1, "t128_v4_c1"}, {128, 4, 2, "t128_v4_c2"}, {128, 4, 4, "t128_v4_c4"},
-    {256, 2, 1, "t256_v2_c1"}, {128, 4, 3, "t128_v4_c3"},
+    {0, 8, 8, 128, 1, true, "t128_v4_c1"},  {0, 8, 8, 128, 2, true, "t128_v4_c2"},
+    {0, 8, 8, 128, 4, true, "t128_v4_c4"},  {0, 8, 8, 256, 1, true, "t256_v2_c1"},
+    {0, 8, 8, 128, 3, true, "t128_v4_c3"},
+    {1, 8, 8, 64, 4, true, "l8x8x8_c4"},    {1, 8, 8, 64, 2, true, "l8x8x8_c2"},
+    {1, 8, 4, 32, 4, true, "l8x8x4_c4"},    {1, 4, 8, 32, 4, true, "l8x4x8_c4"},
+    {1, 16, 8, 128, 2, false, "l8x16x8_c2"}, {1, 8, 16, 128, 2, false, "l8x8x16_c2"},
 };
 constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
 
+// The shape pb_dose, pb_dose_adjoint and pb_count_evaluated use.
+constexpr int kDefaultDoseVariant = 0;
+
+int dose_variant_default() { return kDefaultDoseVariant; }
 int dose_variant_count() { return kNumDoseVariants; }
+
+static bool variant_line(int v)
+{
+    if (v < 0 || v >= kNumDoseVariants) v = kDefaultDoseVariant;
+    return kDoseVariants[v].line != 0;
+}
 const char *dose_variant_name(int v)
 {
     return (v >= 0 && v < kNumDoseVariants) ? kDoseVariants[v].name : "";
+}
+static bool dose_variant_batch(int v)
+{
+    return v >= 0 && v < kNumDoseVariants && kDoseVariants[v].batch;
+}
+
+static unsigned line_tiles(const PbGrid &g, int ty, int tz)
+{
+    return (unsigned)((long long)((g.nx + kLine - 1) / kLine) * ((g.ny + ty - 1) / ty) *
+                      ((g.nz + tz - 1) / tz));
 }
 
 template <int NT, int VPT, int KCULL>
@@ -1279,6 +1825,14 @@ static void launch_dose_t(const PlanArgs &A, unsigned tiles, const float *wet,
                           float *dose, cudaStream_t st)
 {
     k_dose<NT, VPT, KCULL, false><<<tiles, NT, 0, st>>>(A, wet, layers, geo, mu, dose, nullptr);
+}
+
+template <int TY, int TZ, int KCULL>
+static void launch_line_t(const PlanArgs &A, const float *wet, const PbLayer *layers,
+                          const float4 *geo, const float *mu, float *dose, cudaStream_t st)
+{
+    k_dose_line<TY, TZ, KCULL, false><<<line_tiles(A.g, TY, TZ), TY * TZ, 0, st>>>(
+        A, wet, layers, geo, mu, dose, nullptr);
 }
 
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
@@ -1290,9 +1844,16 @@ PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
     fill_args(A, g, beams, n_beams, scale);
     const unsigned tiles = (unsigned)((int64_t)A.tiles_x * A.tiles_y * A.tiles_z);
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
+    if (variant < 0) variant = kDefaultDoseVariant;
     if (beam_dose) {
-        // per-beam output: the default shape only
-        k_dose<128, 4, 1, true><<<tiles, 128, 0, st>>>(A, wet, layers, g4, mu, dose, beam_dose);
+        // per-beam output: the default shape of the variant's family only
+        if (variant_line(variant))
+            k_dose_line<kLineTY, kLineTZ, kLineCull, true>
+                <<<line_tiles(g, kLineTY, kLineTZ), kLineTY * kLineTZ, 0, st>>>(
+                    A, wet, layers, g4, mu, dose, beam_dose);
+        else
+            k_dose<128, 4, 1, true><<<tiles, 128, 0, st>>>(A, wet, layers, g4, mu, dose,
+                                                           beam_dose);
         return check_launch("k_dose");
     }
     switch (variant) {
@@ -1300,6 +1861,12 @@ PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
     case 2: launch_dose_t<128, 4, 4>(A, tiles, wet, layers, g4, mu, dose, st); break;
     case 3: launch_dose_t<256, 2, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
     case 4: launch_dose_t<128, 4, 3>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 5: launch_line_t<8, 8, 4>(A, wet, layers, g4, mu, dose, st); break;
+    case 6: launch_line_t<8, 8, 2>(A, wet, layers, g4, mu, dose, st); break;
+    case 7: launch_line_t<8, 4, 4>(A, wet, layers, g4, mu, dose, st); break;
+    case 8: launch_line_t<4, 8, 4>(A, wet, layers, g4, mu, dose, st); break;
+    case 9: launch_line_t<16, 8, 2>(A, wet, layers, g4, mu, dose, st); break;
+    case 10: launch_line_t<8, 16, 2>(A, wet, layers, g4, mu, dose, st); break;
     default: launch_dose_t<128, 4, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
     }
     return check_launch("k_dose");
@@ -1329,6 +1896,9 @@ PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items
                            unsigned long long *counter, int variant, int blocks,
                            cudaStream_t st)
 {
+    if (!dose_variant_batch(variant))
+        return set_error(PB_ERR_INVALID, "variant %d (%s) is not a batch shape", variant,
+                         dose_variant_name(variant));
     PbStatus s = check_cuda(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st),
                             "cudaMemsetAsync(queue)");
     if (s != PB_OK) return s;
@@ -1338,6 +1908,10 @@ PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items
     case 2: k_dose_batch<128, 4, 4><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     case 3: k_dose_batch<256, 2, 1><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
     case 4: k_dose_batch<128, 4, 3><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 5: k_dose_batch_line<8, 8, 4><<<blocks, 64, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 6: k_dose_batch_line<8, 8, 2><<<blocks, 64, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 7: k_dose_batch_line<8, 4, 4><<<blocks, 32, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 8: k_dose_batch_line<4, 8, 4><<<blocks, 32, 0, st>>>(P, n_plans, n_items, counter); break;
     default: k_dose_batch<128, 4, 1><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
     }
     return check_launch("k_dose_batch");
@@ -1350,7 +1924,8 @@ int dose_variant_threads(int variant)
 
 PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                         const float *wet, const PbLayer *layers, const float *geo,
-                        const float *w, float scale, float *grad, cudaStream_t st)
+                        const float *w, float scale, float *grad, cudaStream_t st,
+                        int variant)
 {
     PlanArgs A;
     fill_args(A, g, beams, n_beams, scale);
@@ -1363,9 +1938,13 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                             "cudaMemsetAsync(grad)");
     if (s != PB_OK) return s;
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
-    k_adjoint_tile<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers,
-                                                    reinterpret_cast<const float4 *>(geo), w,
-                                                    grad);
+    const float4 *g4 = reinterpret_cast<const float4 *>(geo);
+    if (variant_line(variant)) {
+        k_adjoint_line<<<line_tiles(g, kLineTY, kLineTZ), kLineTY * kLineTZ, 0, st>>>(
+            A, wet, layers, g4, w, grad);
+        return check_launch("k_adjoint_line");
+    }
+    k_adjoint_tile<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers, g4, w, grad);
     return check_launch("k_adjoint_tile");
 }
 
@@ -1425,7 +2004,7 @@ PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
 
 PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beams,
                                 const float *wet, const PbLayer *layers, const float *geo,
-                                unsigned long long *count, cudaStream_t st)
+                                unsigned long long *count, cudaStream_t st, int variant)
 {
     PlanArgs A;
     fill_args(A, g, beams, n_beams, 1.0f);
@@ -1433,8 +2012,13 @@ PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beam
                             "cudaMemsetAsync(count)");
     if (s != PB_OK) return s;
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
-    k_dose_count<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers,
-                                                  reinterpret_cast<const float4 *>(geo), count);
+    const float4 *g4 = reinterpret_cast<const float4 *>(geo);
+    if (variant_line(variant)) {
+        k_dose_count_line<<<line_tiles(g, kLineTY, kLineTZ), kLineTY * kLineTZ, 0, st>>>(
+            A, wet, layers, g4, count);
+        return check_launch("k_dose_count_line");
+    }
+    k_dose_count<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers, g4, count);
     return check_launch("k_dose_count");
 }
 

@@ -59,8 +59,11 @@ void texture_destroy(uint64_t h);
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers,
                      const float *geo, const float *mu, float scale,
-                     float *dose, float *beam_dose, cudaStream_t st, int variant = 0);
+                     float *dose, float *beam_dose, cudaStream_t st, int variant = -1);
 
+// variant < 0 selects the default forward shape (dose_variant_default);
+// the adjoint and the operation count use the kernel family of `variant`.
+int dose_variant_default();
 int dose_variant_count();
 const char *dose_variant_name(int v);
 int dose_variant_threads(int variant);
@@ -79,7 +82,7 @@ PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items
 PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                         const float *wet, const PbLayer *layers,
                         const float *geo, const float *w, float scale,
-                        float *grad, cudaStream_t st);
+                        float *grad, cudaStream_t st, int variant = -1);
 
 PbStatus launch_objective(const float *dose, const float *presc,
                           const float *weight, int64_t n, double *obj,
@@ -94,7 +97,7 @@ PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
                             const float *geo, cudaStream_t st);
 PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beams,
                                 const float *wet, const PbLayer *layers, const float *geo,
-                                unsigned long long *count, cudaStream_t st);
+                                unsigned long long *count, cudaStream_t st, int variant = -1);
 PbStatus measure_ex2_rate(double *ops_per_s, cudaStream_t st);
 PbStatus launch_count_pairs(const PbGrid &g, const PbBeam *beams, int n_beams,
                             const float *wet, const PbLayer *layers,

@@ -122,6 +122,9 @@ _SIGS = {
     "pb_dose_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP,
                              _VP]),
     "pb_dose_variant_count": (_I, []),
+    "pb_dose_variant_default": (_I, []),
+    "pb_dose_adjoint_variant": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F,
+                                     _VP, _I, _VP]),
     "pb_dose_variant_name": (ctypes.c_char_p, [_I]),
     "pb_dose_variant": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP, _I,
                              _VP]),

@@ -1,10 +1,15 @@
 """Autotuner for the forward pencil-beam kernel.
 
-The forward kernel exists in several shapes (block threads x voxels per
-thread over an 8x8x8 tile, and the number of spots each thread culls per
-compaction round; ``pb_dose_variant_name`` lists them), and the batched
-persistent launch also takes a number of resident blocks per SM.  Which is
-fastest depends on the grid size, the spot density and the beam count.  The
+The forward kernel exists in several shapes (``pb_dose_variant_name``
+lists them), in two families:
+  t<threads>_v<voxels per thread>_c<k>   8x8x8 voxel tiles, each thread a
+                                         set of voxels evaluated one by one;
+  l8x<TY>x<TZ>_c<k>                      8 x TY x TZ voxel tiles, each thread
+                                         a line of 8 voxels along x;
+with k the spots each thread culls per compaction round.  The batched
+persistent launch takes the shapes whose tiles divide an 8x8x8 block, and a
+number of resident blocks per SM.  Which is fastest depends on the grid
+size, the spot density and the beam count.  The
 tuner times every candidate with CUDA events on the workload at hand (after
 one warm-up run) and keeps the winner in a JSON cache keyed by GPU name and
 a size class, so that later plans of the same class skip the search.
@@ -68,8 +73,45 @@ def variants() -> Tuple[str, ...]:
     return tuple(_lib.lib.pb_dose_variant_name(v).decode() for v in range(n))
 
 
+def default_variant() -> int:
+    """The shape pb_dose uses."""
+    return int(_lib.lib.pb_dose_variant_default())
+
+
+def shape_of(name: str) -> Tuple[str, Tuple[int, int, int], int, int]:
+    """(family "t" or "l", voxel tile (x, y, z), block threads, spots culled
+    per thread per round) of a kernel shape."""
+    parts = name.split("_")
+    k = int(parts[-1][1:])
+    if name.startswith("l"):
+        tile = tuple(int(v) for v in parts[0][1:].split("x"))
+        return "l", tile, tile[1] * tile[2], k
+    return "t", (8, 8, 8), int(parts[0][1:]), k
+
+
 def threads_of(name: str) -> int:
-    return int(name.split("_")[0][1:])
+    return shape_of(name)[2]
+
+
+def round_size(name: str) -> int:
+    """Spots a kernel shape culls per compaction round (threads x k)."""
+    _, _, nt, k = shape_of(name)
+    return nt * k
+
+
+def same_decisions(a: str, b: str) -> bool:
+    """Two shapes whose doses are equal bit for bit: the same family and
+    tile (the same culling decisions and per-voxel arithmetic) and the same
+    round size (the same order of each layer's spots)."""
+    fa, ta, _, _ = shape_of(a)
+    fb, tb, _, _ = shape_of(b)
+    return fa == fb and ta == tb and round_size(a) == round_size(b)
+
+
+def batch_shape(name: str) -> bool:
+    """The persistent batch takes tiles that divide 8x8x8 blocks."""
+    _, (_, ty, tz), _, _ = shape_of(name)
+    return 8 % ty == 0 and 8 % tz == 0
 
 
 def best(candidates: Iterable, run: Callable, reps: int = 3, device=None):
@@ -106,25 +148,29 @@ def tune_plan(dp, reps: int = 3, use_cache: bool = True) -> int:
     return v
 
 
-def rounds_of(name: str) -> int:
-    """Rounds of spots a kernel shape culls at once (t<threads>_v<vpt>_c<k>)."""
-    return int(name.split("_")[2][1:])
-
-
 def max_blocks_per_sm(name: str) -> int:
-    """Resident blocks per SM a kernel shape is compiled for: 6 for 128
-    threads with one round, 5 for other 128-thread shapes, 3 for 256."""
-    if threads_of(name) != 128:
+    """Resident blocks per SM a kernel shape is compiled for.  8x8x8
+    family: 6 for 128 threads with one spot per thread per round, 5 for the
+    other 128-thread shapes, 3 for 256.  Line family: 16 of 32 threads, 8 of
+    64, 4 of 128."""
+    fam, _, nt, k = shape_of(name)
+    if fam == "l":
+        return {32: 16, 64: 8, 128: 4}[nt]
+    if nt != 128:
         return 3
-    return 6 if rounds_of(name) == 1 else 5
+    return 6 if k == 1 else 5
 
 
 def batch_candidates():
     """(variant, blocks per SM) pairs the batch launch accepts."""
     out = []
     for v, name in enumerate(variants()):
-        for bps in range(2, max_blocks_per_sm(name) + 1):
-            out.append((v, bps))
+        if not batch_shape(name):
+            continue
+        top = max_blocks_per_sm(name)
+        lo = 2 if shape_of(name)[0] == "t" else max(1, top // 4)
+        step = 1 if shape_of(name)[0] == "t" else max(1, top // 4)
+        out += [(v, bps) for bps in range(lo, top + 1, step)]
     return out
 
 

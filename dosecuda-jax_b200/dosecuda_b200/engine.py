@@ -294,18 +294,28 @@ class DevicePlan:
         return dose
 
     def adjoint(self, dobj_ddose: torch.Tensor, scale: float = 1.0,
-                out: Optional[torch.Tensor] = None) -> torch.Tensor:
-        """grad[s] (sorted order) = scale * sum_v dobj_ddose[v] K(v, s)."""
+                out: Optional[torch.Tensor] = None,
+                variant: Optional[int] = None) -> torch.Tensor:
+        """grad[s] (sorted order) = scale * sum_v dobj_ddose[v] K(v, s).
+        variant: the kernel family of that forward shape (default: the
+        library's default shape)."""
         self._need_wet()
         if dobj_ddose.dtype != torch.float32 or dobj_ddose.numel() != self.n_vox:
             raise ValueError("dobj_ddose must be float32 with one entry per voxel")
         w = dobj_ddose.contiguous()
         grad = out if out is not None else torch.empty(max(self.n_spots, 1), dtype=torch.float32,
                                                        device=self.device)
-        check(_lib.lib.pb_dose_adjoint(ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p),
-                                       self.n_beams, ptr(self.wet), ptr(self.layers),
-                                       ptr(self.spot_geo), ptr(w), float(scale), ptr(grad),
-                                       _stream(self.device)), "pb_dose_adjoint")
+        if variant is None:
+            check(_lib.lib.pb_dose_adjoint(ctypes.byref(self.grid),
+                                           ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                                           ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
+                                           ptr(w), float(scale), ptr(grad),
+                                           _stream(self.device)), "pb_dose_adjoint")
+        else:
+            check(_lib.lib.pb_dose_adjoint_variant(
+                ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                ptr(self.wet), ptr(self.layers), ptr(self.spot_geo), ptr(w), float(scale),
+                ptr(grad), int(variant), _stream(self.device)), "pb_dose_adjoint_variant")
         return grad[: self.n_spots]
 
     def adjoint_positions(self, dobj_ddose: torch.Tensor, scale: float = 1.0,

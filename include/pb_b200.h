@@ -255,10 +255,16 @@ PbStatus pb_count_evaluated(const PbGrid *grid, const PbBeam *beams, int n_beams
  * reference. */
 PbStatus pb_measure_ex2_rate(double *ops_per_s, void *stream);
 
-/* Forward kernel shapes (block threads x voxels per thread over an 8x8x8
- * tile, spots culled per thread per round) the autotuner chooses from.
- * pb_dose uses variant 0. */
+/* Forward kernel shapes the autotuner chooses from, in two families:
+ * "t<threads>_v<voxels per thread>_c<k>" works on 8x8x8 voxel tiles, each
+ * thread evaluating its voxels one by one; "l8x<TY>x<TZ>_c<k>" works on
+ * 8 x TY x TZ tiles, each thread a line of 8 voxels along x whose squared
+ * distances to a spot's axis are one quadratic; k is the spots each thread
+ * culls per compaction round.  pb_dose, pb_dose_adjoint and
+ * pb_count_evaluated use pb_dose_variant_default().  No counterpart in the
+ * reference (its kernel has one shape, CudaClasses.cuh:14). */
 int pb_dose_variant_count(void);
+int pb_dose_variant_default(void);
 const char *pb_dose_variant_name(int variant);
 PbStatus pb_dose_variant(const PbGrid *grid, const PbBeam *beams, int n_beams,
                          const float *wet_dev, const PbLayer *layers_dev,
@@ -322,6 +328,12 @@ PbStatus pb_dose_adjoint(const PbGrid *grid, const PbBeam *beams, int n_beams,
                          const float *wet_dev, const PbLayer *layers_dev,
                          const float *spot_geo_dev, const float *dobj_dose_dev,
                          float scale, float *grad_dev, void *stream);
+/* pb_dose_adjoint with the kernel family of forward shape `variant`
+ * (pb_dose_variant_name): the same gradient, to float rounding. */
+PbStatus pb_dose_adjoint_variant(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                 const float *wet_dev, const PbLayer *layers_dev,
+                                 const float *spot_geo_dev, const float *dobj_dose_dev,
+                                 float scale, float *grad_dev, int variant, void *stream);
 
 /* Quadratic objective sum_v w_v (D_v - P_v)^2, reduced in FP64 into
  * *obj_dev, and its gradient 2 w_v (D_v - P_v) into resid_dev (nullable).

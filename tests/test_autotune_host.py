@@ -21,6 +21,17 @@ def test_variants_and_batch_candidates():
     assert autotune.max_blocks_per_sm("t128_v4_c2") == 5
     assert autotune.max_blocks_per_sm("t256_v2_c1") == 3
     assert (0, 6) in cands
+    # the line family: voxel-tile shapes as well as round sizes are tuned
+    lines = [n for n in names if autotune.shape_of(n)[0] == "l"]
+    assert {autotune.shape_of(n)[1] for n in lines} >= {(8, 8, 8), (8, 8, 4), (8, 4, 8),
+                                                        (8, 16, 8), (8, 8, 16)}
+    assert autotune.shape_of("l8x8x4_c4") == ("l", (8, 8, 4), 32, 4)
+    assert autotune.round_size("l8x8x8_c4") == 256 == autotune.round_size("t128_v4_c2")
+    assert not autotune.same_decisions("l8x8x8_c4", "t128_v4_c2")
+    assert autotune.same_decisions("t128_v4_c2", "t256_v2_c1")
+    assert autotune.max_blocks_per_sm("l8x8x4_c4") == 16
+    assert autotune.batch_shape("l8x4x8_c4") and not autotune.batch_shape("l8x8x16_c2")
+    assert {names[v] for v, _ in cands} == {n for n in names if autotune.batch_shape(n)}
 
 
 def test_cache_roundtrip(tmp_path, monkeypatch):
