@@ -107,11 +107,45 @@ def grid_of(volume_shape: Sequence[int], spacing: float) -> PbGrid:
     return PbGrid(nx, ny, nz, float(spacing))
 
 
+class TexturePool:
+    """Texture and cell-record handles kept across the plans of one grid,
+    so that repeated dose calls on the same CT refill them instead of
+    allocating and freeing them every time (the reference creates and
+    destroys its texture on every call, TextureClasses.cu:14-41).  Plans
+    that share a pool must run one at a time in stream order on one
+    stream: a pooled handle holds the RLSP it was last filled with."""
+
+    def __init__(self):
+        self._handles = {}
+
+    def holder(self, device: torch.device, shape, kind: str) -> ctypes.c_uint64:
+        key = (device.index, tuple(int(v) for v in shape), kind)
+        h = self._handles.get(key)
+        if h is None:
+            h = ctypes.c_uint64(0)
+            self._handles[key] = h
+        return h
+
+    def close(self) -> None:
+        for (dev, _, _), h in list(self._handles.items()):
+            if h.value:
+                try:
+                    torch.cuda.synchronize(dev)
+                    _lib.lib.pb_texture_destroy(h)
+                except Exception:
+                    pass
+                h.value = 0
+        self._handles.clear()
+
+    def __del__(self):
+        self.close()
+
+
 class DevicePlan:
     """A plan prepared on one GPU (see module docstring)."""
 
     def __init__(self, volume_shape, spacing: float, origin, beams: List[BeamSpec],
-                 device="cuda"):
+                 device="cuda", texture_pool: Optional[TexturePool] = None):
         self.device = require_cuda(device)
         if not beams:
             raise ValueError("a plan needs at least one beam")
@@ -180,11 +214,19 @@ class DevicePlan:
                                            _stream(self.device)), "pb_layer_bounds")
         self.wet: Optional[torch.Tensor] = None
         self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
-        self._tex = ctypes.c_uint64(0)
-        self._cells = ctypes.c_uint64(0)
+        # texture / cell-record handles: the plan's own, or a pool's
+        self._owns_textures = texture_pool is None
+        if texture_pool is None:
+            self._tex = ctypes.c_uint64(0)
+            self._cells = ctypes.c_uint64(0)
+        else:
+            self._tex = texture_pool.holder(self.device, self.shape, "texture")
+            self._cells = texture_pool.holder(self.device, self.shape, "cells")
         self.wet_mode = "texture"
 
     def __del__(self):
+        if not getattr(self, "_owns_textures", True):
+            return
         for name in ("_tex", "_cells"):
             h = getattr(self, name, None)
             if h is not None and h.value:

@@ -172,15 +172,27 @@ class IMPTDoseGrid(DoseGrid):
         optimisation loop reuses (engine.DevicePlan).  wet_mode "texture"
         reproduces the reference's texture-sampled WET; "exact" uses exact
         trilinear interpolation."""
+        return self._prepare(plan, gpu_id, beams, wet_mode, None)
+
+    def _prepare(self, plan, gpu_id, beams, wet_mode, pool):
         self._check_isotropic()
         device = self._device(gpu_id)
         rlsp = self._rlsp_device(plan.machine_name, device)
         beams = plan.beam_list if beams is None else beams
         dp = _engine().DevicePlan(np.shape(self.HU), float(self.spacing[0]),
-                               np.asarray(self.origin, dtype=np.single),
-                               self._specs(plan, beams), device)
+                                  np.asarray(self.origin, dtype=np.single),
+                                  self._specs(plan, beams), device, texture_pool=pool)
         dp.compute_wet(rlsp.reshape(-1), wet_mode=wet_mode)
         return dp
+
+    def _transient(self, plan, gpu_id, beams, wet_mode):
+        """A plan used within one call (computeIMPTPlan, computeIMPTWET): its
+        texture and cell records come from this grid's pool and are kept for
+        the next call."""
+        pool = self.__dict__.get("_pb_texture_pool")
+        if pool is None:
+            pool = self._pb_texture_pool = _engine().TexturePool()
+        return self._prepare(plan, gpu_id, beams, wet_mode, pool)
 
     def _beam_chunks(self, plan):
         """The plan's beams in groups the device kernels take at once (the
@@ -202,7 +214,7 @@ class IMPTDoseGrid(DoseGrid):
         shape = np.shape(self.HU)
         total = None
         for chunk in self._beam_chunks(plan):
-            dp = self.prepareIMPTPlan(plan, gpu_id, beams=chunk, wet_mode=wet_mode)
+            dp = self._transient(plan, gpu_id, chunk, wet_mode)
             dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
             bd_host = bd.cpu().numpy()
             self.beam_doses += [bd_host[b].reshape(shape) for b in range(dp.n_beams)]
@@ -215,7 +227,7 @@ class IMPTDoseGrid(DoseGrid):
         self._check_isotropic()
         out = []
         for chunk in self._beam_chunks(plan):
-            dp = self.prepareIMPTPlan(plan, gpu_id, beams=chunk, wet_mode=wet_mode)
+            dp = self._transient(plan, gpu_id, chunk, wet_mode)
             wet = dp.wet.cpu().numpy()
             for b in range(dp.n_beams):
                 wet_object = VolumeObject()
