@@ -111,6 +111,14 @@ def _hu_curve(machine_name):
     return df["HU"].to_numpy(dtype=np.float64), df["RLSP"].to_numpy(dtype=np.float64)
 
 
+def _pinned_copy(t: torch.Tensor) -> torch.Tensor:
+    """An asynchronous copy of a device tensor into page-locked host memory
+    (torch's pinned-memory cache), on the current stream."""
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    return h
+
+
 def _beam_model(plan, beam):
     try:
         model_index = list(plan.dicom_rangeshifter_label.astype(str)).index(
@@ -174,10 +182,11 @@ class IMPTDoseGrid(DoseGrid):
         trilinear interpolation."""
         return self._prepare(plan, gpu_id, beams, wet_mode, None)
 
-    def _prepare(self, plan, gpu_id, beams, wet_mode, pool):
+    def _prepare(self, plan, gpu_id, beams, wet_mode, pool, rlsp=None):
         self._check_isotropic()
         device = self._device(gpu_id)
-        rlsp = self._rlsp_device(plan.machine_name, device)
+        if rlsp is None:
+            rlsp = self._rlsp_device(plan.machine_name, device)
         beams = plan.beam_list if beams is None else beams
         dp = _engine().DevicePlan(np.shape(self.HU), float(self.spacing[0]),
                                   np.asarray(self.origin, dtype=np.single),
@@ -185,14 +194,14 @@ class IMPTDoseGrid(DoseGrid):
         dp.compute_wet(rlsp.reshape(-1), wet_mode=wet_mode)
         return dp
 
-    def _transient(self, plan, gpu_id, beams, wet_mode):
+    def _transient(self, plan, gpu_id, beams, wet_mode, rlsp=None):
         """A plan used within one call (computeIMPTPlan, computeIMPTWET): its
         texture and cell records come from this grid's pool and are kept for
         the next call."""
         pool = self.__dict__.get("_pb_texture_pool")
         if pool is None:
             pool = self._pb_texture_pool = _engine().TexturePool()
-        return self._prepare(plan, gpu_id, beams, wet_mode, pool)
+        return self._prepare(plan, gpu_id, beams, wet_mode, pool, rlsp)
 
     def _beam_chunks(self, plan):
         """The plan's beams in groups the device kernels take at once (the
@@ -203,24 +212,44 @@ class IMPTDoseGrid(DoseGrid):
 
     def computeIMPTPlan(self, plan, gpu_id=0, wet_mode="texture"):
         """Dose of every beam and their sum, times n_fractions
-        (plan_impt.py:170-206)."""
+        (plan_impt.py:170-206).
+
+        The results come back into page-locked host memory from torch's
+        pinned-memory cache (reused once the previous call's arrays are
+        released), and the RLSP volume's copy runs on a second stream while
+        the WET and dose are computed."""
         self.beam_doses = []
-        self.dose = np.zeros(self.size, dtype=np.single)
         self._check_isotropic()
         if not plan.beam_list:
+            self.dose = np.zeros(self.size, dtype=np.single)
             self.RLSP = self.RLSPFromHU(plan.machine_name, gpu_id)
             self.dose *= plan.n_fractions
             return
         shape = np.shape(self.HU)
-        total = None
+        device = self._device(gpu_id)
+        main = torch.cuda.current_stream(device)
+        rlsp = self._rlsp_device(plan.machine_name, device)
+        side = self.__dict__.get("_pb_copy_stream")
+        if side is None or side.device != device:
+            side = self._pb_copy_stream = torch.cuda.Stream(device)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            rlsp_h = _pinned_copy(rlsp)
+        total, beams_h, keep = None, [], []
         for chunk in self._beam_chunks(plan):
-            dp = self._transient(plan, gpu_id, chunk, wet_mode)
+            dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
             dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
-            bd_host = bd.cpu().numpy()
-            self.beam_doses += [bd_host[b].reshape(shape) for b in range(dp.n_beams)]
+            beams_h.append((_pinned_copy(bd), dp.n_beams))
+            keep.append(bd)
             total = dose if total is None else total + dose
-        self.RLSP = self._device_rlsp.cpu().numpy().reshape(shape)
-        self.dose = total.cpu().numpy().reshape(shape)
+        dose_h = _pinned_copy(total)
+        main.synchronize()
+        side.synchronize()
+        for bd_h, n in beams_h:
+            arr = bd_h.numpy()
+            self.beam_doses += [arr[b].reshape(shape) for b in range(n)]
+        self.RLSP = rlsp_h.numpy().reshape(shape)
+        self.dose = dose_h.numpy().reshape(shape)
 
     def computeIMPTWET(self, plan, gpu_id=0, wet_mode="texture"):
         """Per-beam WET volumes as VolumeObjects (plan_impt.py:208-236)."""
