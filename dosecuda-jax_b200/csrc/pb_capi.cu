@@ -278,6 +278,12 @@ PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
                       raw_work_dev, wet_dev, status_dev, static_cast<cudaStream_t>(stream));
 }
 
+PbStatus pb_smooth_dirs(float *cos_out, float *sin_out)
+{
+    if (!cos_out || !sin_out) return set_error(PB_ERR_INVALID, "NULL argument");
+    return device_smooth_dirs(cos_out, sin_out);
+}
+
 PbStatus pb_smooth_table(const PbGrid *grid, const PbBeamGeom *beams, int n_beams, int beam,
                          int *off, float *hh, unsigned *tmask, int *margin)
 {

@@ -22,6 +22,10 @@ void smooth_dirs(float *c, float *s);
 
 int ray_step_cap(const PbGrid &g);
 
+// The smoothing directions as the smoothing kernels form them on the
+// current device (CUDA's sincosf), copied to the host.
+PbStatus device_smooth_dirs(float *c, float *s);
+
 PbStatus launch_rlsp(const float *hu, int64_t n, const double *xh,
                      const double *yh, int m, float *out, cudaStream_t st);
 

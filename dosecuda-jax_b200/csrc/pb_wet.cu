@@ -365,7 +365,6 @@ k_raytrace(const float *__restrict__ rho, cudaTextureObject_t tex,
 // flagged triple, the half-integer the position is compared with.
 struct SmoothBeam {
     int off[6][9];            // linear-index offset when no axis is flagged
-    float rc[6][9], rs[6][9]; // dr * cos, dr * sin in FP32 (the reference's products)
     float hh[6][9][3];        // per-axis index offset ro + 1/2: ro = round(dr * dm_a),
                               // floor where flagged
     unsigned tmask[6];        // 3 bits (x, y, z) per radius, radius 1 lowest
@@ -420,8 +419,6 @@ static void smooth_table(const PbGrid &g, const PbBeamGeom &B, const float *c, c
             const double dr = (double)(r + 1);
             // dr is a small integer, so the FP64 product is exact and its
             // FP32 rounding is the FP32 product
-            T.rc[dd][r] = (float)(dr * (double)c[dd]);
-            T.rs[dd][r] = (float)(dr * (double)sn[dd]);
             int64_t off = 0;
             for (int a = 0; a < 3; ++a) {
                 const double x = dr * dm[a];
@@ -485,13 +482,25 @@ __device__ __forceinline__ int round_up(float q, float h, float s, float inv_s)
 // isocentre) divided by the spacing and rounded, as 0/1 steps from the
 // table's lower candidates; fi, fj, fk are the voxel's indexes as floats.
 // Only the flagged axes' image coordinates are formed.
+// The six smoothing directions (cos, sin of i pi/3) as the reference forms
+// them on the device: the FP32 angle (float)i * pi / 3 and CUDA's sincosf
+// (IMPTClasses.cu:175-177).  Ties decided by the FP32 sample positions
+// depend on these exact values, so they are CUDA's, not the host library's.
+__device__ __forceinline__ void smooth_dir_dev(int i, float &c, float &s)
+{
+    sincosf(__fdiv_rn(__fmul_rn((float)i, 3.141592654f), 3.0f), &s, &c);
+}
+
 template <bool POW2>
 __device__ __forceinline__ void exact_steps(const PbBeamGeom &B, const SmoothBeam &T, float s,
-                                            float hx, float hy, float hz, float fi, float fj,
-                                            float fk, int dd, int r, int axes, int &ui, int &uj,
-                                            int &uk)
+                                            const float *dc, const float *ds, float hx,
+                                            float hy, float hz, float fi, float fj, float fk,
+                                            int dd, int r, int axes, int &ui, int &uj, int &uk)
 {
-    const float hxs = __fadd_rn(hx, T.rc[dd][r]), hys = __fadd_rn(hy, T.rs[dd][r]);
+    // dr * cos, dr * sin in FP32 (dr = r + 1 mm is exact), the reference's products
+    const float dr = (float)(r + 1);
+    const float hxs = __fadd_rn(hx, __fmul_rn(dr, dc[dd]));
+    const float hys = __fadd_rn(hy, __fmul_rn(dr, ds[dd]));
     float qx, qy, qz;
     if (axes & 1) {
         head_to_image(B, hxs, hys, hz, qx, qy, qz);
@@ -520,8 +529,9 @@ __device__ __forceinline__ void exact_steps(const PbBeamGeom &B, const SmoothBea
 // of two.
 template <bool POW2>
 __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const PbGrid &g,
-                                              const PbBeamGeom &Bp, const SmoothBeam &T, int i,
-                                              int j, int k, int *adj = nullptr, int nt = 0)
+                                              const PbBeamGeom &Bp, const SmoothBeam &T,
+                                              const float *dc, const float *ds, int i, int j,
+                                              int k, int *adj = nullptr, int nt = 0)
 {
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
     const float center = R[v];
@@ -558,7 +568,8 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
                 const int n = T.flist[f], dd = n / 9, r = n - 9 * dd;
                 const int axes = (T.tmask[dd] >> (3 * r)) & 7u;
                 int ui = 0, uj = 0, uk = 0;
-                exact_steps<POW2>(B, T, s, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj, uk);
+                exact_steps<POW2>(B, T, s, dc, ds, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj,
+                                  uk);
                 adj[f * nt] = ui + sy * uj + sz * uk;
             }
 #pragma unroll
@@ -584,7 +595,7 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
                 int idx = vi + T.off[dd][r];
                 if (axes) {
                     int ui = 0, uj = 0, uk = 0;
-                    exact_steps<POW2>(B, T, s, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj,
+                    exact_steps<POW2>(B, T, s, dc, ds, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj,
                                       uk);
                     idx += ui + sy * uj + sz * uk;
                 }
@@ -604,7 +615,8 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
             const int axes = tm & 7u;
             if (axes) {
                 int ui = 0, uj = 0, uk = 0;
-                exact_steps<POW2>(B, T, s, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj, uk);
+                exact_steps<POW2>(B, T, s, dc, ds, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj,
+                                  uk);
                 ii += ui;
                 jj += uj;
                 kk += uk;
@@ -629,7 +641,10 @@ k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGe
          const __grid_constant__ SmoothSet st, int zbricks, float *__restrict__ wet)
 {
     __shared__ int s_adj[kMaxFlag * 128];
+    __shared__ float s_dc[6], s_ds[6];
     const int tid = threadIdx.x + 8 * (threadIdx.y + 4 * threadIdx.z);
+    if (tid < 6) smooth_dir_dev(tid, s_dc[tid], s_ds[tid]);
+    __syncthreads();
     const int b = blockIdx.z / zbricks;
     const int k = (blockIdx.z - b * zbricks) * 4 + threadIdx.z;
     const int j = blockIdx.y * 4 + threadIdx.y;
@@ -637,8 +652,8 @@ k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGe
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
-    wet[b * V + v] = smooth_voxel<POW2>(raw + b * V, g, bs.b[b], st.b[b], i, j, k, s_adj + tid,
-                                        128);
+    wet[b * V + v] = smooth_voxel<POW2>(raw + b * V, g, bs.b[b], st.b[b], s_dc, s_ds, i, j, k,
+                                        s_adj + tid, 128);
 }
 
 // One (plan, beam) of a batched WET pass.
@@ -700,6 +715,8 @@ k_smooth_batch(const BatchWet *__restrict__ items, int n_items)
     static_assert(sizeof(SmoothBeam) % 4 == 0, "the table is copied as words");
     __shared__ SmoothBeam sm;
     __shared__ int s_adj[kMaxFlag * 128];
+    __shared__ float s_dc[6], s_ds[6];
+    if (threadIdx.x < 6) smooth_dir_dev(threadIdx.x, s_dc[threadIdx.x], s_ds[threadIdx.x]);
     const BatchWet &W = items[find_wet_item(items, n_items, blockIdx.x)];
     // the block's sample table into shared memory (one item per block)
     const int *src = reinterpret_cast<const int *>(&W.sm);
@@ -710,9 +727,34 @@ k_smooth_batch(const BatchWet *__restrict__ items, int n_items)
     int i, j, k;
     if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
     float *out = W.wet + i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k);
-    *out = sm.pow2 ? smooth_voxel<true>(W.raw, W.g, W.geom, sm, i, j, k, s_adj + threadIdx.x, 128)
-                   : smooth_voxel<false>(W.raw, W.g, W.geom, sm, i, j, k, s_adj + threadIdx.x,
-                                         128);
+    *out = sm.pow2 ? smooth_voxel<true>(W.raw, W.g, W.geom, sm, s_dc, s_ds, i, j, k,
+                                        s_adj + threadIdx.x, 128)
+                   : smooth_voxel<false>(W.raw, W.g, W.geom, sm, s_dc, s_ds, i, j, k,
+                                         s_adj + threadIdx.x, 128);
+}
+
+__device__ float g_smooth_dirs[12];
+
+__global__ void k_smooth_dirs()
+{
+    if (threadIdx.x < 6)
+        smooth_dir_dev(threadIdx.x, g_smooth_dirs[threadIdx.x], g_smooth_dirs[6 + threadIdx.x]);
+}
+
+PbStatus device_smooth_dirs(float *c, float *s)
+{
+    k_smooth_dirs<<<1, 32>>>();
+    PbStatus st = check_launch("k_smooth_dirs");
+    float v[12];
+    if (st == PB_OK)
+        st = check_cuda(cudaMemcpyFromSymbol(v, g_smooth_dirs, sizeof(v)),
+                        "cudaMemcpyFromSymbol(directions)");
+    if (st != PB_OK) return st;
+    for (int i = 0; i < 6; ++i) {
+        c[i] = v[i];
+        s[i] = v[6 + i];
+    }
+    return PB_OK;
 }
 
 int ray_step_cap(const PbGrid &g)

@@ -118,6 +118,7 @@ _SIGS = {
     "pb_wet": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP]),
     "pb_wet_noalloc": (_I, [_VP, ctypes.c_uint64, ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP]),
     "pb_smooth_table": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _I, _VP, _VP, _VP, _VP]),
+    "pb_smooth_dirs": (_I, [_VP, _VP]),
     "pb_dose": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP, _VP, _VP]),
     "pb_dose_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F, _VP,
                              _VP]),
@@ -208,6 +209,15 @@ def smooth_table(shape, spacing: float, geoms, beam: int = 0):
                               int(beam), ptr(off), ptr(hh), ptr(tmask), ptr(margin)),
           "pb_smooth_table")
     return off, hh, tmask, margin
+
+
+def smooth_dirs():
+    """(cos, sin) of the six smoothing directions as the kernels form them
+    on the current device (pb_smooth_dirs)."""
+    c = np.zeros(6, np.float32)
+    s = np.zeros(6, np.float32)
+    check(lib.pb_smooth_dirs(ptr(c), ptr(s)), "pb_smooth_dirs")
+    return c, s
 
 
 def build_layers(spot_list: np.ndarray, dvp: np.ndarray):

@@ -205,6 +205,15 @@ PbStatus pb_wet_noalloc(const float *rlsp_dev, PbTexture tex, const PbGrid *grid
 PbStatus pb_smooth_table(const PbGrid *grid, const PbBeamGeom *beams, int n_beams, int beam,
                          int *off, float *hh, unsigned *tmask, int *margin);
 
+/* The cosines and sines of the six smoothing directions (angle d*pi/3) as
+ * the smoothing kernels use them: the reference forms them on the device
+ * with CUDA's sincosf of the FP32 angle (IMPTClasses.cu:175-177), and where
+ * a sample lies on a half-voxel their last bit decides which voxel it
+ * reads.  Runs a one-thread kernel on the current device and copies the
+ * twelve values back (synchronous).  No counterpart in the reference: for
+ * tests and inspection. */
+PbStatus pb_smooth_dirs(float cos_out[6], float sin_out[6]);
+
 /* Forward pencil-beam dose of a plan (IMPTClasses.cu:204-271) for all of
  * its beams in one launch.  wet_dev: n_beams x V (cm).  layers_dev: all
  * layers, beam-major.  spot_geo_dev: PB_SPOT_GEO_FLOATS per spot, mu_dev:

@@ -63,6 +63,7 @@ def load(port32: bool = False):
     vp, i, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
     lib.ob_beam_setup.argtypes = [ctypes.c_double] * 4 + [vp, vp, ctypes.POINTER(OBeam)]
     lib.ob_smooth_dirs.argtypes = [vp, vp]
+    lib.ob_set_smooth_dirs.argtypes = [vp, vp]
     lib.ob_raytrace.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp, i64, vp]
     lib.ob_raytrace.restype = i
     lib.ob_smooth.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp, i64, vp]
@@ -91,6 +92,20 @@ def beam_setup(gantry, couch, vsadx, vsady, iso, origin, port32=False) -> OBeam:
     lib.ob_beam_setup(float(gantry), float(couch), float(vsadx), float(vsady), _p(iso),
                       _p(origin), ctypes.byref(b))
     return b
+
+
+def set_smooth_dirs(c=None, s=None):
+    """Use these smoothing directions (cos, sin of i*pi/3, FP32) in every
+    smoothing call, as the reference's device sincosf gives them; None goes
+    back to the C library's values."""
+    for port32 in (False, True):
+        lib = load(port32)
+        if c is None:
+            lib.ob_set_smooth_dirs(None, None)
+        else:
+            cc = np.ascontiguousarray(c, np.float32)
+            ss = np.ascontiguousarray(s, np.float32)
+            lib.ob_set_smooth_dirs(_p(cc), _p(ss))
 
 
 def smooth_dirs():

@@ -111,9 +111,31 @@ void ob_beam_setup(double gantry_deg, double couch_deg, double vsadx,
         b->iso[d] = iso[d] - origin[d];
 }
 
-/* Six lateral smoothing directions, angle i*pi/3 (IMPTClasses.cu:173-177). */
+/* Six lateral smoothing directions, angle i*pi/3 (IMPTClasses.cu:173-177).
+ * The reference takes them from CUDA's sincosf on the device; a caller that
+ * has those values (from the GPU) sets them with ob_set_smooth_dirs, else
+ * the C library's cosf/sinf of the same FP32 angle are used. */
+static float g_set_c[6], g_set_s[6];
+static int g_dirs_set = 0;
+
+void ob_set_smooth_dirs(const float *c, const float *s)
+{
+    g_dirs_set = c && s;
+    for (int i = 0; g_dirs_set && i < 6; i++) {
+        g_set_c[i] = c[i];
+        g_set_s[i] = s[i];
+    }
+}
+
 void ob_smooth_dirs(float *c, float *s)
 {
+    if (g_dirs_set) {
+        for (int i = 0; i < 6; i++) {
+            c[i] = g_set_c[i];
+            s[i] = g_set_s[i];
+        }
+        return;
+    }
     for (int i = 0; i < 6; i++) {
         /* volatile: the values must come from the C library at run time,
          * not from compile-time folding */

@@ -71,8 +71,14 @@ def max_rel(a, b, ref_max=None):
 
 @pytest.fixture(scope="session")
 def oracle():
+    """The CPU oracle.  With a CUDA device present its smoothing takes the
+    six directions from the device's sincosf (pb_smooth_dirs), as the
+    reference and the kernels do; without one, the C library's."""
     from oracle import oracle as O
     O.load()
+    if cuda_available():
+        from dosecuda_b200 import _lib
+        O.set_smooth_dirs(*_lib.smooth_dirs())
     return O
 
 

@@ -2,11 +2,16 @@
 
 * Texture-mode WET and dose of the 3-beam (~8k spots) and 4-beam (~19k
   spots) heterogeneous plans against the reference's own CUDA module
-  (oracle/_ref) at every voxel: dose within 1e-3 of Dmax (the drop-in bar),
-  the pencil-beam pass on the reference's own WET within 2e-4 of Dmax, and
-  the WET maximum stated.  The WET residue is the reference's FP32 running
-  sum (fmaf per 1 mm sample, CudaClasses.cu:206-222) against the FP64 sum
-  here, which grows with the ray length.
+  (oracle/_ref) at every voxel: dose within 1e-3 of Dmax (the drop-in bar)
+  and the WET maximum stated.  The WET residue is the reference's FP32
+  running sum (fmaf per 1 mm sample, CudaClasses.cu:206-222) against the
+  FP64 sum here, which grows with the ray length.
+* The pencil-beam pass alone on the reference's own WET: within 1e-3 of
+  Dmax at every voxel, and at the 40 voxels where it differs most from the
+  reference, within 2e-5 of Dmax of the FP64 oracle on that WET.  At full
+  size the reference's FP32 axis distance |ray|^2 - (t.ray)^2/|t|^2
+  (IMPTClasses.cu:123-133) loses digits to cancellation (both terms are
+  ~Z^2 at depth); this path forms |t x ray|^2/|t|^2, which does not.
 * The 4-beam plan's spot-weight gradient (texture WET, the benchmarked
   step) against the FP64 oracle adjoint on 200 seeded spots, same WET and
   residual: within 1e-4 of max |g| over those spots.
@@ -50,7 +55,8 @@ def curve():
 
 
 @pytest.mark.parametrize("which", ["three_beams_8k", "four_beams_20k"])
-def test_full_size_texture_mode_matches_reference_every_voxel(which, curve, reference_module):
+def test_full_size_texture_mode_matches_reference_every_voxel(which, curve, reference_module,
+                                                               oracle):
     from dosecuda_b200 import engine, phantoms
     case = (phantoms.config_forward_heterogeneous() if which == "three_beams_8k"
             else phantoms.config_gradient())
@@ -65,7 +71,7 @@ def test_full_size_texture_mode_matches_reference_every_voxel(which, curve, refe
 
     rlsp = np.array(np.interp(g.HU, *curve), dtype=np.single)
     ref_total = np.zeros(shape, np.float64)
-    dwet, dbeam, dpass = [], [], []
+    dwet, dbeam, dpass, dor_mine, dor_ref = [], [], [], [], []
     for b, beam in enumerate(plan.beam_list):
         model = _model(plan, beam)
         beam.spot_list = np.asarray(beam.spot_list, np.float32).reshape(-1, 4)
@@ -79,14 +85,27 @@ def test_full_size_texture_mode_matches_reference_every_voxel(which, curve, refe
                                 [engine.BeamSpec(beam.gantry_angle, beam.couch_angle, beam.iso,
                                                  beam.spot_list, model)], DEV)
         one.set_wet(torch.from_numpy(rw).to(DEV))
-        dpass.append(max_rel(one.forward().cpu().numpy().reshape(shape), rd))
+        mine = one.forward().cpu().numpy().reshape(shape)
+        dpass.append(max_rel(mine, rd))
         del one
+        # the FP64 oracle on the reference's WET where the two differ most
+        idx = np.argsort(np.abs(mine - rd).ravel())[-40:].astype(np.int64)
+        m = oracle.Model(model)
+        ob = oracle.beam_setup(beam.gantry_angle, beam.couch_angle, m.vsadx, m.vsady,
+                               beam.iso, g.origin)
+        spots, lay = oracle.build_layers(beam.spot_list, m.dvp)
+        want = oracle.dose(rw, g.spacing[0], ob, m, spots, lay, idx)
+        dmax = float(rd.max())
+        dor_mine.append(float(np.abs(mine.ravel()[idx] - want).max() / dmax))
+        dor_ref.append(float(np.abs(rd.ravel()[idx] - want).max() / dmax))
     dtot = max_rel(dose, ref_total)
     print(f"\n{which}: max |dWET| per beam (cm) {dwet}; beam dose err / Dmax {dbeam}; "
-          f"pass on reference WET {dpass}; plan dose err / Dmax {dtot:.2e}")
+          f"pass on reference WET {dpass}; plan dose err / Dmax {dtot:.2e}; "
+          f"at the worst voxels vs FP64 oracle: this path {dor_mine}, reference {dor_ref}")
     assert dtot <= 1e-3
     assert max(dbeam) <= 1e-3
-    assert max(dpass) <= 2e-4
+    assert max(dpass) <= 1e-3
+    assert max(dor_mine) <= 2e-5
     # FP32 running sum (reference) against FP64 (here) over rays of up to
     # ~700 samples: a few 1e-4 cm; a sample from a wrong cell shows as >= 1e-2
     assert max(dwet) <= 1e-3
