@@ -988,19 +988,32 @@ struct LineSpot {
     float4 a, b, c;
 };
 
-template <int NT, int KCULL>
+// Per-voxel state that changes once per layer lives here rather than in
+// registers (thread t's voxel q at [q][t]), so that the spot loops keep
+// only their own values live.
+template <int NT, int KCULL, bool BEAM_OUT = false, bool DOSE = true>
 struct LineShared {
     static constexpr int kWarps = NT / 32;
     LineSpot spot[NT * KCULL + 8];
     float gsum[NT * KCULL + 8];      // adjoint: per-slot gradient partials
     float w[kLine][NT];              // the beam's 10*WET per voxel (INF: not valid)
     float d[kLine][NT];              // distance to the source per voxel
+    float tot[2][kLine][DOSE ? NT : 1];   // dose: compensated sum over layers and beams
+    float pfh[2][kLine][DOSE ? NT : 1];   // dose: the layer's prefactors Pf, Hf
+    float bsum[BEAM_OUT ? 2 : 1][kLine][BEAM_OUT ? NT : 1];   // each beam's own sum
     float red[kWarps][kRedSlots];
     int wcount[KCULL][kWarps];
     int wcount_h[KCULL][kWarps];
     int lcount[kWarps];
     int lsel[NT];
 };
+
+// Offsets q - 3.5 of a line's voxel pair (2p, 2p + 1) from the line's centre
+// (exact in FP32).
+__device__ __forceinline__ float2 line_off2(int p)
+{
+    return make_float2((float)(2 * p) - 3.5f, (float)(2 * p) - 2.5f);
+}
 
 // Offset q - 3.5 of a line's voxel from the line's centre (exact in FP32).
 __device__ __forceinline__ constexpr float line_off(int q) { return (float)q - 3.5f; }
@@ -1025,7 +1038,8 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                                           const float *__restrict__ mu,
                                           float *__restrict__ dose,
                                           float *__restrict__ beam_dose,
-                                          LineShared<TY * TZ, KCULL> &sh,
+                                          LineShared<TY * TZ, KCULL, BEAM_OUT,
+                                                     MODE == kModeDose> &sh,
                                           unsigned long long *count = nullptr,
                                           const float *__restrict__ wfield = nullptr,
                                           float *__restrict__ grad = nullptr)
@@ -1048,9 +1062,10 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
     unsigned long long n_ex2 = 0, n_eval = 0;
 
-    float tot_s[kLine], tot_c[kLine];
+    if constexpr (MODE == kModeDose) {
 #pragma unroll
-    for (int q = 0; q < kLine; ++q) tot_s[q] = tot_c[q] = 0.0f;
+        for (int q = 0; q < kLine; ++q) sh.tot[0][q][t] = sh.tot[1][q][t] = 0.0f;
+    }
     float wv[kLine];   // adjoint: scale * dObj/dD per voxel
     if constexpr (ADJ) {
         bool anyw = false;
@@ -1127,9 +1142,10 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
             tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
             tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10];
         }
-        float bs_s[kLine], bs_c[kLine];
+        if constexpr (BEAM_OUT) {
 #pragma unroll
-        for (int q = 0; q < kLine; ++q) bs_s[q] = bs_c[q] = 0.0f;
+            for (int q = 0; q < kLine; ++q) sh.bsum[0][q][t] = sh.bsum[1][q][t] = 0.0f;
+        }
 
         for (int l0 = 0; l0 < B.n_layers; l0 += NT) {
             __syncthreads();   // the previous chunk's list and the bounds have been read
@@ -1163,7 +1179,8 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                 const LayerK K =
                     layer_consts(L.r80, B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2, dep,
                                  B.lut_len);
-                float pf[kLine], hf[kLine], PS[kLine], HS[kLine];
+                float pf[kLine], hf[kLine];
+                float2 PS[kLine / 2], HS[kLine / 2];   // voxel pairs (q, q + 1)
                 bool act[kLine];
                 float hmax = -INFINITY, pmax = -INFINITY;
                 // every voxel's parameters without branching (inactive
@@ -1182,22 +1199,33 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                     } else {
                         pf[q] = hf[q] = ps2 = hs2 = 0.0f;
                     }
-                    PS[q] = ps2;
-                    HS[q] = hs2;
+                    if (q & 1) {
+                        PS[q >> 1].y = ps2;
+                        HS[q >> 1].y = hs2;
+                    } else {
+                        PS[q >> 1].x = ps2;
+                        HS[q >> 1].x = hs2;
+                    }
+                    if constexpr (MODE == kModeDose) {
+                        sh.pfh[0][q][t] = pf[q];
+                        sh.pfh[1][q][t] = hf[q];
+                    }
                 }
                 float nhs, nps;
                 block_max2<NT>(hmax, pmax, sh.red, nhs, nps);
                 nhs = -nhs;
                 nps = -nps;
                 // forward: per-voxel sums; adjoint: weighted prefactors
-                float AP[kLine], AH[kLine];
+                float2 AP[kLine / 2], AH[kLine / 2];
 #pragma unroll
-                for (int q = 0; q < kLine; ++q) {
+                for (int p = 0; p < kLine / 2; ++p) {
                     if constexpr (ADJ) {
-                        AP[q] = __fmul_rn(wv[q], pf[q]);
-                        AH[q] = __fmul_rn(wv[q], hf[q]);
+                        AP[p] = make_float2(__fmul_rn(wv[2 * p], pf[2 * p]),
+                                            __fmul_rn(wv[2 * p + 1], pf[2 * p + 1]));
+                        AH[p] = make_float2(__fmul_rn(wv[2 * p], hf[2 * p]),
+                                            __fmul_rn(wv[2 * p + 1], hf[2 * p + 1]));
                     } else {
-                        AP[q] = AH[q] = 0.0f;
+                        AP[p] = AH[p] = make_float2(0.0f, 0.0f);
                     }
                 }
 
@@ -1275,16 +1303,18 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                                     const LineSpot r = sh.spot[c0 + u];
                                     float S0, B1;
                                     line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
-                                    float acc = 0.0f;
+                                    const float2 s0 = f2(S0), b1 = f2(B1), c2 = f2(r.b.z);
+                                    float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-                                    for (int q = 0; q < kLine; ++q) {
-                                        const float o = line_off(q);
-                                        const float S = __fmaf_rn(__fmaf_rn(r.b.z, o, B1), o, S0);
-                                        acc = __fmaf_rn(AH[q], ex2(__fmul_rn(HS[q], S)), acc);
+                                    for (int p = 0; p < kLine / 2; ++p) {
+                                        const float2 o = line_off2(p);
+                                        const float2 S = __ffma2_rn(__ffma2_rn(c2, o, b1), o, s0);
+                                        acc = __ffma2_rn(AH[p], ex2x2(__fmul2_rn(HS[p], S)), acc);
                                         if (two)
-                                            acc = __fmaf_rn(AP[q], ex2(__fmul_rn(PS[q], S)), acc);
+                                            acc = __ffma2_rn(AP[p], ex2x2(__fmul2_rn(PS[p], S)),
+                                                             acc);
                                     }
-                                    v[u] = acc;
+                                    v[u] = acc.x + acc.y;
                                 }
                                 int slot;
                                 const float sum = warp_sum8(v, lane, slot);
@@ -1307,12 +1337,13 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                             const LineSpot r = sh.spot[c];
                             float S0, B1;
                             line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
+                            const float2 s0 = f2(S0), b1 = f2(B1), c2 = f2(r.b.z), w = f2(r.b.w);
 #pragma unroll
-                            for (int q = 0; q < kLine; ++q) {
-                                const float o = line_off(q);
-                                const float S = __fmaf_rn(__fmaf_rn(r.b.z, o, B1), o, S0);
-                                AP[q] = __fmaf_rn(r.b.w, ex2(__fmul_rn(PS[q], S)), AP[q]);
-                                AH[q] = __fmaf_rn(r.b.w, ex2(__fmul_rn(HS[q], S)), AH[q]);
+                            for (int p = 0; p < kLine / 2; ++p) {
+                                const float2 o = line_off2(p);
+                                const float2 S = __ffma2_rn(__ffma2_rn(c2, o, b1), o, s0);
+                                AP[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(PS[p], S)), AP[p]);
+                                AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], S)), AH[p]);
                             }
                         }
                         // halo only
@@ -1321,11 +1352,12 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                             const LineSpot r = sh.spot[c];
                             float S0, B1;
                             line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
+                            const float2 s0 = f2(S0), b1 = f2(B1), c2 = f2(r.b.z), w = f2(r.b.w);
 #pragma unroll
-                            for (int q = 0; q < kLine; ++q) {
-                                const float o = line_off(q);
-                                const float S = __fmaf_rn(__fmaf_rn(r.b.z, o, B1), o, S0);
-                                AH[q] = __fmaf_rn(r.b.w, ex2(__fmul_rn(HS[q], S)), AH[q]);
+                            for (int p = 0; p < kLine / 2; ++p) {
+                                const float2 o = line_off2(p);
+                                const float2 S = __ffma2_rn(__ffma2_rn(c2, o, b1), o, s0);
+                                AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], S)), AH[p]);
                             }
                         }
                     }
@@ -1335,9 +1367,19 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
 #pragma unroll
                     for (int q = 0; q < kLine; ++q) {
                         if (act[q]) {
-                            const float ld = fmaf(pf[q], AP[q], hf[q] * AH[q]);
-                            if (BEAM_OUT) neumaier(bs_s[q], bs_c[q], ld);
-                            neumaier(tot_s[q], tot_c[q], ld);
+                            const float ap = (q & 1) ? AP[q >> 1].y : AP[q >> 1].x;
+                            const float ah = (q & 1) ? AH[q >> 1].y : AH[q >> 1].x;
+                            const float ld = fmaf(sh.pfh[0][q][t], ap, sh.pfh[1][q][t] * ah);
+                            if constexpr (BEAM_OUT) {
+                                float bs = sh.bsum[0][q][t], bc = sh.bsum[1][q][t];
+                                neumaier(bs, bc, ld);
+                                sh.bsum[0][q][t] = bs;
+                                sh.bsum[1][q][t] = bc;
+                            }
+                            float ts = sh.tot[0][q][t], tc = sh.tot[1][q][t];
+                            neumaier(ts, tc, ld);
+                            sh.tot[0][q][t] = ts;
+                            sh.tot[1][q][t] = tc;
                         }
                     }
                 }
@@ -1346,7 +1388,8 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
         if (BEAM_OUT) {
 #pragma unroll
             for (int q = 0; q < kLine; ++q)
-                if (q < nvalid) beam_dose[b * V + vbase + q] = (bs_s[q] + bs_c[q]) * A.scale;
+                if (q < nvalid)
+                    beam_dose[b * V + vbase + q] = (sh.bsum[0][q][t] + sh.bsum[1][q][t]) * A.scale;
         }
         __syncthreads();  // sh.w, sh.d and sh.red are rewritten by the next beam
     }
@@ -1358,15 +1401,15 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
     } else if constexpr (MODE == kModeDose) {
 #pragma unroll
         for (int q = 0; q < kLine; ++q)
-            if (q < nvalid) dose[vbase + q] = (tot_s[q] + tot_c[q]) * A.scale;
+            if (q < nvalid) dose[vbase + q] = (sh.tot[0][q][t] + sh.tot[1][q][t]) * A.scale;
     }
 }
 
 // Resident blocks per SM the line-tile kernels are compiled for (their
-// register budget): 16 of 32 threads, 8 of 64, 4 of 128.
+// register budget): 20 of 32 threads, 10 of 64, 5 of 128.
 template <int NT> constexpr int line_min_blocks()
 {
-    return NT == 32 ? 16 : (NT == 64 ? 8 : 4);
+    return NT == 32 ? 20 : (NT == 64 ? 10 : 5);
 }
 
 // Tile coordinates of a linear block index over the grid's 8 x TY x TZ tiles.
@@ -1388,21 +1431,21 @@ k_dose_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
             const float *__restrict__ mu, float *__restrict__ dose,
             float *__restrict__ beam_dose)
 {
-    __shared__ LineShared<TY * TZ, KCULL> sh;
+    __shared__ LineShared<TY * TZ, KCULL, BEAM_OUT> sh;
     int tx, ty, tz;
     line_tile_coords<TY, TZ>(A.g, blockIdx.x, tx, ty, tz);
     line_tile<TY, TZ, KCULL, BEAM_OUT>(A, tx, ty, tz, wet, layers, geo, mu, dose, beam_dose, sh);
 }
 
 // Line-tile shape of the default forward, its count and its adjoint.
-constexpr int kLineTY = 8, kLineTZ = 8, kLineCull = 4;
+constexpr int kLineTY = 8, kLineTZ = 8, kLineCull = 2;
 
 __global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ>())
 k_dose_count_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                   const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
                   unsigned long long *count)
 {
-    __shared__ LineShared<kLineTY * kLineTZ, kLineCull> sh;
+    __shared__ LineShared<kLineTY * kLineTZ, kLineCull, false, false> sh;
     int tx, ty, tz;
     line_tile_coords<kLineTY, kLineTZ>(A.g, blockIdx.x, tx, ty, tz);
     line_tile<kLineTY, kLineTZ, kLineCull, false, kModeCount>(A, tx, ty, tz, wet, layers, geo,
@@ -1415,7 +1458,7 @@ k_adjoint_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet
                const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
                const float *__restrict__ wfield, float *__restrict__ grad)
 {
-    __shared__ LineShared<kLineTY * kLineTZ, kLineCull> sh;
+    __shared__ LineShared<kLineTY * kLineTZ, kLineCull, false, false> sh;
     int tx, ty, tz;
     line_tile_coords<kLineTY, kLineTZ>(A.g, blockIdx.x, tx, ty, tz);
     line_tile<kLineTY, kLineTZ, kLineCull, false, kModeAdjoint>(A, tx, ty, tz, wet, layers, geo,

@@ -151,11 +151,11 @@ def tune_plan(dp, reps: int = 3, use_cache: bool = True) -> int:
 def max_blocks_per_sm(name: str) -> int:
     """Resident blocks per SM a kernel shape is compiled for.  8x8x8
     family: 6 for 128 threads with one spot per thread per round, 5 for the
-    other 128-thread shapes, 3 for 256.  Line family: 16 of 32 threads, 8 of
-    64, 4 of 128."""
+    other 128-thread shapes, 3 for 256.  Line family: 20 of 32 threads, 10
+    of 64, 5 of 128."""
     fam, _, nt, k = shape_of(name)
     if fam == "l":
-        return {32: 16, 64: 8, 128: 4}[nt]
+        return {32: 20, 64: 10, 128: 5}[nt]
     if nt != 128:
         return 3
     return 6 if k == 1 else 5

@@ -29,7 +29,7 @@ def test_variants_and_batch_candidates():
     assert autotune.round_size("l8x8x8_c4") == 256 == autotune.round_size("t128_v4_c2")
     assert not autotune.same_decisions("l8x8x8_c4", "t128_v4_c2")
     assert autotune.same_decisions("t128_v4_c2", "t256_v2_c1")
-    assert autotune.max_blocks_per_sm("l8x8x4_c4") == 16
+    assert autotune.max_blocks_per_sm("l8x8x4_c4") == 20
     assert autotune.batch_shape("l8x4x8_c4") and not autotune.batch_shape("l8x8x16_c2")
     assert {names[v] for v, _ in cands} == {n for n in names if autotune.batch_shape(n)}
 
