@@ -64,6 +64,7 @@ def load(port32: bool = False):
     lib.ob_beam_setup.argtypes = [ctypes.c_double] * 4 + [vp, vp, ctypes.POINTER(OBeam)]
     lib.ob_smooth_dirs.argtypes = [vp, vp]
     lib.ob_set_smooth_dirs.argtypes = [vp, vp]
+    lib.ob_set_fuse.argtypes = [vp]
     lib.ob_raytrace.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp, i64, vp]
     lib.ob_raytrace.restype = i
     lib.ob_smooth.argtypes = [vp, ctypes.POINTER(OGrid), ctypes.POINTER(OBeam), vp, i64, vp]
@@ -106,6 +107,19 @@ def set_smooth_dirs(c=None, s=None):
             cc = np.ascontiguousarray(c, np.float32)
             ss = np.ascontiguousarray(s, np.float32)
             lib.ob_set_smooth_dirs(_p(cc), _p(ss))
+
+
+def set_fuse(modes=None):
+    """Fused multiply-adds in the FP32 rotations and smoothing samples (see
+    ob_set_fuse): nine modes, or None for none."""
+    for port32 in (False, True):
+        lib = load(port32)
+        if modes is None:
+            lib.ob_set_fuse(None)
+        else:
+            m = np.ascontiguousarray(modes, np.int32)
+            assert m.shape == (9,)
+            lib.ob_set_fuse(_p(m))
 
 
 def smooth_dirs():

@@ -153,17 +153,37 @@ static inline void vox_mm(const ob_grid *g, const ob_beam *b, int i, int j,
     p[2] = (float)k * g->s - b->iso[2];
 }
 
+/* Which products of the FP32 rotation expressions are fused into a
+ * multiply-add, as a compiler that contracts a*b + c*d may do: per entry 0
+ * (unfused), 1 (fma of the first product with the rounded second), 2 (of
+ * the second with the rounded first).  Entries: image_to_head xt, zt, xg,
+ * yg (0-3), head_to_image xg, yg, xt, zt (4-7), and the smoothing sample
+ * h + dr * direction (8: 0 or 1).  Default all 0. */
+static int g_fuse[9];
+
+void ob_set_fuse(const int *m)
+{
+    for (int i = 0; i < 9; i++) g_fuse[i] = m ? m[i] : 0;
+}
+
+static inline float ab_cd(float a, float b, float c, float d, int mode)
+{
+    if (mode == 1) return fmaf(a, b, c * d);
+    if (mode == 2) return fmaf(c, d, a * b);
+    return a * b + c * d;
+}
+
 /* Image -> beam's-eye (head) frame, FP32, fixed order (CudaClasses.cu:65-95). */
 static inline void image_to_head_f(const ob_beam *b, const float *p, float *h)
 {
     float sx = -b->sinta, cx = b->costa;
-    float xt = p[0] * cx + p[2] * sx;
+    float xt = ab_cd(p[0], cx, p[2], sx, g_fuse[0]);
     float yt = p[1];
-    float zt = -p[0] * sx + p[2] * cx;
+    float zt = ab_cd(-p[0], sx, p[2], cx, g_fuse[1]);
     sx = -b->singa;
     cx = b->cosga;
-    float xg = xt * cx - yt * sx;
-    float yg = xt * sx + yt * cx;
+    float xg = ab_cd(xt, cx, -yt, sx, g_fuse[2]);
+    float yg = ab_cd(xt, sx, yt, cx, g_fuse[3]);
     h[0] = -xg;
     h[1] = zt;
     h[2] = yg;
@@ -174,14 +194,14 @@ static inline void head_to_image_f(const ob_beam *b, const float *h, float *p)
 {
     float xz = -h[0], yz = h[2], zz = h[1];
     float sx = b->singa, cx = b->cosga;
-    float xg = xz * cx - yz * sx;
-    float yg = xz * sx + yz * cx;
+    float xg = ab_cd(xz, cx, -yz, sx, g_fuse[4]);
+    float yg = ab_cd(xz, sx, yz, cx, g_fuse[5]);
     float zg = zz;
     sx = b->sinta;
     cx = b->costa;
-    p[0] = xg * cx + zg * sx;
+    p[0] = ab_cd(xg, cx, zg, sx, g_fuse[6]);
     p[1] = yg;
-    p[2] = -xg * sx + zg * cx;
+    p[2] = ab_cd(-xg, sx, zg, cx, g_fuse[7]);
 }
 
 /* Image -> head frame in FP64 (continuous use only). */
@@ -326,8 +346,8 @@ static int smooth_samples(const float *raw, const ob_grid *g, const ob_beam *b,
         float dr = 1.0f;
         while (dr < center * 10.0f && dr < 10.0f) {
             float hc[3], pc[3];
-            hc[0] = h[0] + dr * dc[d];
-            hc[1] = h[1] + dr * ds[d];
+            hc[0] = g_fuse[8] ? fmaf(dr, dc[d], h[0]) : h[0] + dr * dc[d];
+            hc[1] = g_fuse[8] ? fmaf(dr, ds[d], h[1]) : h[1] + dr * ds[d];
             hc[2] = h[2];
             head_to_image_f(b, hc, pc);
             int ii = (int)roundf((pc[0] + b->iso[0]) / g->s);
@@ -396,8 +416,8 @@ void ob_smooth_choices(const ob_grid *g, const ob_beam *b, int32_t *out)
             float dr = 1.0f;
             for (int r = 0; r < 9; r++) {
                 float hc[3], pc[3];
-                hc[0] = h[0] + dr * dc[d];
-                hc[1] = h[1] + dr * ds[d];
+                hc[0] = g_fuse[8] ? fmaf(dr, dc[d], h[0]) : h[0] + dr * dc[d];
+                hc[1] = g_fuse[8] ? fmaf(dr, ds[d], h[1]) : h[1] + dr * ds[d];
                 hc[2] = h[2];
                 head_to_image_f(b, hc, pc);
                 int32_t *o = out + ((v * 6 + d) * 9 + r) * 3;
