@@ -25,13 +25,16 @@ struct BeamGeomSet {
     PbBeamGeom b[PB_MAX_BEAMS];
 };
 
+// Voxel index -> mm relative to the isocentre, i*s - iso: the reference's
+// expression (CudaClasses.cuh:106-110) as its compiler contracts it, one
+// fused multiply-add.
 __device__ __forceinline__ void vox_mm(const PbBeamGeom &b, float s, int i,
                                        int j, int k, float &x, float &y,
                                        float &z)
 {
-    x = __fsub_rn(__fmul_rn((float)i, s), b.iso[0]);
-    y = __fsub_rn(__fmul_rn((float)j, s), b.iso[1]);
-    z = __fsub_rn(__fmul_rn((float)k, s), b.iso[2]);
+    x = __fmaf_rn((float)i, s, -b.iso[0]);
+    y = __fmaf_rn((float)j, s, -b.iso[1]);
+    z = __fmaf_rn((float)k, s, -b.iso[2]);
 }
 
 // Image frame -> beam's-eye (head) frame: couch about y, then gantry about
@@ -67,6 +70,45 @@ __device__ __forceinline__ void head_to_image(const PbBeamGeom &b, float hx,
     px = __fadd_rn(__fmul_rn(xg, cx), __fmul_rn(zg, sx));
     py = yg;
     pz = __fadd_rn(__fmul_rn(-xg, sx), __fmul_rn(zg, cx));
+}
+
+// The two rotations as the reference's compiled code evaluates them
+// (CudaClasses.cu:65-126): its compiler contracts each a*b + c*d into one
+// fused multiply-add and a rounded product -- in the image -> head rotation
+// the second product is fused, in the head -> image rotation the first.
+// The smoothing's half-voxel ties depend on these last bits (established
+// against the reference module's output on oblique beams).
+__device__ __forceinline__ void image_to_head_ref(const PbBeamGeom &b, float px,
+                                                  float py, float pz, float &hx,
+                                                  float &hy, float &hz)
+{
+    float sx = -b.sinta, cx = b.costa;
+    const float xt = __fmaf_rn(pz, sx, __fmul_rn(px, cx));
+    const float yt = py;
+    const float zt = __fmaf_rn(pz, cx, __fmul_rn(-px, sx));
+    sx = -b.singa;
+    cx = b.cosga;
+    const float xg = __fmaf_rn(-yt, sx, __fmul_rn(xt, cx));
+    const float yg = __fmaf_rn(yt, cx, __fmul_rn(xt, sx));
+    hx = -xg;
+    hy = zt;
+    hz = yg;
+}
+
+__device__ __forceinline__ void head_to_image_ref(const PbBeamGeom &b, float hx,
+                                                  float hy, float hz, float &px,
+                                                  float &py, float &pz)
+{
+    const float xz = -hx, yz = hz, zz = hy;
+    float sx = b.singa, cx = b.cosga;
+    const float xg = __fmaf_rn(xz, cx, __fmul_rn(-yz, sx));
+    const float yg = __fmaf_rn(xz, sx, __fmul_rn(yz, cx));
+    const float zg = zz;
+    sx = b.sinta;
+    cx = b.costa;
+    px = __fmaf_rn(xg, cx, __fmul_rn(zg, sx));
+    py = yg;
+    pz = __fmaf_rn(-xg, sx, __fmul_rn(zg, cx));
 }
 
 // Unit vector from a voxel toward the source: FP32 difference, FP64 norm,

@@ -1827,17 +1827,19 @@ struct DoseVariant {
     const char *name;
 };
 static const DoseVariant kDoseVariants[] = {
+    {1, 8, 8, 64, 2, true, "l8x8x8_c2"},    {1, 8, 8, 64, 4, true, "l8x8x8_c4"},
+    {1, 8, 4, 32, 4, true, "l8x8x4_c4"},    {1, 4, 8, 32, 4, true, "l8x4x8_c4"},
+    {1, 16, 8, 128, 2, false, "l8x16x8_c2"}, {1, 8, 16, 128, 2, false, "l8x8x16_c2"},
     {0, 8, 8, 128, 1, true, "t128_v4_c1"},  {0, 8, 8, 128, 2, true, "t128_v4_c2"},
     {0, 8, 8, 128, 4, true, "t128_v4_c4"},  {0, 8, 8, 256, 1, true, "t256_v2_c1"},
     {0, 8, 8, 128, 3, true, "t128_v4_c3"},
-    {1, 8, 8, 64, 4, true, "l8x8x8_c4"},    {1, 8, 8, 64, 2, true, "l8x8x8_c2"},
-    {1, 8, 4, 32, 4, true, "l8x8x4_c4"},    {1, 4, 8, 32, 4, true, "l8x4x8_c4"},
-    {1, 16, 8, 128, 2, false, "l8x16x8_c2"}, {1, 8, 16, 128, 2, false, "l8x8x16_c2"},
 };
 constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
 
-// The shape pb_dose, pb_dose_adjoint and pb_count_evaluated use.
+// The shape pb_dose and pb_count_evaluated use, and the family of
+// pb_dose_adjoint's kernel (true: line tiles).
 constexpr int kDefaultDoseVariant = 0;
+constexpr bool kAdjointLine = false;
 
 int dose_variant_default() { return kDefaultDoseVariant; }
 int dose_variant_count() { return kNumDoseVariants; }
@@ -1900,17 +1902,17 @@ PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
         return check_launch("k_dose");
     }
     switch (variant) {
-    case 1: launch_dose_t<128, 4, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
-    case 2: launch_dose_t<128, 4, 4>(A, tiles, wet, layers, g4, mu, dose, st); break;
-    case 3: launch_dose_t<256, 2, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
-    case 4: launch_dose_t<128, 4, 3>(A, tiles, wet, layers, g4, mu, dose, st); break;
-    case 5: launch_line_t<8, 8, 4>(A, wet, layers, g4, mu, dose, st); break;
-    case 6: launch_line_t<8, 8, 2>(A, wet, layers, g4, mu, dose, st); break;
-    case 7: launch_line_t<8, 4, 4>(A, wet, layers, g4, mu, dose, st); break;
-    case 8: launch_line_t<4, 8, 4>(A, wet, layers, g4, mu, dose, st); break;
-    case 9: launch_line_t<16, 8, 2>(A, wet, layers, g4, mu, dose, st); break;
-    case 10: launch_line_t<8, 16, 2>(A, wet, layers, g4, mu, dose, st); break;
-    default: launch_dose_t<128, 4, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 1: launch_line_t<8, 8, 4>(A, wet, layers, g4, mu, dose, st); break;
+    case 2: launch_line_t<8, 4, 4>(A, wet, layers, g4, mu, dose, st); break;
+    case 3: launch_line_t<4, 8, 4>(A, wet, layers, g4, mu, dose, st); break;
+    case 4: launch_line_t<16, 8, 2>(A, wet, layers, g4, mu, dose, st); break;
+    case 5: launch_line_t<8, 16, 2>(A, wet, layers, g4, mu, dose, st); break;
+    case 6: launch_dose_t<128, 4, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 7: launch_dose_t<128, 4, 2>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 8: launch_dose_t<128, 4, 4>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 9: launch_dose_t<256, 2, 1>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    case 10: launch_dose_t<128, 4, 3>(A, tiles, wet, layers, g4, mu, dose, st); break;
+    default: launch_line_t<8, 8, 2>(A, wet, layers, g4, mu, dose, st); break;
     }
     return check_launch("k_dose");
 }
@@ -1947,15 +1949,15 @@ PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items
     if (s != PB_OK) return s;
     const BatchDose *P = static_cast<const BatchDose *>(plans_dev);
     switch (variant) {
-    case 1: k_dose_batch<128, 4, 2><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 2: k_dose_batch<128, 4, 4><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 3: k_dose_batch<256, 2, 1><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 4: k_dose_batch<128, 4, 3><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 5: k_dose_batch_line<8, 8, 4><<<blocks, 64, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 6: k_dose_batch_line<8, 8, 2><<<blocks, 64, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 7: k_dose_batch_line<8, 4, 4><<<blocks, 32, 0, st>>>(P, n_plans, n_items, counter); break;
-    case 8: k_dose_batch_line<4, 8, 4><<<blocks, 32, 0, st>>>(P, n_plans, n_items, counter); break;
-    default: k_dose_batch<128, 4, 1><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 1: k_dose_batch_line<8, 8, 4><<<blocks, 64, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 2: k_dose_batch_line<8, 4, 4><<<blocks, 32, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 3: k_dose_batch_line<4, 8, 4><<<blocks, 32, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 6: k_dose_batch<128, 4, 1><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 7: k_dose_batch<128, 4, 2><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 8: k_dose_batch<128, 4, 4><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 9: k_dose_batch<256, 2, 1><<<blocks, 256, 0, st>>>(P, n_plans, n_items, counter); break;
+    case 10: k_dose_batch<128, 4, 3><<<blocks, 128, 0, st>>>(P, n_plans, n_items, counter); break;
+    default: k_dose_batch_line<8, 8, 2><<<blocks, 64, 0, st>>>(P, n_plans, n_items, counter); break;
     }
     return check_launch("k_dose_batch");
 }
@@ -1982,7 +1984,7 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
     if (s != PB_OK) return s;
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
-    if (variant_line(variant)) {
+    if (variant < 0 ? kAdjointLine : variant_line(variant)) {
         k_adjoint_line<<<line_tiles(g, kLineTY, kLineTZ), kLineTY * kLineTZ, 0, st>>>(
             A, wet, layers, g4, w, grad);
         return check_launch("k_adjoint_line");

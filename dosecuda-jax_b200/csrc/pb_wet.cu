@@ -497,23 +497,24 @@ __device__ __forceinline__ void exact_steps(const PbBeamGeom &B, const SmoothBea
                                             float hy, float hz, float fi, float fj, float fk,
                                             int dd, int r, int axes, int &ui, int &uj, int &uk)
 {
-    // dr * cos, dr * sin in FP32 (dr = r + 1 mm is exact), the reference's products
+    // h + dr * (cos, sin), dr = r + 1 mm, each one fused multiply-add as the
+    // reference's compiled code forms it (IMPTClasses.cu:180-181)
     const float dr = (float)(r + 1);
-    const float hxs = __fadd_rn(hx, __fmul_rn(dr, dc[dd]));
-    const float hys = __fadd_rn(hy, __fmul_rn(dr, ds[dd]));
+    const float hxs = __fmaf_rn(dr, dc[dd], hx);
+    const float hys = __fmaf_rn(dr, ds[dd], hy);
     float qx, qy, qz;
     if (axes & 1) {
-        head_to_image(B, hxs, hys, hz, qx, qy, qz);
+        head_to_image_ref(B, hxs, hys, hz, qx, qy, qz);
         ui = round_up<POW2>(__fadd_rn(qx, B.iso[0]), __fadd_rn(fi, T.hh[dd][r][0]), s,
                             T.inv_s);
     }
     if (axes & 2) {
-        head_to_image(B, hxs, hys, hz, qx, qy, qz);
+        head_to_image_ref(B, hxs, hys, hz, qx, qy, qz);
         uj = round_up<POW2>(__fadd_rn(qy, B.iso[1]), __fadd_rn(fj, T.hh[dd][r][1]), s,
                             T.inv_s);
     }
     if (axes & 4) {
-        head_to_image(B, hxs, hys, hz, qx, qy, qz);
+        head_to_image_ref(B, hxs, hys, hz, qx, qy, qz);
         uk = round_up<POW2>(__fadd_rn(qz, B.iso[2]), __fadd_rn(fk, T.hh[dd][r][2]), s,
                             T.inv_s);
     }
@@ -542,7 +543,7 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
     const PbBeamGeom B = Bp;   // the rotation and isocentre in registers
     float px, py, pz, hx, hy, hz;
     vox_mm(B, g.spacing, i, j, k, px, py, pz);
-    image_to_head(B, px, py, pz, hx, hy, hz);
+    image_to_head_ref(B, px, py, pz, hx, hy, hz);
     const float s = g.spacing;
     const float fi = (float)i, fj = (float)j, fk = (float)k;
     float sum = center;

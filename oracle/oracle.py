@@ -111,7 +111,7 @@ def set_smooth_dirs(c=None, s=None):
 
 def set_fuse(modes=None):
     """Fused multiply-adds in the FP32 rotations and smoothing samples (see
-    ob_set_fuse): nine modes, or None for none."""
+    ob_set_fuse): nine modes, or None for the reference's own pattern."""
     for port32 in (False, True):
         lib = load(port32)
         if modes is None:

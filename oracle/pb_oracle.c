@@ -145,25 +145,32 @@ void ob_smooth_dirs(float *c, float *s)
     }
 }
 
+/* i*s - iso as one fused multiply-add, as the reference's compiler
+ * contracts CudaClasses.cuh:106-110. */
 static inline void vox_mm(const ob_grid *g, const ob_beam *b, int i, int j,
                           int k, float *p)
 {
-    p[0] = (float)i * g->s - b->iso[0];
-    p[1] = (float)j * g->s - b->iso[1];
-    p[2] = (float)k * g->s - b->iso[2];
+    p[0] = fmaf((float)i, g->s, -b->iso[0]);
+    p[1] = fmaf((float)j, g->s, -b->iso[1]);
+    p[2] = fmaf((float)k, g->s, -b->iso[2]);
 }
 
 /* Which products of the FP32 rotation expressions are fused into a
- * multiply-add, as a compiler that contracts a*b + c*d may do: per entry 0
- * (unfused), 1 (fma of the first product with the rounded second), 2 (of
+ * multiply-add, as the reference's compiler contracts a*b + c*d: per entry
+ * 0 (unfused), 1 (fma of the first product with the rounded second), 2 (of
  * the second with the rounded first).  Entries: image_to_head xt, zt, xg,
  * yg (0-3), head_to_image xg, yg, xt, zt (4-7), and the smoothing sample
- * h + dr * direction (8: 0 or 1).  Default all 0. */
-static int g_fuse[9];
+ * h + dr * direction (8: 0 or 1).  Default: the reference's compiled
+ * arithmetic (CudaClasses.cu:65-126, IMPTClasses.cu:180-181) -- image ->
+ * head fuses the second product, head -> image the first, the sample is
+ * one multiply-add -- established against the reference module's smoothed
+ * WET on oblique beams. */
+static const int k_fuse_ref[9] = {2, 2, 2, 2, 1, 1, 1, 1, 1};
+static int g_fuse[9] = {2, 2, 2, 2, 1, 1, 1, 1, 1};
 
 void ob_set_fuse(const int *m)
 {
-    for (int i = 0; i < 9; i++) g_fuse[i] = m ? m[i] : 0;
+    for (int i = 0; i < 9; i++) g_fuse[i] = m ? m[i] : k_fuse_ref[i];
 }
 
 static inline float ab_cd(float a, float b, float c, float d, int mode)
