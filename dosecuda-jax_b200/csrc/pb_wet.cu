@@ -371,16 +371,7 @@ struct SmoothBeam {
     int margin[3];            // interior: margin_a <= i_a <= n_a - 1 - margin_a
     float inv_s;              // 1 / spacing in FP32
     int pow2;                 // the spacing is a power of two: inv_s is exact
-    int nflag;                // (direction, radius) pairs with a flagged axis
-    unsigned char flist[56];  // those pairs, dd * 9 + r, in the reference's order
-    signed char fslot[6][9];  // slot of (dd, r) in flist, -1 when none of its axes is
-    signed char pad_[2];
 };
-
-// Flagged (direction, radius) pairs whose per-voxel index steps the
-// interior smoothing path keeps in shared memory; beams with more take the
-// general interior path.
-constexpr int kMaxFlag = 32;
 
 struct SmoothSet {
     SmoothBeam b[PB_MAX_BEAMS];
@@ -434,14 +425,6 @@ static void smooth_table(const PbGrid &g, const PbBeamGeom &B, const float *c, c
         }
         T.tmask[dd] = m;
     }
-    int nf = 0;
-    for (int dd = 0; dd < 6; ++dd)
-        for (int r = 0; r < 9; ++r) {
-            const bool any = (T.tmask[dd] >> (3 * r)) & 7u;
-            T.fslot[dd][r] = any ? (signed char)nf : (signed char)-1;
-            if (any) T.flist[nf++] = (unsigned char)(dd * 9 + r);
-        }
-    T.nflag = nf;
 }
 
 static void smooth_set(const PbGrid &g, const PbBeamGeom *beams, int n_beams, SmoothSet &o)
@@ -532,7 +515,7 @@ template <bool POW2>
 __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const PbGrid &g,
                                               const PbBeamGeom &Bp, const SmoothBeam &T,
                                               const float *dc, const float *ds, int i, int j,
-                                              int k, int *adj = nullptr, int nt = 0)
+                                              int k)
 {
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
     const float center = R[v];
@@ -559,35 +542,8 @@ __device__ __forceinline__ float smooth_voxel(const float *__restrict__ R, const
         // 32-bit.  A sample past the voxel's count is loaded and not added,
         // without a branch.
         const int vi = (int)v, sy = g.nx, sz = g.nx * g.ny;
-        if (adj && T.nflag <= kMaxFlag) {
-            // The flagged pairs' index steps first, in a loop over the
-            // beam's list (uniform), each kept in this thread's column of
-            // adj; then the 54 samples fully unrolled, each a table offset
-            // plus, for a flagged pair, its step: the same samples summed in
-            // the same order as the loop below.
-            for (int f = 0; f < T.nflag; ++f) {
-                const int n = T.flist[f], dd = n / 9, r = n - 9 * dd;
-                const int axes = (T.tmask[dd] >> (3 * r)) & 7u;
-                int ui = 0, uj = 0, uk = 0;
-                exact_steps<POW2>(B, T, s, dc, ds, hx, hy, hz, fi, fj, fk, dd, r, axes, ui, uj,
-                                  uk);
-                adj[f * nt] = ui + sy * uj + sz * uk;
-            }
-#pragma unroll
-            for (int dd = 0; dd < 6; ++dd) {
-#pragma unroll
-                for (int r = 0; r < 9; ++r) {
-                    int idx = vi + T.off[dd][r];
-                    const int f = T.fslot[dd][r];
-                    if (f >= 0) idx += adj[f * nt];
-                    const float x = __ldg(R + idx);
-                    sum = r < nr ? __fadd_rn(sum, x) : sum;
-                }
-            }
-            return __fdiv_rn(sum, (float)(6 * nr + 1));
-        }
-        // radii unrolled by three: fully unrolled, this loop (ties formed
-        // inline) no longer fits the instruction cache
+        // Radii unrolled by three: fully unrolled, the loop no longer fits
+        // the instruction cache.
         for (int dd = 0; dd < 6; ++dd) {
             const unsigned tm = T.tmask[dd];   // the same for the whole beam
 #pragma unroll 3
@@ -641,7 +597,6 @@ __global__ void __launch_bounds__(128, POW2 ? 12 : 1)
 k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGeomSet bs,
          const __grid_constant__ SmoothSet st, int zbricks, float *__restrict__ wet)
 {
-    __shared__ int s_adj[kMaxFlag * 128];
     __shared__ float s_dc[6], s_ds[6];
     const int tid = threadIdx.x + 8 * (threadIdx.y + 4 * threadIdx.z);
     if (tid < 6) smooth_dir_dev(tid, s_dc[tid], s_ds[tid]);
@@ -653,8 +608,7 @@ k_smooth(const float *__restrict__ raw, PbGrid g, const __grid_constant__ BeamGe
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     const int64_t v = i + (int64_t)g.nx * (j + (int64_t)g.ny * k);
-    wet[b * V + v] = smooth_voxel<POW2>(raw + b * V, g, bs.b[b], st.b[b], s_dc, s_ds, i, j, k,
-                                        s_adj + tid, 128);
+    wet[b * V + v] = smooth_voxel<POW2>(raw + b * V, g, bs.b[b], st.b[b], s_dc, s_ds, i, j, k);
 }
 
 // One (plan, beam) of a batched WET pass.
@@ -715,7 +669,6 @@ k_smooth_batch(const BatchWet *__restrict__ items, int n_items)
 {
     static_assert(sizeof(SmoothBeam) % 4 == 0, "the table is copied as words");
     __shared__ SmoothBeam sm;
-    __shared__ int s_adj[kMaxFlag * 128];
     __shared__ float s_dc[6], s_ds[6];
     if (threadIdx.x < 6) smooth_dir_dev(threadIdx.x, s_dc[threadIdx.x], s_ds[threadIdx.x]);
     const BatchWet &W = items[find_wet_item(items, n_items, blockIdx.x)];
@@ -728,10 +681,8 @@ k_smooth_batch(const BatchWet *__restrict__ items, int n_items)
     int i, j, k;
     if (!brick_voxel(W, blockIdx.x, i, j, k)) return;
     float *out = W.wet + i + (int64_t)W.g.nx * (j + (int64_t)W.g.ny * k);
-    *out = sm.pow2 ? smooth_voxel<true>(W.raw, W.g, W.geom, sm, s_dc, s_ds, i, j, k,
-                                        s_adj + threadIdx.x, 128)
-                   : smooth_voxel<false>(W.raw, W.g, W.geom, sm, s_dc, s_ds, i, j, k,
-                                         s_adj + threadIdx.x, 128);
+    *out = sm.pow2 ? smooth_voxel<true>(W.raw, W.g, W.geom, sm, s_dc, s_ds, i, j, k)
+                   : smooth_voxel<false>(W.raw, W.g, W.geom, sm, s_dc, s_ds, i, j, k);
 }
 
 __device__ float g_smooth_dirs[12];
