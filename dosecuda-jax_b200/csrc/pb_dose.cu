@@ -1839,7 +1839,7 @@ constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]
 // The shape pb_dose and pb_count_evaluated use, and the family of
 // pb_dose_adjoint's kernel (true: line tiles).
 constexpr int kDefaultDoseVariant = 0;
-constexpr bool kAdjointLine = false;
+constexpr bool kAdjointLine = true;
 
 int dose_variant_default() { return kDefaultDoseVariant; }
 int dose_variant_count() { return kNumDoseVariants; }

@@ -87,9 +87,9 @@ def test_adjoint_families_agree():
     g = {f: dp.adjoint(w, variant=v).clone() for f, v in fams.items()}
     m = float(g["t"].abs().max())
     assert m > 0 and float((g["l"] - g["t"]).abs().max()) <= 1e-5 * m
-    # the default adjoint is one of them (its cross-tile sums are float
-    # atomics, so only to rounding)
-    assert float((dp.adjoint(w) - g["t"]).abs().max()) <= 1e-5 * m
+    # the default adjoint is the line family's (its cross-tile sums are
+    # float atomics, so only to rounding)
+    assert float((dp.adjoint(w) - g["l"]).abs().max()) <= 1e-5 * m
 
 
 def test_batch_variants_and_grids_agree(cases):
