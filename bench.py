@@ -64,7 +64,16 @@ L2_NOTE = "flushed (256 MiB write) between timed iterations"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu captures of
 # this workload (seed 3, texture WET) on the kernels as built now; the command
 # and the figures are in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md
-NCU_TRAFFIC = {"k_dose": None, "k_adjoint_tile": None}
+NCU_TRAFFIC = {"k_dose_line": None, "k_adjoint_line": None}
+
+
+def kernel_names():
+    """Names of the forward and adjoint kernels the default shape launches."""
+    from dosecuda_b200 import _lib, autotune
+    name = _lib.lib.pb_dose_variant_name(autotune.default_variant()).decode()
+    if autotune.shape_of(name)[0] == "l":
+        return "k_dose_line", "k_adjoint_line"
+    return "k_dose", "k_adjoint_tile"
 
 
 def _peaks():
@@ -369,14 +378,14 @@ def run_mine(args, world, rank, local):
                          (3 if args.mode == "grad" else 0)) * args.steps,
         "clocks": clk.summary(),
     }
-    line.update(rooflines(dp, kms, V, E, dev))
+    line.update(rooflines(dp, kms, V, E, dev, resid))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case, dp, E)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def rooflines(dp, kms, V, E, dev) -> dict:
+def rooflines(dp, kms, V, E, dev, adjoint_field=None) -> dict:
     """Roofline lines of every kernel group over 1 ms in the step.
 
     HBM: algorithmic bytes per launch (each input read once, each output
@@ -410,20 +419,19 @@ def rooflines(dp, kms, V, E, dev) -> dict:
     # and its weight, the LUT rows
     bytes_dose = 4 * V * (B + 1) + 36 * S + lut
     n_ex2, n_eval = dp.count_evaluated()
-    out = {"roofline": hbm_line("k_dose (forward pencil-beam sum)", bytes_dose, kms["dose"],
-                                NCU_TRAFFIC["k_dose"]),
-           "compute_roofline": sfu_line("k_dose", n_ex2, n_eval, kms["dose"])}
+    k_dose, k_adj = kernel_names()
+    out = {"roofline": hbm_line(f"{k_dose} (forward pencil-beam sum)", bytes_dose, kms["dose"],
+                                NCU_TRAFFIC.get(k_dose)),
+           "compute_roofline": sfu_line(k_dose, n_ex2, n_eval, kms["dose"])}
     lines = {}
     if kms.get("adjoint"):
-        # k_adjoint_tile: WET of every beam and dObj/dD read, per spot 32 B of
+        # adjoint: WET of every beam and dObj/dD read, per spot 32 B of
         # geometry and its gradient written, the LUT rows
         bytes_adj = 4 * V * (B + 1) + 36 * S + lut
-        lines["adjoint"] = [hbm_line("k_adjoint_tile", bytes_adj, kms["adjoint"],
-                                     NCU_TRAFFIC["k_adjoint_tile"])]
-        counts = getattr(dp, "count_evaluated_adjoint", None)
-        if counts is not None and getattr(dp, "_last_adjoint_field", None) is not None:
-            a_ex2, a_eval = counts(dp._last_adjoint_field)
-            lines["adjoint"].append(sfu_line("k_adjoint_tile", a_ex2, a_eval, kms["adjoint"]))
+        lines["adjoint"] = [hbm_line(k_adj, bytes_adj, kms["adjoint"], NCU_TRAFFIC.get(k_adj))]
+        if adjoint_field is not None:
+            a_ex2, a_eval = dp.count_evaluated_adjoint(adjoint_field)
+            lines["adjoint"].append(sfu_line(k_adj, a_ex2, a_eval, kms["adjoint"]))
     if kms.get("wet"):
         # WET pass: RLSP read once (texture fill and cell records), raw WET
         # written and read back by the smoothing, smoothed WET written

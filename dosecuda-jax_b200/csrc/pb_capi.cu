@@ -396,6 +396,19 @@ PbStatus pb_count_evaluated(const PbGrid *grid, const PbBeam *beams, int n_beams
                                   count_dev, static_cast<cudaStream_t>(stream));
 }
 
+PbStatus pb_count_evaluated_adjoint(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                    const float *wet_dev, const PbLayer *layers_dev,
+                                    const float *spot_geo_dev, const float *dobj_dose_dev,
+                                    float scale, unsigned long long *count_dev, void *stream)
+{
+    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev);
+    if (s != PB_OK) return s;
+    if (!dobj_dose_dev || !count_dev) return set_error(PB_ERR_INVALID, "NULL argument");
+    return launch_count_evaluated(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev,
+                                  count_dev, static_cast<cudaStream_t>(stream), -1,
+                                  dobj_dose_dev, scale);
+}
+
 PbStatus pb_measure_ex2_rate(double *ops_per_s, void *stream)
 {
     if (!ops_per_s) return set_error(PB_ERR_INVALID, "ops_per_s is NULL");

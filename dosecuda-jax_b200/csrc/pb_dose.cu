@@ -622,6 +622,16 @@ __device__ __forceinline__ void dose_tile(const PlanArgs &A, int tile,
             for (int c = threadIdx.x; c < 2 * (kCull * kThreads + 8); c += kThreads)
                 gsum_xy[c] = 0.0f;
     }
+    if constexpr (COUNT) {
+        // counting for the adjoint: the tiles it skips are skipped here too
+        if (wfield != nullptr) {
+            bool anyw = false;
+#pragma unroll
+            for (int q = 0; q < kVpt; ++q)
+                anyw |= valid[q] && __ldg(wfield + vidx[q]) * A.scale != 0.0f;
+            if (!__syncthreads_or(anyw)) return;
+        }
+    }
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
@@ -1077,6 +1087,16 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
         if (!__syncthreads_or(anyw)) return;
         for (int c = t; c < kCap + 8; c += NT) sh.gsum[c] = 0.0f;
     }
+    if constexpr (COUNT) {
+        // counting for the adjoint: the tiles it skips are skipped here too
+        if (wfield != nullptr) {
+            bool anyw = false;
+#pragma unroll
+            for (int q = 0; q < kLine; ++q)
+                anyw |= q < nvalid && __ldg(wfield + vbase + q) * A.scale != 0.0f;
+            if (!__syncthreads_or(anyw)) return;
+        }
+    }
 
     for (int b = 0; b < A.n_beams; ++b) {
         const PbBeam &B = A.beams[b];
@@ -1443,14 +1463,14 @@ constexpr int kLineTY = 8, kLineTZ = 8, kLineCull = 2;
 __global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ>())
 k_dose_count_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                   const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
-                  unsigned long long *count)
+                  unsigned long long *count, const float *__restrict__ wfield)
 {
     __shared__ LineShared<kLineTY * kLineTZ, kLineCull, false, false> sh;
     int tx, ty, tz;
     line_tile_coords<kLineTY, kLineTZ>(A.g, blockIdx.x, tx, ty, tz);
     line_tile<kLineTY, kLineTZ, kLineCull, false, kModeCount>(A, tx, ty, tz, wet, layers, geo,
                                                               nullptr, nullptr, nullptr, sh,
-                                                              count);
+                                                              count, wfield);
 }
 
 __global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ>())
@@ -1495,11 +1515,11 @@ k_dose(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 __global__ void __launch_bounds__(128, dose_min_blocks<128, 1>())
 k_dose_count(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
              const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
-             unsigned long long *count)
+             unsigned long long *count, const float *__restrict__ wfield)
 {
     __shared__ DoseShared<128, 1> sh;
     dose_tile<128, 4, 1, false, kModeCount>(A, blockIdx.x, wet, layers, geo, nullptr, nullptr,
-                                            nullptr, sh, count);
+                                            nullptr, sh, count, wfield);
 }
 
 // Spot-weight gradient: dose_tile in adjoint mode, shape of pb_dose's kernel.
@@ -1836,10 +1856,9 @@ static const DoseVariant kDoseVariants[] = {
 };
 constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
 
-// The shape pb_dose and pb_count_evaluated use, and the family of
-// pb_dose_adjoint's kernel (true: line tiles).
+// The shape pb_dose and pb_count_evaluated use; pb_dose_adjoint runs the
+// adjoint kernel of its family.
 constexpr int kDefaultDoseVariant = 0;
-constexpr bool kAdjointLine = true;
 
 int dose_variant_default() { return kDefaultDoseVariant; }
 int dose_variant_count() { return kNumDoseVariants; }
@@ -1984,7 +2003,7 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
     if (s != PB_OK) return s;
     const int64_t tiles = (int64_t)A.tiles_x * A.tiles_y * A.tiles_z;
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
-    if (variant < 0 ? kAdjointLine : variant_line(variant)) {
+    if (variant_line(variant)) {
         k_adjoint_line<<<line_tiles(g, kLineTY, kLineTZ), kLineTY * kLineTZ, 0, st>>>(
             A, wet, layers, g4, w, grad);
         return check_launch("k_adjoint_line");
@@ -2049,10 +2068,11 @@ PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
 
 PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beams,
                                 const float *wet, const PbLayer *layers, const float *geo,
-                                unsigned long long *count, cudaStream_t st, int variant)
+                                unsigned long long *count, cudaStream_t st, int variant,
+                                const float *wfield, float scale)
 {
     PlanArgs A;
-    fill_args(A, g, beams, n_beams, 1.0f);
+    fill_args(A, g, beams, n_beams, scale);
     PbStatus s = check_cuda(cudaMemsetAsync(count, 0, 2 * sizeof(unsigned long long), st),
                             "cudaMemsetAsync(count)");
     if (s != PB_OK) return s;
@@ -2060,10 +2080,10 @@ PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beam
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
     if (variant_line(variant)) {
         k_dose_count_line<<<line_tiles(g, kLineTY, kLineTZ), kLineTY * kLineTZ, 0, st>>>(
-            A, wet, layers, g4, count);
+            A, wet, layers, g4, count, wfield);
         return check_launch("k_dose_count_line");
     }
-    k_dose_count<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers, g4, count);
+    k_dose_count<<<(unsigned)tiles, 128, 0, st>>>(A, wet, layers, g4, count, wfield);
     return check_launch("k_dose_count");
 }
 

@@ -101,7 +101,8 @@ PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
                             const float *geo, cudaStream_t st);
 PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beams,
                                 const float *wet, const PbLayer *layers, const float *geo,
-                                unsigned long long *count, cudaStream_t st, int variant = -1);
+                                unsigned long long *count, cudaStream_t st, int variant = -1,
+                                const float *wfield = nullptr, float scale = 1.0f);
 PbStatus measure_ex2_rate(double *ops_per_s, cudaStream_t st);
 PbStatus launch_count_pairs(const PbGrid &g, const PbBeam *beams, int n_beams,
                             const float *wet, const PbLayer *layers,

@@ -139,6 +139,8 @@ _SIGS = {
     "pb_dose_adjoint_positions": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _VP,
                                        _F, _VP, _VP, _VP, _VP]),
     "pb_count_evaluated": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _VP]),
+    "pb_count_evaluated_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP,
+                                        ctypes.c_float, _VP, _VP]),
     "pb_measure_ex2_rate": (_I, [ctypes.POINTER(ctypes.c_double), _VP]),
     "pb_proton_raytrace_host": (_I, [_I, _D, _D, _VP, _VP, _F, _VP, _VP, _D, _D, _VP]),
     "pb_proton_spot_host": (_I, [_I, _D, _D, _VP, _VP, _VP, _VP, _I, _I, _I, _VP, _VP, _F,

@@ -400,6 +400,22 @@ class DevicePlan:
         v = c.cpu().tolist()
         return int(v[0]), int(v[1])
 
+    def count_evaluated_adjoint(self, dobj_dose, scale: float = 1.0):
+        """(SFU exp2 operations, spot-voxel evaluations) one adjoint on the
+        field `dobj_dose` issues: the forward's decisions on the tiles the
+        adjoint does not skip."""
+        self._need_wet()
+        if dobj_dose.dtype != torch.float32 or dobj_dose.numel() != self.n_vox:
+            raise ValueError("dobj_dose must be float32 with one entry per voxel")
+        w = dobj_dose.contiguous()
+        c = torch.zeros(2, dtype=torch.int64, device=self.device)
+        check(_lib.lib.pb_count_evaluated_adjoint(
+            ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+            ptr(self.wet), ptr(self.layers), ptr(self.spot_geo), ptr(w), float(scale), ptr(c),
+            _stream(self.device)), "pb_count_evaluated_adjoint")
+        v = c.cpu().tolist()
+        return int(v[0]), int(v[1])
+
 
 def measure_ex2_rate(device) -> float:
     """Measured SFU exp2 throughput of a device (operations/s)."""

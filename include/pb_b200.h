@@ -258,6 +258,15 @@ PbStatus pb_count_evaluated(const PbGrid *grid, const PbBeam *beams, int n_beams
                             const float *spot_geo_dev, unsigned long long *count_dev,
                             void *stream);
 
+/* As pb_count_evaluated, for what pb_dose_adjoint issues on the field
+ * dobj_dose_dev with this scale: the tiles whose scale * dObj/dD is zero at
+ * every voxel are skipped, as the adjoint skips them, and the count follows
+ * the adjoint's kernel family.  No counterpart in the reference. */
+PbStatus pb_count_evaluated_adjoint(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                    const float *wet_dev, const PbLayer *layers_dev,
+                                    const float *spot_geo_dev, const float *dobj_dose_dev,
+                                    float scale, unsigned long long *count_dev, void *stream);
+
 /* Measured SFU exp2 throughput of the current device (operations/s): a
  * fixed kernel of independent exp2 chains on every SM, best of three
  * timed runs.  Synchronises with the stream.  No counterpart in the

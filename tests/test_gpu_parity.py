@@ -505,6 +505,24 @@ def test_layer_bounds_change_no_result(pkg, small, which):
     assert torch.allclose(g1, g2, rtol=1e-5, atol=1e-6 * float(g1.abs().max()))
 
 
+def test_adjoint_counts_follow_its_tile_skip(small):
+    """pb_count_evaluated_adjoint: on a field nonzero everywhere it counts
+    the forward's work; on a zero field nothing; on a field nonzero in one
+    slab of z only the tiles that reach the slab, so less than the forward
+    and more than nothing."""
+    dp = small.grid.prepareIMPTPlan(small.plan, 0)
+    fwd = dp.count_evaluated()
+    V = dp.n_vox
+    assert dp.count_evaluated_adjoint(torch.ones(V, device=DEV)) == fwd
+    assert dp.count_evaluated_adjoint(torch.ones(V, device=DEV), scale=2.0) == fwd
+    assert dp.count_evaluated_adjoint(torch.zeros(V, device=DEV)) == (0, 0)
+    nz = small.grid.HU.shape[0]
+    slab = torch.zeros(small.grid.HU.shape, device=DEV)
+    slab[nz // 2] = 1.0
+    part = dp.count_evaluated_adjoint(slab.reshape(-1))
+    assert 0 < part[0] < fwd[0] and 0 < part[1] < fwd[1]
+
+
 def test_layer_bounds_values(pkg, small):
     """pb_layer_bounds against a host recomputation: spot boxes and the LUT
     row maxima exactly, the halo-sigma bound at least the formula's maximum
