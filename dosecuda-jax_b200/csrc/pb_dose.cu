@@ -34,6 +34,7 @@
 // over a thread's voxels meet across the warp with a transposed butterfly,
 // across the block in shared memory, and go to the gradient with one global
 // atomic per spot per (tile, layer).
+#include <type_traits>
 #include "pb_internal.h"
 
 namespace pb {
@@ -44,6 +45,7 @@ struct PlanArgs {
     PbGrid g;
     int n_beams;
     int tiles_x, tiles_y, tiles_z;
+    int centre[3];   // voxel holding the mean isocentre (clamped to the grid)
     float scale;
     PbBeam beams[PB_MAX_BEAMS];
 };
@@ -1314,8 +1316,9 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                         // both terms: slots [0, n2); halo only: [kCap - n1, kCap);
                         // a group's slots past its class hold other records or
                         // padding, and their sums are dropped
-                        for (int two = 1; two >= 0; --two) {
-                            const int lo = two ? 0 : kCap - n1, hi = two ? n2 : kCap;
+                        // (the class is a compile-time constant of each
+                        // loop, so neither loop body branches on it)
+                        auto groups = [&](auto two, const int lo, const int hi) {
                             for (int c0 = lo; c0 < hi; c0 += 8) {
                                 float v[8];
 #pragma unroll
@@ -1330,7 +1333,7 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                                         const float2 o = line_off2(p);
                                         const float2 S = __ffma2_rn(__ffma2_rn(c2, o, b1), o, s0);
                                         acc = __ffma2_rn(AH[p], ex2x2(__fmul2_rn(HS[p], S)), acc);
-                                        if (two)
+                                        if constexpr (decltype(two)::value)
                                             acc = __ffma2_rn(AP[p], ex2x2(__fmul2_rn(PS[p], S)),
                                                              acc);
                                     }
@@ -1341,7 +1344,9 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                                 if ((lane & 3) == 0 && c0 + slot < hi && sum != 0.0f)
                                     atomicAdd(&sh.gsum[c0 + slot], sum);
                             }
-                        }
+                        };
+                        groups(std::true_type{}, 0, n2);
+                        groups(std::false_type{}, kCap - n1, kCap);
                         __syncthreads();
                         // each surviving spot's tile sum to its gradient
                         for (int c = t; c < n2 + n1; c += NT) {
@@ -1432,16 +1437,48 @@ template <int NT> constexpr int line_min_blocks()
     return NT == 32 ? 20 : (NT == 64 ? 10 : 5);
 }
 
-// Tile coordinates of a linear block index over the grid's 8 x TY x TZ tiles.
+#ifndef PB_TILE_ORDER
+#define PB_TILE_ORDER 1
+#endif
+
+// The r-th index of 0..n-1 taken outward from c: c, c+1, c-1, c+2, c-2, ...
+// and, once one side is used up, the rest of the other side in order.
+__device__ __forceinline__ int center_out(int r, int n, int c)
+{
+    const int m = min(c, n - 1 - c);
+    if (r <= 2 * m) {
+        const int k = (r + 1) >> 1;
+        return (r & 1) ? c + k : c - k;
+    }
+    const int j = r - 2 * m;
+    return c - m == 0 ? c + m + j : c - m - j;
+}
+
+// Tile of a linear block index over the grid's 8 x TY x TZ tiles.  Blocks
+// start in launch order, so the tiles are handed out from the tile holding
+// the plan's centre (the mean isocentre) outward, z slabs first: the tiles
+// most beams cross, the longest ones, start early and the launch does not
+// end on a few of them while the other SMs idle.
 template <int TY, int TZ>
-__device__ __forceinline__ void line_tile_coords(const PbGrid &g, long long tile, int &tx,
+__device__ __forceinline__ void line_tile_coords(const PlanArgs &A, long long tile, int &tx,
                                                  int &ty, int &tz)
 {
+    const PbGrid &g = A.g;
     const int nx8 = (g.nx + kLine - 1) / kLine, nty = (g.ny + TY - 1) / TY;
-    tx = (int)(tile % nx8);
+    const int rx = (int)(tile % nx8);
     tile /= nx8;
-    ty = (int)(tile % nty);
-    tz = (int)(tile / nty);
+    const int ry = (int)(tile % nty);
+    const int rz = (int)(tile / nty);
+    if (PB_TILE_ORDER == 0) {
+        tx = rx;
+        ty = ry;
+        tz = rz;
+        return;
+    }
+    const int ntz = (g.nz + TZ - 1) / TZ;
+    tx = center_out(rx, nx8, min(max(A.centre[0] / kLine, 0), nx8 - 1));
+    ty = center_out(ry, nty, min(max(A.centre[1] / TY, 0), nty - 1));
+    tz = center_out(rz, ntz, min(max(A.centre[2] / TZ, 0), ntz - 1));
 }
 
 template <int TY, int TZ, int KCULL, bool BEAM_OUT>
@@ -1453,7 +1490,7 @@ k_dose_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 {
     __shared__ LineShared<TY * TZ, KCULL, BEAM_OUT> sh;
     int tx, ty, tz;
-    line_tile_coords<TY, TZ>(A.g, blockIdx.x, tx, ty, tz);
+    line_tile_coords<TY, TZ>(A, blockIdx.x, tx, ty, tz);
     line_tile<TY, TZ, KCULL, BEAM_OUT>(A, tx, ty, tz, wet, layers, geo, mu, dose, beam_dose, sh);
 }
 
@@ -1467,7 +1504,7 @@ k_dose_count_line(const __grid_constant__ PlanArgs A, const float *__restrict__ 
 {
     __shared__ LineShared<kLineTY * kLineTZ, kLineCull, false, false> sh;
     int tx, ty, tz;
-    line_tile_coords<kLineTY, kLineTZ>(A.g, blockIdx.x, tx, ty, tz);
+    line_tile_coords<kLineTY, kLineTZ>(A, blockIdx.x, tx, ty, tz);
     line_tile<kLineTY, kLineTZ, kLineCull, false, kModeCount>(A, tx, ty, tz, wet, layers, geo,
                                                               nullptr, nullptr, nullptr, sh,
                                                               count, wfield);
@@ -1480,7 +1517,7 @@ k_adjoint_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet
 {
     __shared__ LineShared<kLineTY * kLineTZ, kLineCull, false, false> sh;
     int tx, ty, tz;
-    line_tile_coords<kLineTY, kLineTZ>(A.g, blockIdx.x, tx, ty, tz);
+    line_tile_coords<kLineTY, kLineTZ>(A, blockIdx.x, tx, ty, tz);
     line_tile<kLineTY, kLineTZ, kLineCull, false, kModeAdjoint>(A, tx, ty, tz, wet, layers, geo,
                                                                 nullptr, nullptr, nullptr, sh,
                                                                 nullptr, wfield, grad);
@@ -1831,7 +1868,16 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
     A.tiles_y = (g.ny + 7) / 8;
     A.tiles_z = (g.nz + 7) / 8;
     A.scale = scale;
-    for (int b = 0; b < n_beams; ++b) A.beams[b] = beams[b];
+    double c[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < n_beams; ++b) {
+        A.beams[b] = beams[b];
+        for (int a = 0; a < 3; ++a) c[a] += beams[b].geom.iso[a];
+    }
+    const int n[3] = {g.nx, g.ny, g.nz};
+    for (int a = 0; a < 3; ++a) {
+        const double v = n_beams > 0 && g.spacing > 0.0f ? c[a] / n_beams / g.spacing : 0.0;
+        A.centre[a] = v != v ? 0 : (int)fmin(fmax(v, 0.0), (double)(n[a] - 1));
+    }
 }
 
 // Forward kernel variants the autotuner chooses from.  Two families:
