@@ -458,6 +458,31 @@ __device__ __forceinline__ float warp_sum8(float (&v)[8], int lane, int &slot)
     return t;
 }
 
+// Sum over the warp of N per-lane values v[0..N-1] (N = 1, 2, 4 or 8; one
+// per spot): log2 N transposed butterfly levels, each halving the values a
+// lane holds, then plain levels down to offset 1.  On return the lanes whose
+// low log2(32 / N) bits are 0 hold the total of spot `slot`.
+template <int N>
+__device__ __forceinline__ float warp_sum_n(float (&v)[N], int lane, int &slot)
+{
+    static_assert(N == 1 || N == 2 || N == 4 || N == 8, "1, 2, 4 or 8 values");
+    slot = 0;
+#pragma unroll
+    for (int h = N / 2, off = 16; h >= 1; h /= 2, off /= 2) {
+        const bool up = lane & off;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const float send = up ? v[i] : v[i + h], keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+        }
+        slot = 2 * slot + (up ? 1 : 0);
+    }
+    float t = v[0];
+#pragma unroll
+    for (int off = 16 / N; off >= 1; off /= 2) t += __shfl_xor_sync(0xffffffffu, t, off);
+    return t;
+}
+
 // Spot-position derivatives of the adjoint sums.  With q = |t x ray|^2 *
 // it2 the scaled squared axis distance (axis_r2), the spot's factor at a
 // voxel is mu (Pf 2^(ps2 q) + Hf 2^(hs2 q)), so
@@ -1318,32 +1343,47 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                         // padding, and their sums are dropped
                         // (the class is a compile-time constant of each
                         // loop, so neither loop body branches on it)
-                        auto groups = [&](auto two, const int lo, const int hi) {
-                            for (int c0 = lo; c0 < hi; c0 += 8) {
-                                float v[8];
+                        // groups of 8 spots, the rest in groups of 4, 2 and 1,
+                        // so that no padding slot is evaluated
+                        auto group = [&](auto two, auto n, const int c0) {
+                            constexpr int N = decltype(n)::value;
+                            float v[N];
 #pragma unroll
-                                for (int u = 0; u < 8; ++u) {
-                                    const LineSpot r = sh.spot[c0 + u];
-                                    float S0, B1;
-                                    line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
-                                    const float2 s0 = f2(S0), b1 = f2(B1), c2 = f2(r.b.z);
-                                    float2 acc = make_float2(0.0f, 0.0f);
+                            for (int u = 0; u < N; ++u) {
+                                const LineSpot r = sh.spot[c0 + u];
+                                float S0, B1;
+                                line_spot(r, Xc, Yc, gxc, gyc, S0, B1);
+                                const float2 s0 = f2(S0), b1 = f2(B1), c2 = f2(r.b.z);
+                                float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-                                    for (int p = 0; p < kLine / 2; ++p) {
-                                        const float2 o = line_off2(p);
-                                        const float2 S = __ffma2_rn(__ffma2_rn(c2, o, b1), o, s0);
-                                        acc = __ffma2_rn(AH[p], ex2x2(__fmul2_rn(HS[p], S)), acc);
-                                        if constexpr (decltype(two)::value)
-                                            acc = __ffma2_rn(AP[p], ex2x2(__fmul2_rn(PS[p], S)),
-                                                             acc);
-                                    }
-                                    v[u] = acc.x + acc.y;
+                                for (int p = 0; p < kLine / 2; ++p) {
+                                    const float2 o = line_off2(p);
+                                    const float2 S = __ffma2_rn(__ffma2_rn(c2, o, b1), o, s0);
+                                    acc = __ffma2_rn(AH[p], ex2x2(__fmul2_rn(HS[p], S)), acc);
+                                    if constexpr (decltype(two)::value)
+                                        acc = __ffma2_rn(AP[p], ex2x2(__fmul2_rn(PS[p], S)),
+                                                         acc);
                                 }
-                                int slot;
-                                const float sum = warp_sum8(v, lane, slot);
-                                if ((lane & 3) == 0 && c0 + slot < hi && sum != 0.0f)
-                                    atomicAdd(&sh.gsum[c0 + slot], sum);
+                                v[u] = acc.x + acc.y;
                             }
+                            int slot;
+                            const float sum = warp_sum_n<N>(v, lane, slot);
+                            if ((lane & (32 / N - 1)) == 0 && sum != 0.0f)
+                                atomicAdd(&sh.gsum[c0 + slot], sum);
+                        };
+                        auto groups = [&](auto two, const int lo, const int hi) {
+                            int c0 = lo;
+                            for (; c0 + 8 <= hi; c0 += 8)
+                                group(two, std::integral_constant<int, 8>{}, c0);
+                            if (hi - c0 >= 4) {
+                                group(two, std::integral_constant<int, 4>{}, c0);
+                                c0 += 4;
+                            }
+                            if (hi - c0 >= 2) {
+                                group(two, std::integral_constant<int, 2>{}, c0);
+                                c0 += 2;
+                            }
+                            if (hi - c0 >= 1) group(two, std::integral_constant<int, 1>{}, c0);
                         };
                         groups(std::true_type{}, 0, n2);
                         groups(std::false_type{}, kCap - n1, kCap);
@@ -1494,8 +1534,43 @@ k_dose_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
     line_tile<TY, TZ, KCULL, BEAM_OUT>(A, tx, ty, tz, wet, layers, geo, mu, dose, beam_dose, sh);
 }
 
-// Line-tile shape of the default forward, its count and its adjoint.
-constexpr int kLineTY = 8, kLineTZ = 8, kLineCull = 2;
+// Forward kernel variants the autotuner chooses from.  Two families:
+//   t<threads>_v<voxels per thread>_c<k>  8x8x8 tiles, each thread a set of
+//       voxels evaluated one by one (dose_tile);
+//   l8x<TY>x<TZ>_c<k>  8 x TY x TZ tiles, each thread a line of 8 voxels
+//       along x evaluated as a quadratic (line_tile);
+// k = spots each thread culls per compaction round.  `batch` marks the
+// shapes the persistent batch kernel takes (tiles dividing 8x8x8 units).
+struct DoseVariant {
+    int line, ty, tz, nt, kcull;
+    bool batch;
+    const char *name;
+};
+constexpr DoseVariant kDoseVariants[] = {
+    {1, 8, 8, 64, 2, true, "l8x8x8_c2"},    {1, 8, 8, 64, 4, true, "l8x8x8_c4"},
+    {1, 8, 4, 32, 4, true, "l8x8x4_c4"},    {1, 4, 8, 32, 4, true, "l8x4x8_c4"},
+    {1, 16, 8, 128, 2, false, "l8x16x8_c2"}, {1, 8, 16, 128, 2, false, "l8x8x16_c2"},
+    {0, 8, 8, 128, 1, true, "t128_v4_c1"},  {0, 8, 8, 128, 2, true, "t128_v4_c2"},
+    {0, 8, 8, 128, 4, true, "t128_v4_c4"},  {0, 8, 8, 256, 1, true, "t256_v2_c1"},
+    {0, 8, 8, 128, 3, true, "t128_v4_c3"},
+};
+constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
+
+// The shape pb_dose and pb_count_evaluated use; pb_dose_adjoint runs the
+// adjoint kernel of its family.
+#ifndef PB_DEFAULT_DOSE_VARIANT
+#define PB_DEFAULT_DOSE_VARIANT 0
+#endif
+constexpr int kDefaultDoseVariant = PB_DEFAULT_DOSE_VARIANT;
+static_assert(kDefaultDoseVariant >= 0 && kDefaultDoseVariant < kNumDoseVariants,
+              "default shape");
+
+// Line-tile shape of the counts and the adjoint (and of the per-beam
+// forward): the default's when it is a line shape, else l8x8x8_c2.
+constexpr int kLineShape = kDoseVariants[kDefaultDoseVariant].line ? kDefaultDoseVariant : 0;
+static_assert(kDoseVariants[kLineShape].line, "a line shape");
+constexpr int kLineTY = kDoseVariants[kLineShape].ty, kLineTZ = kDoseVariants[kLineShape].tz,
+              kLineCull = kDoseVariants[kLineShape].kcull;
 
 __global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ>())
 k_dose_count_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
@@ -1880,31 +1955,6 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
     }
 }
 
-// Forward kernel variants the autotuner chooses from.  Two families:
-//   t<threads>_v<voxels per thread>_c<k>  8x8x8 tiles, each thread a set of
-//       voxels evaluated one by one (dose_tile);
-//   l8x<TY>x<TZ>_c<k>  8 x TY x TZ tiles, each thread a line of 8 voxels
-//       along x evaluated as a quadratic (line_tile);
-// k = spots each thread culls per compaction round.  `batch` marks the
-// shapes the persistent batch kernel takes (tiles dividing 8x8x8 units).
-struct DoseVariant {
-    int line, ty, tz, nt, kcull;
-    bool batch;
-    const char *name;
-};
-static const DoseVariant kDoseVariants[] = {
-    {1, 8, 8, 64, 2, true, "l8x8x8_c2"},    {1, 8, 8, 64, 4, true, "l8x8x8_c4"},
-    {1, 8, 4, 32, 4, true, "l8x8x4_c4"},    {1, 4, 8, 32, 4, true, "l8x4x8_c4"},
-    {1, 16, 8, 128, 2, false, "l8x16x8_c2"}, {1, 8, 16, 128, 2, false, "l8x8x16_c2"},
-    {0, 8, 8, 128, 1, true, "t128_v4_c1"},  {0, 8, 8, 128, 2, true, "t128_v4_c2"},
-    {0, 8, 8, 128, 4, true, "t128_v4_c4"},  {0, 8, 8, 256, 1, true, "t256_v2_c1"},
-    {0, 8, 8, 128, 3, true, "t128_v4_c3"},
-};
-constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]);
-
-// The shape pb_dose and pb_count_evaluated use; pb_dose_adjoint runs the
-// adjoint kernel of its family.
-constexpr int kDefaultDoseVariant = 0;
 
 int dose_variant_default() { return kDefaultDoseVariant; }
 int dose_variant_count() { return kNumDoseVariants; }
