@@ -1559,14 +1559,16 @@ constexpr int kNumDoseVariants = sizeof(kDoseVariants) / sizeof(kDoseVariants[0]
 // The shape pb_dose and pb_count_evaluated use; pb_dose_adjoint runs the
 // adjoint kernel of its family.
 #ifndef PB_DEFAULT_DOSE_VARIANT
-#define PB_DEFAULT_DOSE_VARIANT 0
+#define PB_DEFAULT_DOSE_VARIANT 4   // l8x16x8_c2
 #endif
 constexpr int kDefaultDoseVariant = PB_DEFAULT_DOSE_VARIANT;
 static_assert(kDefaultDoseVariant >= 0 && kDefaultDoseVariant < kNumDoseVariants,
               "default shape");
 
 // Line-tile shape of the counts and the adjoint (and of the per-beam
-// forward): the default's when it is a line shape, else l8x8x8_c2.
+// forward): the default's when it is a line shape, else l8x8x8_c2.  On
+// the 4-beam 256x256x160 plan l8x16x8_c2 measured 6.72 ms forward and
+// 7.12 ms adjoint, against 6.83 and 7.55 ms for l8x8x8_c2.
 constexpr int kLineShape = kDoseVariants[kDefaultDoseVariant].line ? kDefaultDoseVariant : 0;
 static_assert(kDoseVariants[kLineShape].line, "a line shape");
 constexpr int kLineTY = kDoseVariants[kLineShape].ty, kLineTZ = kDoseVariants[kLineShape].tz,

@@ -78,6 +78,17 @@ def default_variant() -> int:
     return int(_lib.lib.pb_dose_variant_default())
 
 
+def default_batch_variant() -> int:
+    """The shape the batch uses before tuning: the default when the batch
+    takes it, else the first batch shape of the default's family."""
+    names = variants()
+    d = default_variant()
+    if batch_shape(names[d]):
+        return d
+    fam = shape_of(names[d])[0]
+    return next(v for v, n in enumerate(names) if shape_of(n)[0] == fam and batch_shape(n))
+
+
 def shape_of(name: str) -> Tuple[str, Tuple[int, int, int], int, int]:
     """(family "t" or "l", voxel tile (x, y, z), block threads, spots culled
     per thread per round) of a kernel shape."""

@@ -65,7 +65,7 @@ class BatchPlans:
         check(_lib.lib.pb_batch_setup(ctypes.cast(recs, ctypes.c_void_p), self.n_plans,
                                       ptr(self.work), ctypes.byref(self.info),
                                       engine._stream(self.device)), "pb_batch_setup")
-        self.variant = autotune.default_variant()
+        self.variant = autotune.default_batch_variant()
         self.blocks_per_sm = 4
 
     @property

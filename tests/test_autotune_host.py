@@ -32,6 +32,10 @@ def test_variants_and_batch_candidates():
     assert autotune.max_blocks_per_sm("l8x8x4_c4") == 20
     assert autotune.batch_shape("l8x4x8_c4") and not autotune.batch_shape("l8x8x16_c2")
     assert {names[v] for v, _ in cands} == {n for n in names if autotune.batch_shape(n)}
+    # the default forward shape, and the batch's own default when the
+    # persistent kernel cannot take it
+    assert names[autotune.default_variant()] == "l8x16x8_c2"
+    assert names[autotune.default_batch_variant()] == "l8x8x8_c2"
 
 
 def test_cache_roundtrip(tmp_path, monkeypatch):
