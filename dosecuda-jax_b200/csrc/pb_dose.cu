@@ -46,6 +46,7 @@ struct PlanArgs {
     int n_beams;
     int tiles_x, tiles_y, tiles_z;
     int centre[3];   // voxel holding the mean isocentre (clamped to the grid)
+    int z0, z1;      // line-tile launches: only the voxel planes z0 <= k < z1
     float scale;
     PbBeam beams[PB_MAX_BEAMS];
 };
@@ -1512,13 +1513,13 @@ __device__ __forceinline__ void line_tile_coords(const PlanArgs &A, long long ti
     if (PB_TILE_ORDER == 0) {
         tx = rx;
         ty = ry;
-        tz = rz;
+        tz = A.z0 / TZ + rz;
         return;
     }
-    const int ntz = (g.nz + TZ - 1) / TZ;
+    const int tz0 = A.z0 / TZ, ntz = (A.z1 + TZ - 1) / TZ - tz0;
     tx = center_out(rx, nx8, min(max(A.centre[0] / kLine, 0), nx8 - 1));
     ty = center_out(ry, nty, min(max(A.centre[1] / TY, 0), nty - 1));
-    tz = center_out(rz, ntz, min(max(A.centre[2] / TZ, 0), ntz - 1));
+    tz = tz0 + center_out(rz, ntz, min(max(A.centre[2] / TZ - tz0, 0), ntz - 1));
 }
 
 template <int TY, int TZ, int KCULL, bool BEAM_OUT>
@@ -1945,6 +1946,8 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
     A.tiles_y = (g.ny + 7) / 8;
     A.tiles_z = (g.nz + 7) / 8;
     A.scale = scale;
+    A.z0 = 0;
+    A.z1 = g.nz;
     double c[3] = {0.0, 0.0, 0.0};
     for (int b = 0; b < n_beams; ++b) {
         A.beams[b] = beams[b];
@@ -1959,6 +1962,7 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
 
 
 int dose_variant_default() { return kDefaultDoseVariant; }
+int dose_slab_planes() { return kLineTZ; }
 int dose_variant_count() { return kNumDoseVariants; }
 
 static bool variant_line(int v)
@@ -1975,10 +1979,11 @@ static bool dose_variant_batch(int v)
     return v >= 0 && v < kNumDoseVariants && kDoseVariants[v].batch;
 }
 
-static unsigned line_tiles(const PbGrid &g, int ty, int tz)
+static unsigned line_tiles(const PbGrid &g, int ty, int tz, int z0 = 0, int z1 = -1)
 {
+    if (z1 < 0) z1 = g.nz;
     return (unsigned)((long long)((g.nx + kLine - 1) / kLine) * ((g.ny + ty - 1) / ty) *
-                      ((g.nz + tz - 1) / tz));
+                      ((z1 + tz - 1) / tz - z0 / tz));
 }
 
 template <int NT, int VPT, int KCULL>
@@ -1993,20 +1998,36 @@ template <int TY, int TZ, int KCULL>
 static void launch_line_t(const PlanArgs &A, const float *wet, const PbLayer *layers,
                           const float4 *geo, const float *mu, float *dose, cudaStream_t st)
 {
-    k_dose_line<TY, TZ, KCULL, false><<<line_tiles(A.g, TY, TZ), TY * TZ, 0, st>>>(
+    k_dose_line<TY, TZ, KCULL, false><<<line_tiles(A.g, TY, TZ, A.z0, A.z1), TY * TZ, 0, st>>>(
         A, wet, layers, geo, mu, dose, nullptr);
 }
 
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers, const float *geo,
                      const float *mu, float scale, float *dose, float *beam_dose,
-                     cudaStream_t st, int variant)
+                     cudaStream_t st, int variant, int z0, int z1)
 {
     PlanArgs A;
     fill_args(A, g, beams, n_beams, scale);
     const unsigned tiles = (unsigned)((int64_t)A.tiles_x * A.tiles_y * A.tiles_z);
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
     if (variant < 0) variant = kDefaultDoseVariant;
+    if (z0 != 0 || (z1 >= 0 && z1 != g.nz)) {
+        // a slab of planes: the default line shape only (the caller checks
+        // the bounds against its tile depth)
+        if (!variant_line(variant) || variant != kDefaultDoseVariant)
+            return set_error(PB_ERR_INVALID, "a slab needs the default line shape");
+        A.z0 = z0;
+        A.z1 = z1;
+        if (z0 >= z1) return PB_OK;
+        if (beam_dose)
+            k_dose_line<kLineTY, kLineTZ, kLineCull, true>
+                <<<line_tiles(g, kLineTY, kLineTZ, z0, z1), kLineTY * kLineTZ, 0, st>>>(
+                    A, wet, layers, g4, mu, dose, beam_dose);
+        else
+            launch_line_t<kLineTY, kLineTZ, kLineCull>(A, wet, layers, g4, mu, dose, st);
+        return check_launch("k_dose_line");
+    }
     if (beam_dose) {
         // per-beam output: the default shape of the variant's family only
         if (variant_line(variant))

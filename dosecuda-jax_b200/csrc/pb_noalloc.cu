@@ -24,7 +24,6 @@
 // (cudaGetSymbolAddress, with the device current) on its first call in that
 // context, and keeps it for that context: one set-up per device, repeated
 // only if the device's context is re-created (after cudaDeviceReset, say).
-// Make that first call before any stream capture.
 #include <cuda.h>
 
 #include <mutex>

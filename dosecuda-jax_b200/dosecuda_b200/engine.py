@@ -321,6 +321,32 @@ class DevicePlan:
                                _stream(self.device)), "pb_dose")
         return (dose, bd) if beam_doses else dose
 
+    def forward_slab(self, z_begin: int, z_end: int, dose: torch.Tensor,
+                     beam_doses: Optional[torch.Tensor] = None,
+                     mu_sorted: Optional[torch.Tensor] = None, scale: float = 1.0) -> None:
+        """The forward of the voxel planes z_begin <= z < z_end only, into
+        `dose` (V) and, if given, `beam_doses` (n_beams x V); other planes
+        are left as they are (pb_dose_slab).  The bounds are multiples of
+        slab_planes() or nz."""
+        self._need_wet()
+        mu = (self.mu_sorted if mu_sorted is None else mu_sorted).contiguous()
+        if mu.dtype != torch.float32 or mu.numel() != self.n_spots:
+            raise ValueError("mu must be float32 with one entry per spot")
+        for t, n in ((dose, self.n_vox), (beam_doses, self.n_beams * self.n_vox)):
+            if t is not None and (t.dtype != torch.float32 or t.numel() != n or
+                                  not t.is_contiguous() or t.device != self.device):
+                raise ValueError("dose buffers must be contiguous float32 on the plan's device")
+        check(_lib.lib.pb_dose_slab(ctypes.byref(self.grid),
+                                    ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                                    ptr(self.wet), ptr(self.layers), ptr(self.spot_geo), ptr(mu),
+                                    float(scale), ptr(dose), ptr(beam_doses), int(z_begin),
+                                    int(z_end), _stream(self.device)), "pb_dose_slab")
+
+    @staticmethod
+    def slab_planes() -> int:
+        """Plane multiple that forward_slab's bounds take."""
+        return int(_lib.lib.pb_dose_slab_planes())
+
     def forward_variant(self, variant: int, mu_sorted: Optional[torch.Tensor] = None,
                         scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Forward dose with one of the kernel shapes of pb_dose_variant."""

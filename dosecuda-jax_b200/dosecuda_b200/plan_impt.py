@@ -119,6 +119,13 @@ def _pinned_copy(t: torch.Tensor) -> torch.Tensor:
     return h
 
 
+def _slabs(nz: int, step: int, n: int = 4):
+    """About n slabs of z planes, bounds multiples of `step` (the last ends
+    at nz)."""
+    size = max(step, -(-nz // n // step) * step)
+    return [(z, min(z + size, nz)) for z in range(0, nz, size)]
+
+
 def _beam_model(plan, beam):
     try:
         model_index = list(plan.dicom_rangeshifter_label.astype(str)).index(
@@ -235,14 +242,38 @@ class IMPTDoseGrid(DoseGrid):
         side.wait_stream(main)
         with torch.cuda.stream(side):
             rlsp_h = _pinned_copy(rlsp)
+        chunks = self._beam_chunks(plan)
         total, beams_h, keep = None, [], []
-        for chunk in self._beam_chunks(plan):
-            dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
-            dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
-            beams_h.append((_pinned_copy(bd), dp.n_beams))
-            keep.append(bd)
-            total = dose if total is None else total + dose
-        dose_h = _pinned_copy(total)
+        if len(chunks) == 1:
+            # one launch per slab of z planes; each slab's planes go back to
+            # the host on the copy stream while the next slab computes
+            dp = self._transient(plan, gpu_id, chunks[0], wet_mode, rlsp)
+            V, nb = dp.n_vox, dp.n_beams
+            dose = torch.empty(V, dtype=torch.float32, device=device)
+            bd = torch.empty((nb, V), dtype=torch.float32, device=device)
+            dose_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
+            bd_h = torch.empty((nb, V), dtype=torch.float32, pin_memory=True)
+            plane = shape[1] * shape[2]
+            for z0, z1 in _slabs(shape[0], dp.slab_planes()):
+                dp.forward_slab(z0, z1, dose, bd, scale=float(plan.n_fractions))
+                done = torch.cuda.Event()
+                done.record(main)
+                side.wait_event(done)
+                lo, hi = z0 * plane, z1 * plane
+                with torch.cuda.stream(side):
+                    dose_h[lo:hi].copy_(dose[lo:hi], non_blocking=True)
+                    for b in range(nb):
+                        bd_h[b, lo:hi].copy_(bd[b, lo:hi], non_blocking=True)
+            beams_h.append((bd_h, nb))
+            keep += [dose, bd]
+        else:
+            for chunk in chunks:
+                dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
+                dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
+                beams_h.append((_pinned_copy(bd), dp.n_beams))
+                keep.append(bd)
+                total = dose if total is None else total + dose
+            dose_h = _pinned_copy(total)
         main.synchronize()
         side.synchronize()
         for bd_h, n in beams_h:

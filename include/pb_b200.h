@@ -184,8 +184,7 @@ PbStatus pb_wet(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
  * n_beams x V above that is rejected with PB_ERR_INVALID.  The call
  * allocates nothing (tex, if non-zero, comes from pb_texture_create made
  * earlier; tex = 0 needs nothing else).  Its first call on a device looks
- * up the array's device address; make it before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race and must be
+ * up the array's device address.  All calls share the array: calls that overlap on the GPU race and must be
  * serialised by the caller. */
 #define PB_NOALLOC_MAX_WET_FLOATS (8u * 1024u * 1024u)
 PbStatus pb_wet_noalloc(const float *rlsp_dev, PbTexture tex, const PbGrid *grid,
@@ -337,6 +336,20 @@ PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
  * graph once and replayed.  Concurrent runs on one work_dev race. */
 PbStatus pb_batch_run(const PbBatchInfo *info, void *work_dev, int flags, int variant,
                       int blocks_per_sm, int *status_dev, void *stream);
+
+/* pb_dose over the voxel planes z_begin <= z < z_end only: the dose (and,
+ * with beam_dose_dev, every beam's dose) of those planes is written and
+ * the other planes are left as they are; each plane gets the same bits as
+ * from pb_dose.  The bounds are multiples of pb_dose_slab_planes() (the
+ * default shape's tile depth), z_end may also be nz; z_begin == z_end does
+ * nothing.  A caller copies the planes of one slab back to the host while
+ * the next slab computes.  No counterpart in the reference. */
+PbStatus pb_dose_slab(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                      const float *wet_dev, const PbLayer *layers_dev,
+                      const float *spot_geo_dev, const float *mu_dev, float scale,
+                      float *dose_dev, float *beam_dose_dev, int z_begin, int z_end,
+                      void *stream);
+int pb_dose_slab_planes(void);
 
 /* Adjoint of pb_dose: grad_dev[s] = scale * sum_v dobj_dose_dev[v] * K(v,s)
  * for every spot s, where K(v,s) is the dose per unit weight of spot s at
