@@ -63,8 +63,11 @@ L2_FLUSH_BYTES = 256 << 20
 L2_NOTE = "flushed (256 MiB write) between timed iterations"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu captures of
 # this workload (seed 3, texture WET) on the kernels as built now; the command
-# and the figures are in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md
-NCU_TRAFFIC = {"k_dose_line": None, "k_adjoint_line": None}
+# and the figures are in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md.
+# Reported only for that workload ("wet": k_raytrace + k_smooth).
+NCU_TRAFFIC = {"k_dose_line": 199_179_520, "k_adjoint_line": 130_792_704,
+               "wet": 849_633_024}
+NCU_TRAFFIC_WORKLOAD = {"seed": 3, "wet_mode": "texture"}
 
 
 def kernel_names():
@@ -296,6 +299,10 @@ def run_mine(args, world, rank, local):
     def e2e_grad():
         host_step(hu_h, presc_h, wts_h, mu_h, dose_out, grad_out, obj_out)
 
+    # the step's input in page-locked host memory (the same values): the
+    # HU volume goes up asynchronously
+    g.HU = hu_h.numpy().reshape(np.shape(g.HU))
+
     def e2e_forward():
         # the reference's call: host HU in; host dose, per-beam doses and
         # RLSP out (spot sort, layer build, texture creation included)
@@ -378,14 +385,16 @@ def run_mine(args, world, rank, local):
                          (3 if args.mode == "grad" else 0)) * args.steps,
         "clocks": clk.summary(),
     }
-    line.update(rooflines(dp, kms, V, E, dev, resid))
+    same = args.seed == NCU_TRAFFIC_WORKLOAD["seed"] and \
+        args.wet_mode == NCU_TRAFFIC_WORKLOAD["wet_mode"]
+    line.update(rooflines(dp, kms, V, E, dev, resid, NCU_TRAFFIC if same else {}))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case, dp, E)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def rooflines(dp, kms, V, E, dev, adjoint_field=None) -> dict:
+def rooflines(dp, kms, V, E, dev, adjoint_field=None, traffic=None) -> dict:
     """Roofline lines of every kernel group over 1 ms in the step.
 
     HBM: algorithmic bytes per launch (each input read once, each output
@@ -421,14 +430,14 @@ def rooflines(dp, kms, V, E, dev, adjoint_field=None) -> dict:
     n_ex2, n_eval = dp.count_evaluated()
     k_dose, k_adj = kernel_names()
     out = {"roofline": hbm_line(f"{k_dose} (forward pencil-beam sum)", bytes_dose, kms["dose"],
-                                NCU_TRAFFIC.get(k_dose)),
+                                traffic.get(k_dose)),
            "compute_roofline": sfu_line(k_dose, n_ex2, n_eval, kms["dose"])}
     lines = {}
     if kms.get("adjoint"):
         # adjoint: WET of every beam and dObj/dD read, per spot 32 B of
         # geometry and its gradient written, the LUT rows
         bytes_adj = 4 * V * (B + 1) + 36 * S + lut
-        lines["adjoint"] = [hbm_line(k_adj, bytes_adj, kms["adjoint"], NCU_TRAFFIC.get(k_adj))]
+        lines["adjoint"] = [hbm_line(k_adj, bytes_adj, kms["adjoint"], traffic.get(k_adj))]
         if adjoint_field is not None:
             a_ex2, a_eval = dp.count_evaluated_adjoint(adjoint_field)
             lines["adjoint"].append(sfu_line(k_adj, a_ex2, a_eval, kms["adjoint"]))
@@ -436,7 +445,7 @@ def rooflines(dp, kms, V, E, dev, adjoint_field=None) -> dict:
         # WET pass: RLSP read once (texture fill and cell records), raw WET
         # written and read back by the smoothing, smoothed WET written
         lines["wet"] = [hbm_line("WET (cell records + k_raytrace + k_smooth)",
-                                 4 * V * (1 + 3 * B), kms["wet"])]
+                                 4 * V * (1 + 3 * B), kms["wet"], traffic.get("wet"))]
     if kms.get("rlsp"):
         lines["rlsp"] = [hbm_line("k_rlsp", 8 * V, kms["rlsp"])]
     out["kernel_rooflines"] = lines

@@ -315,34 +315,6 @@ PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams, const flo
                        dose_dev, beam_dose_dev, static_cast<cudaStream_t>(stream));
 }
 
-PbStatus pb_dose_slab(const PbGrid *grid, const PbBeam *beams, int n_beams,
-                      const float *wet_dev, const PbLayer *layers_dev,
-                      const float *spot_geo_dev, const float *mu_dev, float scale,
-                      float *dose_dev, float *beam_dose_dev, int z_begin, int z_end,
-                      void *stream)
-{
-    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev);
-    if (s != PB_OK) return s;
-    if (!dose_dev) return set_error(PB_ERR_INVALID, "dose is NULL");
-    if (!mu_dev) {
-        for (int b = 0; b < n_beams; ++b)
-            if (beams[b].n_layers) return set_error(PB_ERR_INVALID, "mu is NULL");
-    }
-    const int step = dose_slab_planes();
-    if (z_begin < 0 || z_end > grid->nz || z_begin > z_end)
-        return set_error(PB_ERR_INVALID, "slab [%d, %d) outside 0..%d", z_begin, z_end,
-                         grid->nz);
-    if (z_begin % step != 0 || (z_end % step != 0 && z_end != grid->nz))
-        return set_error(PB_ERR_INVALID, "slab [%d, %d): bounds must be multiples of %d "
-                         "(or the grid's nz)", z_begin, z_end, step);
-    if (z_begin == z_end) return PB_OK;
-    return launch_dose(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev, mu_dev, scale,
-                       dose_dev, beam_dose_dev, static_cast<cudaStream_t>(stream), -1, z_begin,
-                       z_end);
-}
-
-int pb_dose_slab_planes(void) { return dose_slab_planes(); }
-
 PbStatus pb_dose_adjoint(const PbGrid *grid, const PbBeam *beams, int n_beams,
                          const float *wet_dev, const PbLayer *layers_dev,
                          const float *spot_geo_dev, const float *dobj_dose_dev, float scale,

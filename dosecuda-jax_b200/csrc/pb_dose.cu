@@ -46,7 +46,6 @@ struct PlanArgs {
     int n_beams;
     int tiles_x, tiles_y, tiles_z;
     int centre[3];   // voxel holding the mean isocentre (clamped to the grid)
-    int z0, z1;      // line-tile launches: only the voxel planes z0 <= k < z1
     float scale;
     PbBeam beams[PB_MAX_BEAMS];
 };
@@ -63,7 +62,8 @@ struct __align__(16) SpotRec {
 
 struct TileBounds {
     float x0, x1, y0, y1, gx0, gx1, gy0, gy1;  // BEV box and divergence factors
-    float d0, d1, w0;                          // source distance range, least 10*WET
+    float d0, d1, w0, w1;                      // source distance range, least and
+                                               // greatest 10*WET
 };
 
 // Slots of the per-warp reduction array: 11 for tile_bounds, 2 for block_max2.
@@ -229,8 +229,8 @@ __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y
                                                   float (*s_red)[kRedSlots])
 {
     constexpr int kWarps = NT / 32;
-    float v[11] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
-                   INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY};
+    float v[12] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
+                   INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
         if (!valid[q]) continue;
@@ -239,29 +239,31 @@ __device__ __forceinline__ TileBounds tile_bounds(const float *X, const float *Y
         v[4] = fminf(v[4], GX[q]); v[5] = fmaxf(v[5], GX[q]);
         v[6] = fminf(v[6], GY[q]); v[7] = fmaxf(v[7], GY[q]);
         v[8] = fminf(v[8], D[q]);  v[9] = fmaxf(v[9], D[q]);
-        v[10] = fminf(v[10], W[q] == W[q] ? W[q] : -INFINITY);   // a NaN depth is never skipped
+        // a NaN depth is never skipped: it widens both depth bounds
+        v[10] = fminf(v[10], W[q] == W[q] ? W[q] : -INFINITY);
+        v[11] = fmaxf(v[11], W[q] == W[q] ? W[q] : INFINITY);
     }
     // slot m: odd = max, even = min
 #pragma unroll
-    for (int m = 0; m < 11; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
+    for (int m = 0; m < 12; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
 #pragma unroll
-        for (int m = 0; m < 11; ++m) s_red[warp][m] = v[m];
+        for (int m = 0; m < 12; ++m) s_red[warp][m] = v[m];
     }
     __syncthreads();
-    float r[11];
+    float r[12];
 #pragma unroll
-    for (int m = 0; m < 11; ++m) r[m] = s_red[0][m];
+    for (int m = 0; m < 12; ++m) r[m] = s_red[0][m];
     for (int w = 1; w < kWarps; ++w) {
 #pragma unroll
-        for (int m = 0; m < 11; ++m)
+        for (int m = 0; m < 12; ++m)
             r[m] = (m & 1) ? fmaxf(r[m], s_red[w][m]) : fminf(r[m], s_red[w][m]);
     }
     TileBounds tb;
     tb.x0 = r[0]; tb.x1 = r[1]; tb.y0 = r[2]; tb.y1 = r[3];
     tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
-    tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10];
+    tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10]; tb.w1 = r[11];
     return tb;
 }
 
@@ -299,6 +301,28 @@ __device__ __forceinline__ void block_max2(float a, float b, float (*s_red)[kRed
 // [the tile's least 10*WET, 1.1 R80].  Margins (1 % on sigma^2, 0.1 % on
 // it2) cover the kernels' FP32 and SFU arithmetic, so a skipped layer is
 // one whose every spot the per-spot cull would drop: the dose is the same.
+// An upper bound of the nuclear-halo sigma of layer_params (mm) over the
+// depths w0 <= w <= w1 (10*WET, mm): with the depth clamped to
+// [0.1, R80 - 0.1] as there, c_log log(w + 3) and -c_sh / (w - R80 - 5)^2
+// are monotone in w (w - R80 - 5 <= -5.1 < 0), so each is largest at an
+// end of the range; 0.06 w - 7.4e-5 w^2 is concave, largest at an end or
+// at its vertex.  INFINITY when the range is empty or not a number.
+__device__ __forceinline__ float halo_sigma_bound(float r80, float w0, float w1)
+{
+    const float top = r80 - 0.1f;
+    const float lo = fminf(fmaxf(w0, 0.1f), top), hi = fminf(fmaxf(w1, 0.1f), top);
+    if (!(lo <= hi)) return INFINITY;
+    const float cl = 0.0014f * r80, cs = 0.22f * r80;
+    const float l0 = cl * logf(lo + 3.0f), l1 = cl * logf(hi + 3.0f);
+    const float a0 = lo - r80 - 5.0f, a1 = hi - r80 - 5.0f;
+    const float q0 = -cs / (a0 * a0), q1 = -cs / (a1 * a1);
+    float p = fmaxf(0.06f * lo - 7.4e-5f * lo * lo, 0.06f * hi - 7.4e-5f * hi * hi);
+    const float wv = 0.06f / (2.0f * 7.4e-5f);
+    if (wv > lo && wv < hi) p = fmaxf(p, 0.06f * wv - 7.4e-5f * wv * wv);
+    const float b = 2.85f + fmaxf(l0, l1) + fmaxf(q0, q1) + p;
+    return b != b ? INFINITY : fmaxf(b, 0.0f) * 1.001f + 1e-3f;
+}
+
 __device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &tb,
                                            const PbBeam &B, float cut)
 {
@@ -330,7 +354,10 @@ __device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &t
         if (dv > dlo && dv < dhi) q = fmaxf(q, fabsf(fmaf(fmaf(ca, dv, cb), dv, cc)));
     }
     const float st = q + L.mcs_max;
-    const float sig2 = fmaf(L.sh_max, L.sh_max, st * st) * 1.01f + 1e-2f;
+    // the halo sigma over the tile's active depths (they are <= cut), or
+    // over every depth, whichever is smaller
+    const float shb = fminf(L.sh_max, halo_sigma_bound(L.r80, tb.w0, fminf(tb.w1, cut)));
+    const float sig2 = fmaf(shb, shb, st * st) * 1.01f + 1e-2f;
     const float e = r2 * it2 * ((0.5f * kLog2e) / sig2);
     return e >= kCullLog2;
 }
@@ -1147,8 +1174,8 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
         {
             // the beam's depth and source distance per voxel into shared
             // memory; the tile's box over its valid voxels
-            float v[11] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
-                           INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY};
+            float v[12] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
+                           INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
 #pragma unroll
             for (int q = 0; q < kLine; ++q) {
                 const float o = line_off(q);
@@ -1166,29 +1193,32 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                     v[8] = fminf(v[8], dd); v[9] = fmaxf(v[9], dd);
                     // the least depth over voxels that can be active; a NaN
                     // depth is never skipped
-                    if (!ADJ || wv[q] != 0.0f) v[10] = fminf(v[10], w == w ? w : -INFINITY);
+                    if (!ADJ || wv[q] != 0.0f) {
+                        v[10] = fminf(v[10], w == w ? w : -INFINITY);
+                        v[11] = fmaxf(v[11], w == w ? w : INFINITY);
+                    }
                 }
                 sh.w[q][t] = w;
                 sh.d[q][t] = dd;
             }
 #pragma unroll
-            for (int m = 0; m < 11; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
+            for (int m = 0; m < 12; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
             if (lane == 0) {
 #pragma unroll
-                for (int m = 0; m < 11; ++m) sh.red[warp][m] = v[m];
+                for (int m = 0; m < 12; ++m) sh.red[warp][m] = v[m];
             }
             __syncthreads();
-            float r[11];
+            float r[12];
 #pragma unroll
-            for (int m = 0; m < 11; ++m) r[m] = sh.red[0][m];
+            for (int m = 0; m < 12; ++m) r[m] = sh.red[0][m];
             for (int w = 1; w < kWarps; ++w) {
 #pragma unroll
-                for (int m = 0; m < 11; ++m)
+                for (int m = 0; m < 12; ++m)
                     r[m] = (m & 1) ? fmaxf(r[m], sh.red[w][m]) : fminf(r[m], sh.red[w][m]);
             }
             tb.x0 = r[0]; tb.x1 = r[1]; tb.y0 = r[2]; tb.y1 = r[3];
             tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
-            tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10];
+            tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10]; tb.w1 = r[11];
         }
         if constexpr (BEAM_OUT) {
 #pragma unroll
@@ -1513,13 +1543,13 @@ __device__ __forceinline__ void line_tile_coords(const PlanArgs &A, long long ti
     if (PB_TILE_ORDER == 0) {
         tx = rx;
         ty = ry;
-        tz = A.z0 / TZ + rz;
+        tz = rz;
         return;
     }
-    const int tz0 = A.z0 / TZ, ntz = (A.z1 + TZ - 1) / TZ - tz0;
+    const int ntz = (g.nz + TZ - 1) / TZ;
     tx = center_out(rx, nx8, min(max(A.centre[0] / kLine, 0), nx8 - 1));
     ty = center_out(ry, nty, min(max(A.centre[1] / TY, 0), nty - 1));
-    tz = tz0 + center_out(rz, ntz, min(max(A.centre[2] / TZ - tz0, 0), ntz - 1));
+    tz = center_out(rz, ntz, min(max(A.centre[2] / TZ, 0), ntz - 1));
 }
 
 template <int TY, int TZ, int KCULL, bool BEAM_OUT>
@@ -1946,8 +1976,6 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
     A.tiles_y = (g.ny + 7) / 8;
     A.tiles_z = (g.nz + 7) / 8;
     A.scale = scale;
-    A.z0 = 0;
-    A.z1 = g.nz;
     double c[3] = {0.0, 0.0, 0.0};
     for (int b = 0; b < n_beams; ++b) {
         A.beams[b] = beams[b];
@@ -1962,7 +1990,6 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
 
 
 int dose_variant_default() { return kDefaultDoseVariant; }
-int dose_slab_planes() { return kLineTZ; }
 int dose_variant_count() { return kNumDoseVariants; }
 
 static bool variant_line(int v)
@@ -1979,11 +2006,10 @@ static bool dose_variant_batch(int v)
     return v >= 0 && v < kNumDoseVariants && kDoseVariants[v].batch;
 }
 
-static unsigned line_tiles(const PbGrid &g, int ty, int tz, int z0 = 0, int z1 = -1)
+static unsigned line_tiles(const PbGrid &g, int ty, int tz)
 {
-    if (z1 < 0) z1 = g.nz;
     return (unsigned)((long long)((g.nx + kLine - 1) / kLine) * ((g.ny + ty - 1) / ty) *
-                      ((z1 + tz - 1) / tz - z0 / tz));
+                      ((g.nz + tz - 1) / tz));
 }
 
 template <int NT, int VPT, int KCULL>
@@ -1998,36 +2024,20 @@ template <int TY, int TZ, int KCULL>
 static void launch_line_t(const PlanArgs &A, const float *wet, const PbLayer *layers,
                           const float4 *geo, const float *mu, float *dose, cudaStream_t st)
 {
-    k_dose_line<TY, TZ, KCULL, false><<<line_tiles(A.g, TY, TZ, A.z0, A.z1), TY * TZ, 0, st>>>(
+    k_dose_line<TY, TZ, KCULL, false><<<line_tiles(A.g, TY, TZ), TY * TZ, 0, st>>>(
         A, wet, layers, geo, mu, dose, nullptr);
 }
 
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers, const float *geo,
                      const float *mu, float scale, float *dose, float *beam_dose,
-                     cudaStream_t st, int variant, int z0, int z1)
+                     cudaStream_t st, int variant)
 {
     PlanArgs A;
     fill_args(A, g, beams, n_beams, scale);
     const unsigned tiles = (unsigned)((int64_t)A.tiles_x * A.tiles_y * A.tiles_z);
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
     if (variant < 0) variant = kDefaultDoseVariant;
-    if (z0 != 0 || (z1 >= 0 && z1 != g.nz)) {
-        // a slab of planes: the default line shape only (the caller checks
-        // the bounds against its tile depth)
-        if (!variant_line(variant) || variant != kDefaultDoseVariant)
-            return set_error(PB_ERR_INVALID, "a slab needs the default line shape");
-        A.z0 = z0;
-        A.z1 = z1;
-        if (z0 >= z1) return PB_OK;
-        if (beam_dose)
-            k_dose_line<kLineTY, kLineTZ, kLineCull, true>
-                <<<line_tiles(g, kLineTY, kLineTZ, z0, z1), kLineTY * kLineTZ, 0, st>>>(
-                    A, wet, layers, g4, mu, dose, beam_dose);
-        else
-            launch_line_t<kLineTY, kLineTZ, kLineCull>(A, wet, layers, g4, mu, dose, st);
-        return check_launch("k_dose_line");
-    }
     if (beam_dose) {
         // per-beam output: the default shape of the variant's family only
         if (variant_line(variant))

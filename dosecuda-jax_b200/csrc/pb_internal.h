@@ -63,9 +63,7 @@ void texture_destroy(uint64_t h);
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers,
                      const float *geo, const float *mu, float scale,
-                     float *dose, float *beam_dose, cudaStream_t st, int variant = -1,
-                     int z0 = 0, int z1 = -1);
-int dose_slab_planes();
+                     float *dose, float *beam_dose, cudaStream_t st, int variant = -1);
 
 // variant < 0 selects the default forward shape (dose_variant_default);
 // the adjoint and the operation count use the kernel family of `variant`.

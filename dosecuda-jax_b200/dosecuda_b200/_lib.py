@@ -124,9 +124,6 @@ _SIGS = {
                              _VP]),
     "pb_dose_variant_count": (_I, []),
     "pb_dose_variant_default": (_I, []),
-    "pb_dose_slab": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, ctypes.c_float,
-                          _VP, _VP, _I, _I, _VP]),
-    "pb_dose_slab_planes": (_I, []),
     "pb_dose_adjoint_variant": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _F,
                                      _VP, _I, _VP]),
     "pb_dose_variant_name": (ctypes.c_char_p, [_I]),

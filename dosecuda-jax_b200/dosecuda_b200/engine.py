@@ -145,7 +145,11 @@ class DevicePlan:
     """A plan prepared on one GPU (see module docstring)."""
 
     def __init__(self, volume_shape, spacing: float, origin, beams: List[BeamSpec],
-                 device="cuda", texture_pool: Optional[TexturePool] = None):
+                 device="cuda", texture_pool: Optional[TexturePool] = None,
+                 defer_spots: bool = False):
+        """defer_spots: set up the beam geometry only (enough for the WET);
+        load_spots() then sorts the spots into layers and uploads them, for
+        instance on another stream while the WET runs."""
         self.device = require_cuda(device)
         if not beams:
             raise ValueError("a plan needs at least one beam")
@@ -159,15 +163,38 @@ class DevicePlan:
 
         self.geoms = (_lib.PbBeamGeom * self.n_beams)()
         self.tables: List[ModelTables] = []
+        for b, bs in enumerate(beams):
+            self.tables.append(model_tables(bs.model, self.device))
+            self.geoms[b] = _lib.beam_setup(bs.gantry_angle, bs.couch_angle, bs.model.VSADX,
+                                            bs.model.VSADY, bs.iso, origin)
+        self.wet: Optional[torch.Tensor] = None
+        self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # texture / cell-record handles: the plan's own, or a pool's
+        self._owns_textures = texture_pool is None
+        if texture_pool is None:
+            self._tex = ctypes.c_uint64(0)
+            self._cells = ctypes.c_uint64(0)
+        else:
+            self._tex = texture_pool.holder(self.device, self.shape, "texture")
+            self._cells = texture_pool.holder(self.device, self.shape, "cells")
+        self.wet_mode = "texture"
+        self._spec = beams
+        self.spots_loaded = False
+        if not defer_spots:
+            self.load_spots()
+
+    def load_spots(self) -> None:
+        """Spots sorted into energy layers, their geometry, the layer
+        records and their culling bounds, on the device (stream-ordered on
+        the current stream)."""
+        if self.spots_loaded:
+            return
         layer_blocks, geo_blocks, mu_blocks, perm_blocks = [], [], [], []
         self.spot_offsets = [0]
         self.layer_offsets = [0]
         self.n_layers: List[int] = []
-        for b, bs in enumerate(beams):
-            t = model_tables(bs.model, self.device)
-            self.tables.append(t)
-            self.geoms[b] = _lib.beam_setup(bs.gantry_angle, bs.couch_angle, bs.model.VSADX,
-                                            bs.model.VSADY, bs.iso, origin)
+        for b, bs in enumerate(self._spec):
+            t = self.tables[b]
             sl = np.ascontiguousarray(bs.spot_list, dtype=np.float32).reshape(-1, 4)
             spots, layers, perm = _lib.build_layers(sl, t.dvp_host)
             geo = _lib.spot_geometry(spots, self.geoms[b].vsadx, self.geoms[b].vsady)
@@ -212,17 +239,7 @@ class DevicePlan:
             check(_lib.lib.pb_layer_bounds(ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
                                            ptr(self.layers), ptr(self.spot_geo),
                                            _stream(self.device)), "pb_layer_bounds")
-        self.wet: Optional[torch.Tensor] = None
-        self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
-        # texture / cell-record handles: the plan's own, or a pool's
-        self._owns_textures = texture_pool is None
-        if texture_pool is None:
-            self._tex = ctypes.c_uint64(0)
-            self._cells = ctypes.c_uint64(0)
-        else:
-            self._tex = texture_pool.holder(self.device, self.shape, "texture")
-            self._cells = texture_pool.holder(self.device, self.shape, "cells")
-        self.wet_mode = "texture"
+        self.spots_loaded = True
 
     def __del__(self):
         if not getattr(self, "_owns_textures", True):
@@ -299,6 +316,8 @@ class DevicePlan:
         self.wet = wet.to(self.device).reshape(self.n_beams, self.n_vox).contiguous()
 
     def _need_wet(self):
+        if not self.spots_loaded:
+            raise RuntimeError("the plan's spots are not loaded (load_spots)")
         if self.wet is None:
             raise RuntimeError("WET has not been computed for this plan")
 
@@ -320,32 +339,6 @@ class DevicePlan:
                                ptr(mu), float(scale), ptr(dose), ptr(bd),
                                _stream(self.device)), "pb_dose")
         return (dose, bd) if beam_doses else dose
-
-    def forward_slab(self, z_begin: int, z_end: int, dose: torch.Tensor,
-                     beam_doses: Optional[torch.Tensor] = None,
-                     mu_sorted: Optional[torch.Tensor] = None, scale: float = 1.0) -> None:
-        """The forward of the voxel planes z_begin <= z < z_end only, into
-        `dose` (V) and, if given, `beam_doses` (n_beams x V); other planes
-        are left as they are (pb_dose_slab).  The bounds are multiples of
-        slab_planes() or nz."""
-        self._need_wet()
-        mu = (self.mu_sorted if mu_sorted is None else mu_sorted).contiguous()
-        if mu.dtype != torch.float32 or mu.numel() != self.n_spots:
-            raise ValueError("mu must be float32 with one entry per spot")
-        for t, n in ((dose, self.n_vox), (beam_doses, self.n_beams * self.n_vox)):
-            if t is not None and (t.dtype != torch.float32 or t.numel() != n or
-                                  not t.is_contiguous() or t.device != self.device):
-                raise ValueError("dose buffers must be contiguous float32 on the plan's device")
-        check(_lib.lib.pb_dose_slab(ctypes.byref(self.grid),
-                                    ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
-                                    ptr(self.wet), ptr(self.layers), ptr(self.spot_geo), ptr(mu),
-                                    float(scale), ptr(dose), ptr(beam_doses), int(z_begin),
-                                    int(z_end), _stream(self.device)), "pb_dose_slab")
-
-    @staticmethod
-    def slab_planes() -> int:
-        """Plane multiple that forward_slab's bounds take."""
-        return int(_lib.lib.pb_dose_slab_planes())
 
     def forward_variant(self, variant: int, mu_sorted: Optional[torch.Tensor] = None,
                         scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:

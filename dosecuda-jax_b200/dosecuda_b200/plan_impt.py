@@ -119,13 +119,6 @@ def _pinned_copy(t: torch.Tensor) -> torch.Tensor:
     return h
 
 
-def _slabs(nz: int, step: int, n: int = 4):
-    """About n slabs of z planes, bounds multiples of `step` (the last ends
-    at nz)."""
-    size = max(step, -(-nz // n // step) * step)
-    return [(z, min(z + size, nz)) for z in range(0, nz, size)]
-
-
 def _beam_model(plan, beam):
     try:
         model_index = list(plan.dicom_rangeshifter_label.astype(str)).index(
@@ -161,7 +154,9 @@ class IMPTDoseGrid(DoseGrid):
                             "resampling CT")
 
     def _rlsp_device(self, machine_name, device):
-        hu = torch.from_numpy(np.ascontiguousarray(self.HU, dtype=np.single)).to(device)
+        # an HU array in page-locked memory goes up asynchronously
+        hu_h = torch.from_numpy(np.ascontiguousarray(self.HU, dtype=np.single))
+        hu = hu_h.to(device, non_blocking=hu_h.is_pinned())
         xh, yh = _hu_curve(machine_name)
         rlsp = _engine().rlsp_from_hu(hu, xh, yh)
         self._device_rlsp = rlsp
@@ -245,27 +240,23 @@ class IMPTDoseGrid(DoseGrid):
         chunks = self._beam_chunks(plan)
         total, beams_h, keep = None, [], []
         if len(chunks) == 1:
-            # one launch per slab of z planes; each slab's planes go back to
-            # the host on the copy stream while the next slab computes
-            dp = self._transient(plan, gpu_id, chunks[0], wet_mode, rlsp)
-            V, nb = dp.n_vox, dp.n_beams
-            dose = torch.empty(V, dtype=torch.float32, device=device)
-            bd = torch.empty((nb, V), dtype=torch.float32, device=device)
-            dose_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
-            bd_h = torch.empty((nb, V), dtype=torch.float32, pin_memory=True)
-            plane = shape[1] * shape[2]
-            for z0, z1 in _slabs(shape[0], dp.slab_planes()):
-                dp.forward_slab(z0, z1, dose, bd, scale=float(plan.n_fractions))
-                done = torch.cuda.Event()
-                done.record(main)
-                side.wait_event(done)
-                lo, hi = z0 * plane, z1 * plane
-                with torch.cuda.stream(side):
-                    dose_h[lo:hi].copy_(dose[lo:hi], non_blocking=True)
-                    for b in range(nb):
-                        bd_h[b, lo:hi].copy_(bd[b, lo:hi], non_blocking=True)
-            beams_h.append((bd_h, nb))
-            keep += [dose, bd]
+            # the WET is queued first; the spots are sorted into layers and
+            # uploaded on the copy stream while it runs
+            pool = self.__dict__.get("_pb_texture_pool")
+            if pool is None:
+                pool = self._pb_texture_pool = _engine().TexturePool()
+            dp = _engine().DevicePlan(shape, float(self.spacing[0]),
+                                      np.asarray(self.origin, dtype=np.single),
+                                      self._specs(plan, chunks[0]), device, texture_pool=pool,
+                                      defer_spots=True)
+            dp.compute_wet(rlsp.reshape(-1), check_status=False, wet_mode=wet_mode)
+            with torch.cuda.stream(side):
+                dp.load_spots()
+            main.wait_stream(side)
+            dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
+            beams_h.append((_pinned_copy(bd), dp.n_beams))
+            dose_h = _pinned_copy(dose)
+            keep += [dose, bd, dp]
         else:
             for chunk in chunks:
                 dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
@@ -276,6 +267,9 @@ class IMPTDoseGrid(DoseGrid):
             dose_h = _pinned_copy(total)
         main.synchronize()
         side.synchronize()
+        if len(chunks) == 1 and int(dp._status.item()) & _engine()._lib.PB_ERR_RAY_CAP:
+            raise _engine()._lib.PbError(_engine()._lib.PB_ERR_RAY_CAP,
+                                         "a WET ray reached its step cap")
         for bd_h, n in beams_h:
             arr = bd_h.numpy()
             self.beam_doses += [arr[b].reshape(shape) for b in range(n)]

@@ -337,20 +337,6 @@ PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
 PbStatus pb_batch_run(const PbBatchInfo *info, void *work_dev, int flags, int variant,
                       int blocks_per_sm, int *status_dev, void *stream);
 
-/* pb_dose over the voxel planes z_begin <= z < z_end only: the dose (and,
- * with beam_dose_dev, every beam's dose) of those planes is written and
- * the other planes are left as they are; each plane gets the same bits as
- * from pb_dose.  The bounds are multiples of pb_dose_slab_planes() (the
- * default shape's tile depth), z_end may also be nz; z_begin == z_end does
- * nothing.  A caller copies the planes of one slab back to the host while
- * the next slab computes.  No counterpart in the reference. */
-PbStatus pb_dose_slab(const PbGrid *grid, const PbBeam *beams, int n_beams,
-                      const float *wet_dev, const PbLayer *layers_dev,
-                      const float *spot_geo_dev, const float *mu_dev, float scale,
-                      float *dose_dev, float *beam_dose_dev, int z_begin, int z_end,
-                      void *stream);
-int pb_dose_slab_planes(void);
-
 /* Adjoint of pb_dose: grad_dev[s] = scale * sum_v dobj_dose_dev[v] * K(v,s)
  * for every spot s, where K(v,s) is the dose per unit weight of spot s at
  * voxel v.  Matrix-free: footprints are recomputed.  grad_dev is

@@ -505,38 +505,6 @@ def test_layer_bounds_change_no_result(pkg, small, which):
     assert torch.allclose(g1, g2, rtol=1e-5, atol=1e-6 * float(g1.abs().max()))
 
 
-def test_dose_slabs_equal_the_whole_forward(small):
-    """pb_dose_slab: slabs of z planes written one by one give the whole
-    forward's dose and per-beam doses bit for bit; planes outside a slab
-    are left alone; bounds off the tile depth are rejected."""
-    from dosecuda_b200 import _lib
-    from dosecuda_b200.plan_impt import _slabs
-    dp = small.grid.prepareIMPTPlan(small.plan, 0)
-    d_all, bd_all = dp.forward(scale=2.0, beam_doses=True)
-    nz = small.grid.HU.shape[0]
-    step = dp.slab_planes()
-    assert step in (4, 8, 16)
-    for n in (1, 2, 3, 5):
-        dose = torch.full((dp.n_vox,), -1.0, device=DEV)
-        bd = torch.full((dp.n_beams, dp.n_vox), -1.0, device=DEV)
-        slabs = _slabs(nz, step, n)
-        for z0, z1 in slabs[1:]:
-            dp.forward_slab(z0, z1, dose, bd, scale=2.0)
-        plane = dp.n_vox // nz
-        z0, z1 = slabs[0]
-        assert bool((dose[: z1 * plane] == -1.0).all())      # not written yet
-        dp.forward_slab(z0, z1, dose, bd, scale=2.0)
-        assert torch.equal(dose, d_all) and torch.equal(bd, bd_all)
-        d_only = torch.full((dp.n_vox,), -1.0, device=DEV)
-        dp.forward_slab(z0, z1, d_only, scale=2.0)            # dose alone
-        assert torch.equal(d_only[: z1 * plane], d_all[: z1 * plane])
-    with pytest.raises(_lib.PbError, match="multiples"):
-        dp.forward_slab(1, nz, dose, bd)
-    with pytest.raises(_lib.PbError, match="outside"):
-        dp.forward_slab(0, nz + step, dose, bd)
-    dp.forward_slab(step, step, dose, bd)                      # empty: nothing
-
-
 def test_adjoint_counts_follow_its_tile_skip(small):
     """pb_count_evaluated_adjoint: on a field nonzero everywhere it counts
     the forward's work; on a zero field nothing; on a field nonzero in one
