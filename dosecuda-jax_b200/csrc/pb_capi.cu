@@ -74,7 +74,8 @@ static PbStatus check_grid(const PbGrid *g)
 }
 
 static PbStatus check_beams(const PbGrid *g, const PbBeam *beams, int n_beams,
-                            const float *wet, const PbLayer *layers, const float *geo)
+                            const float *wet, const PbLayer *layers, const float *geo,
+                            bool need_geo = true)
 {
     PbStatus s = check_grid(g);
     if (s != PB_OK) return s;
@@ -87,7 +88,8 @@ static PbStatus check_beams(const PbGrid *g, const PbBeam *beams, int n_beams,
         if (B.n_layers < 0 || B.layer_start < 0 || B.spot_start < 0 || B.n_spots < 0)
             return set_error(PB_ERR_INVALID, "beam %d: negative layer/spot range", b);
         if (B.n_layers == 0) continue;
-        if (!layers || !geo) return set_error(PB_ERR_INVALID, "layers/spot geometry is NULL");
+        if (!layers || (need_geo && !geo))
+            return set_error(PB_ERR_INVALID, "layers/spot geometry is NULL");
         if (!B.dvp_dev || !B.depths_dev || !B.sigmas_dev || !B.idds_dev)
             return set_error(PB_ERR_INVALID, "beam %d: model table is NULL", b);
         if (B.lut_len <= 0 || B.lut_len > PB_MAX_LUT_LEN)
@@ -313,6 +315,60 @@ PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams, const flo
     }
     return launch_dose(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev, mu_dev, scale,
                        dose_dev, beam_dose_dev, static_cast<cudaStream_t>(stream));
+}
+
+long long pb_tile_order_count(const PbGrid *grid)
+{
+    return check_grid(grid) == PB_OK ? tile_order_count(*grid) : -1;
+}
+
+size_t pb_tile_order_work_size(const PbGrid *grid)
+{
+    return check_grid(grid) == PB_OK ? tile_order_work_size(*grid) : 0;
+}
+
+PbStatus pb_tile_order(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                       const float *wet_dev, const PbLayer *layers_dev, void *work_dev,
+                       int *order_dev, void *stream)
+{
+    // the order reads the layers and the model tables, not the spots
+    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, nullptr, false);
+    if (s != PB_OK) return s;
+    if (!work_dev || !order_dev) return set_error(PB_ERR_INVALID, "work or order is NULL");
+    return launch_tile_order(*grid, beams, n_beams, wet_dev, layers_dev, work_dev, order_dev,
+                             static_cast<cudaStream_t>(stream));
+}
+
+PbStatus pb_dose_ordered(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                         const float *wet_dev, const PbLayer *layers_dev,
+                         const float *spot_geo_dev, const float *mu_dev, float scale,
+                         float *dose_dev, float *beam_dose_dev, const int *order_dev,
+                         void *stream)
+{
+    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev);
+    if (s != PB_OK) return s;
+    if (!dose_dev) return set_error(PB_ERR_INVALID, "dose is NULL");
+    if (!mu_dev) {
+        for (int b = 0; b < n_beams; ++b)
+            if (beams[b].n_layers) return set_error(PB_ERR_INVALID, "mu is NULL");
+    }
+    return launch_dose(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev, mu_dev, scale,
+                       dose_dev, beam_dose_dev, static_cast<cudaStream_t>(stream), -1,
+                       order_dev);
+}
+
+PbStatus pb_dose_adjoint_ordered(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                 const float *wet_dev, const PbLayer *layers_dev,
+                                 const float *spot_geo_dev, const float *dobj_dose_dev,
+                                 float scale, float *grad_dev, const int *order_dev,
+                                 void *stream)
+{
+    PbStatus s = check_beams(grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev);
+    if (s != PB_OK) return s;
+    if (!dobj_dose_dev || !grad_dev) return set_error(PB_ERR_INVALID, "NULL argument");
+    return launch_adjoint(*grid, beams, n_beams, wet_dev, layers_dev, spot_geo_dev,
+                          dobj_dose_dev, scale, grad_dev, static_cast<cudaStream_t>(stream), -1,
+                          order_dev);
 }
 
 PbStatus pb_dose_adjoint(const PbGrid *grid, const PbBeam *beams, int n_beams,

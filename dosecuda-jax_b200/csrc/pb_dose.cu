@@ -34,6 +34,7 @@
 // over a thread's voxels meet across the warp with a transposed butterfly,
 // across the block in shared memory, and go to the gradient with one global
 // atomic per spot per (tile, layer).
+#include <climits>
 #include <type_traits>
 #include "pb_internal.h"
 
@@ -46,6 +47,7 @@ struct PlanArgs {
     int n_beams;
     int tiles_x, tiles_y, tiles_z;
     int centre[3];   // voxel holding the mean isocentre (clamped to the grid)
+    const int *order;   // line-tile launches: tile of each block (raster index), or NULL
     float scale;
     PbBeam beams[PB_MAX_BEAMS];
 };
@@ -323,25 +325,33 @@ __device__ __forceinline__ float halo_sigma_bound(float r80, float w0, float w1)
     return b != b ? INFINITY : fmaxf(b, 0.0f) * 1.001f + 1e-3f;
 }
 
-__device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &tb,
-                                           const PbBeam &B, float cut)
+// The layer's spot box (at the isocentre plane) scaled to the tile's depth
+// range by the divergence factors: the box every spot's axis crosses the
+// tile in.
+__device__ __forceinline__ void layer_box(const PbLayer &L, const TileBounds &tb, float &pxl,
+                                          float &pxh, float &pyl, float &pyh)
 {
-    if (!L.bound_ok) return false;
     const float a0 = L.sx0 * tb.gx0, a1 = L.sx0 * tb.gx1, a2 = L.sx1 * tb.gx0,
                 a3 = L.sx1 * tb.gx1;
     const float b0 = L.sy0 * tb.gy0, b1 = L.sy0 * tb.gy1, b2 = L.sy1 * tb.gy0,
                 b3 = L.sy1 * tb.gy1;
-    const float pxl = fminf(fminf(a0, a1), fminf(a2, a3));
-    const float pxh = fmaxf(fmaxf(a0, a1), fmaxf(a2, a3));
-    const float pyl = fminf(fminf(b0, b1), fminf(b2, b3));
-    const float pyh = fmaxf(fmaxf(b0, b1), fmaxf(b2, b3));
-    const float dx = fmaxf(0.0f, fmaxf(tb.x0 - pxh, pxl - tb.x1));
-    const float dy = fmaxf(0.0f, fmaxf(tb.y0 - pyh, pyl - tb.y1));
-    const float r2 = dx * dx + dy * dy;
-    if (!(r2 > 0.0f)) return false;
+    pxl = fminf(fminf(a0, a1), fminf(a2, a3));
+    pxh = fmaxf(fmaxf(a0, a1), fmaxf(a2, a3));
+    pyl = fminf(fminf(b0, b1), fminf(b2, b3));
+    pyh = fmaxf(fmaxf(b0, b1), fmaxf(b2, b3));
+}
+
+// A lower bound of 1/|t|^2 over the layer's spots (it2) and an upper bound
+// of the widest Gaussian's sigma^2 at the tile (sig2): sigma in air over
+// the tile's source-distance range plus the LUT's largest |sigma_mcs|, and
+// the halo sigma over the tile's active depths (or over every depth,
+// whichever is smaller).  False when no bound applies (NaN, empty tile).
+__device__ __forceinline__ bool layer_sig2(const PbLayer &L, const TileBounds &tb,
+                                           const PbBeam &B, float cut, float &it2, float &sig2)
+{
     const float mx = fmaxf(L.sx0 * L.sx0, L.sx1 * L.sx1) / (B.geom.vsadx * B.geom.vsadx);
     const float my = fmaxf(L.sy0 * L.sy0, L.sy1 * L.sy1) / (B.geom.vsady * B.geom.vsady);
-    const float it2 = 0.999f / (1.0f + mx + my);
+    it2 = 0.999f / (1.0f + mx + my);
     const float *cabc = B.dvp_dev + (size_t)B.dvp_len * L.energy_id + 2;
     const float ca = __ldg(cabc), cb = __ldg(cabc + 1), cc = __ldg(cabc + 2);
     const float off = 0.7f * L.r80;
@@ -354,10 +364,23 @@ __device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &t
         if (dv > dlo && dv < dhi) q = fmaxf(q, fabsf(fmaf(fmaf(ca, dv, cb), dv, cc)));
     }
     const float st = q + L.mcs_max;
-    // the halo sigma over the tile's active depths (they are <= cut), or
-    // over every depth, whichever is smaller
     const float shb = fminf(L.sh_max, halo_sigma_bound(L.r80, tb.w0, fminf(tb.w1, cut)));
-    const float sig2 = fmaf(shb, shb, st * st) * 1.01f + 1e-2f;
+    sig2 = fmaf(shb, shb, st * st) * 1.01f + 1e-2f;
+    return true;
+}
+
+__device__ __forceinline__ bool layer_skip(const PbLayer &L, const TileBounds &tb,
+                                           const PbBeam &B, float cut)
+{
+    if (!L.bound_ok) return false;
+    float pxl, pxh, pyl, pyh;
+    layer_box(L, tb, pxl, pxh, pyl, pyh);
+    const float dx = fmaxf(0.0f, fmaxf(tb.x0 - pxh, pxl - tb.x1));
+    const float dy = fmaxf(0.0f, fmaxf(tb.y0 - pyh, pyl - tb.y1));
+    const float r2 = dx * dx + dy * dy;
+    if (!(r2 > 0.0f)) return false;
+    float it2, sig2;
+    if (!layer_sig2(L, tb, B, cut, it2, sig2)) return false;
     const float e = r2 * it2 * ((0.5f * kLog2e) / sig2);
     return e >= kCullLog2;
 }
@@ -1530,12 +1553,25 @@ __device__ __forceinline__ int center_out(int r, int n, int c)
 // the plan's centre (the mean isocentre) outward, z slabs first: the tiles
 // most beams cross, the longest ones, start early and the launch does not
 // end on a few of them while the other SMs idle.
+//
+// With A.order (pb_tile_order: the tiles by estimated cost, most expensive
+// first) block b takes tile A.order[b] instead; an entry outside the grid's
+// tiles makes the block return (false) without touching anything.
 template <int TY, int TZ>
-__device__ __forceinline__ void line_tile_coords(const PlanArgs &A, long long tile, int &tx,
+__device__ __forceinline__ bool line_tile_coords(const PlanArgs &A, long long tile, int &tx,
                                                  int &ty, int &tz)
 {
     const PbGrid &g = A.g;
     const int nx8 = (g.nx + kLine - 1) / kLine, nty = (g.ny + TY - 1) / TY;
+    const int ntz = (g.nz + TZ - 1) / TZ;
+    if (A.order != nullptr) {
+        const long long o = A.order[tile];
+        if (o < 0 || o >= (long long)nx8 * nty * ntz) return false;
+        tx = (int)(o % nx8);
+        ty = (int)((o / nx8) % nty);
+        tz = (int)(o / ((long long)nx8 * nty));
+        return true;
+    }
     const int rx = (int)(tile % nx8);
     tile /= nx8;
     const int ry = (int)(tile % nty);
@@ -1544,12 +1580,12 @@ __device__ __forceinline__ void line_tile_coords(const PlanArgs &A, long long ti
         tx = rx;
         ty = ry;
         tz = rz;
-        return;
+        return true;
     }
-    const int ntz = (g.nz + TZ - 1) / TZ;
     tx = center_out(rx, nx8, min(max(A.centre[0] / kLine, 0), nx8 - 1));
     ty = center_out(ry, nty, min(max(A.centre[1] / TY, 0), nty - 1));
     tz = center_out(rz, ntz, min(max(A.centre[2] / TZ, 0), ntz - 1));
+    return true;
 }
 
 template <int TY, int TZ, int KCULL, bool BEAM_OUT>
@@ -1561,7 +1597,7 @@ k_dose_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
 {
     __shared__ LineShared<TY * TZ, KCULL, BEAM_OUT> sh;
     int tx, ty, tz;
-    line_tile_coords<TY, TZ>(A, blockIdx.x, tx, ty, tz);
+    if (!line_tile_coords<TY, TZ>(A, blockIdx.x, tx, ty, tz)) return;
     line_tile<TY, TZ, KCULL, BEAM_OUT>(A, tx, ty, tz, wet, layers, geo, mu, dose, beam_dose, sh);
 }
 
@@ -1612,7 +1648,7 @@ k_dose_count_line(const __grid_constant__ PlanArgs A, const float *__restrict__ 
 {
     __shared__ LineShared<kLineTY * kLineTZ, kLineCull, false, false> sh;
     int tx, ty, tz;
-    line_tile_coords<kLineTY, kLineTZ>(A, blockIdx.x, tx, ty, tz);
+    if (!line_tile_coords<kLineTY, kLineTZ>(A, blockIdx.x, tx, ty, tz)) return;
     line_tile<kLineTY, kLineTZ, kLineCull, false, kModeCount>(A, tx, ty, tz, wet, layers, geo,
                                                               nullptr, nullptr, nullptr, sh,
                                                               count, wfield);
@@ -1625,10 +1661,179 @@ k_adjoint_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet
 {
     __shared__ LineShared<kLineTY * kLineTZ, kLineCull, false, false> sh;
     int tx, ty, tz;
-    line_tile_coords<kLineTY, kLineTZ>(A, blockIdx.x, tx, ty, tz);
+    if (!line_tile_coords<kLineTY, kLineTZ>(A, blockIdx.x, tx, ty, tz)) return;
     line_tile<kLineTY, kLineTZ, kLineCull, false, kModeAdjoint>(A, tx, ty, tz, wet, layers, geo,
                                                                 nullptr, nullptr, nullptr, sh,
                                                                 nullptr, wfield, grad);
+}
+
+// ------------------------------------------------------------ tile order
+//
+// The line tiles' work spans more than two orders of magnitude (tens of us
+// for a tile no spot reaches, milliseconds for one that every beam crosses
+// near the target), and blocks start in launch order, so a launch whose
+// longest tiles start late ends on a few of them.  k_tile_cost estimates each
+// tile's cost and k_order_* sort the tiles by it, most expensive first (a
+// bucket sort on log2 of the cost); the forward and the adjoint then take
+// their tiles in that order (PlanArgs::order).  The order changes when the
+// work is done, not what each tile computes.
+
+// Cost units: one spot evaluated over a tile; a kept (tile, layer) pair
+// also pays its per-voxel Gaussian parameters and the cull, about this many.
+constexpr float kPairCost = 24.0f;
+constexpr int kOrderBuckets = 1024;
+
+// Estimated work of a kept (tile, layer) pair: kPairCost plus the layer's
+// spots times the fraction of its spot box, scaled to the tile's depth, that
+// lies within the cull radius of the tile's box (from the same sigma bound
+// as the layer skip); 0 for a pair the dose kernels do not keep.
+__device__ __forceinline__ float layer_pair_cost(const PbLayer &L, const TileBounds &tb,
+                                                 const PbBeam &B)
+{
+    const float cut = __fmul_rn(1.1f, L.r80);
+    if (!(L.n_spots > 0 && tb.w0 <= cut) || layer_skip(L, tb, B, cut)) return 0.0f;
+    float frac = 1.0f;
+    float pxl, pxh, pyl, pyh, it2, sig2;
+    if (L.bound_ok && layer_sig2(L, tb, B, cut, it2, sig2)) {
+        layer_box(L, tb, pxl, pxh, pyl, pyh);
+        const float R = sqrtf(kCullLog2 * sig2 / ((0.5f * kLog2e) * it2));
+        auto part = [](float lo, float hi, float a, float b) {
+            const float ov = fminf(hi, b) - fmaxf(lo, a);
+            const float len = hi - lo;
+            if (!(ov > 0.0f)) return 0.0f;
+            return len > 1e-3f ? fminf(ov / len, 1.0f) : 1.0f;
+        };
+        frac = part(pxl, pxh, tb.x0 - R, tb.x1 + R) * part(pyl, pyh, tb.y0 - R, tb.y1 + R);
+    }
+    return kPairCost + (float)L.n_spots * frac;
+}
+
+// One block per line tile (raster index: x fastest): its box and depth
+// range per beam as line_tile forms them, then the estimated cost of every
+// layer pair it keeps.
+template <int TY, int TZ>
+__global__ void __launch_bounds__(TY * TZ)
+k_tile_cost(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
+            const PbLayer *__restrict__ layers, float *__restrict__ cost)
+{
+    constexpr int NT = TY * TZ, kWarps = NT / 32;
+    __shared__ float s_red[kWarps][kRedSlots];
+    __shared__ float s_cost[kWarps];
+    const int nx8 = (A.g.nx + kLine - 1) / kLine, nty = (A.g.ny + TY - 1) / TY;
+    const long long tile = blockIdx.x;
+    const int tx = (int)(tile % nx8), ty = (int)((tile / nx8) % nty);
+    const int tz = (int)(tile / ((long long)nx8 * nty));
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int i0 = tx * kLine, j = ty * TY + t % TY, k = tz * TZ + t / TY;
+    const int nvalid = (j < A.g.ny && k < A.g.nz) ? min(kLine, A.g.nx - i0) : 0;
+    const int64_t vbase = i0 + (int64_t)A.g.nx * (j + (int64_t)A.g.ny * k);
+    const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
+    float c = 0.0f;
+    for (int b = 0; b < A.n_beams; ++b) {
+        const PbBeam &B = A.beams[b];
+        float dX, dY, dZ;
+        image_to_head(B.geom, A.g.spacing, 0.0f, 0.0f, dX, dY, dZ);
+        const float dgx = -__fdiv_rn(dZ, B.geom.vsadx), dgy = -__fdiv_rn(dZ, B.geom.vsady);
+        float Xc, Yc, Zc;
+        {
+            float px, py, pz, X0, Y0, Z0;
+            vox_mm(B.geom, A.g.spacing, i0, j, k, px, py, pz);
+            image_to_head(B.geom, px, py, pz, X0, Y0, Z0);
+            Xc = __fmaf_rn(3.5f, dX, X0);
+            Yc = __fmaf_rn(3.5f, dY, Y0);
+            Zc = __fmaf_rn(3.5f, dZ, Z0);
+        }
+        const float gxc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsadx));
+        const float gyc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsady));
+        float v[12] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
+                       INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
+#pragma unroll
+        for (int q = 0; q < kLine; ++q) {
+            if (q >= nvalid) continue;
+            const float o = line_off(q);
+            const float X = __fmaf_rn(o, dX, Xc), Y = __fmaf_rn(o, dY, Yc);
+            const float Z = __fmaf_rn(o, dZ, Zc);
+            const float w = __fmul_rn(__ldg(wet + b * V + vbase + q), 10.0f);
+            const float dd = source_distance(B, X, Y, Z);
+            const float GX = __fmaf_rn(o, dgx, gxc), GY = __fmaf_rn(o, dgy, gyc);
+            v[0] = fminf(v[0], X);  v[1] = fmaxf(v[1], X);
+            v[2] = fminf(v[2], Y);  v[3] = fmaxf(v[3], Y);
+            v[4] = fminf(v[4], GX); v[5] = fmaxf(v[5], GX);
+            v[6] = fminf(v[6], GY); v[7] = fmaxf(v[7], GY);
+            v[8] = fminf(v[8], dd); v[9] = fmaxf(v[9], dd);
+            v[10] = fminf(v[10], w == w ? w : -INFINITY);
+            v[11] = fmaxf(v[11], w == w ? w : INFINITY);
+        }
+#pragma unroll
+        for (int m = 0; m < 12; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
+        if (lane == 0) {
+#pragma unroll
+            for (int m = 0; m < 12; ++m) s_red[warp][m] = v[m];
+        }
+        __syncthreads();
+        float r[12];
+#pragma unroll
+        for (int m = 0; m < 12; ++m) r[m] = s_red[0][m];
+        for (int w = 1; w < kWarps; ++w) {
+#pragma unroll
+            for (int m = 0; m < 12; ++m)
+                r[m] = (m & 1) ? fmaxf(r[m], s_red[w][m]) : fminf(r[m], s_red[w][m]);
+        }
+        TileBounds tb;
+        tb.x0 = r[0]; tb.x1 = r[1]; tb.y0 = r[2]; tb.y1 = r[3];
+        tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
+        tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10]; tb.w1 = r[11];
+        for (int l = t; l < B.n_layers; l += NT)
+            c += layer_pair_cost(layers[B.layer_start + l], tb, B);
+        __syncthreads();   // s_red is rewritten by the next beam
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) s_cost[warp] = c;
+    __syncthreads();
+    if (t == 0) {
+        float total = 0.0f;
+        for (int w = 0; w < kWarps; ++w) total += s_cost[w];
+        cost[tile] = total;
+    }
+}
+
+// Bucket of a cost, most expensive last: 32 buckets per octave.
+__device__ __forceinline__ int order_bucket(float c)
+{
+    const float x = log2f(1.0f + fmaxf(c, 0.0f)) * 32.0f;
+    return x < (float)(kOrderBuckets - 1) ? (int)x : kOrderBuckets - 1;
+}
+
+__global__ void k_order_hist(const float *__restrict__ cost, int n, int *__restrict__ hist)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(hist + order_bucket(cost[i]), 1);
+}
+
+// Start of each bucket in the order, the most expensive bucket first (one
+// block of kOrderBuckets threads; the counts are replaced by the starts).
+__global__ void __launch_bounds__(kOrderBuckets) k_order_scan(int *hist)
+{
+    __shared__ int s[kOrderBuckets];
+    const int t = threadIdx.x;
+    s[t] = hist[kOrderBuckets - 1 - t];   // descending cost
+    __syncthreads();
+    for (int off = 1; off < kOrderBuckets; off <<= 1) {
+        const int add = t >= off ? s[t - off] : 0;
+        __syncthreads();
+        s[t] += add;
+        __syncthreads();
+    }
+    // exclusive start of bucket (kOrderBuckets - 1 - t)
+    hist[kOrderBuckets - 1 - t] = t > 0 ? s[t - 1] : 0;
+}
+
+__global__ void k_order_scatter(const float *__restrict__ cost, int n, int *__restrict__ start,
+                                int *__restrict__ order)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) order[atomicAdd(start + order_bucket(cost[i]), 1)] = i;
 }
 
 #ifndef PB_DOSE_MIN_BLOCKS
@@ -1976,6 +2181,7 @@ static void fill_args(PlanArgs &A, const PbGrid &g, const PbBeam *beams, int n_b
     A.tiles_y = (g.ny + 7) / 8;
     A.tiles_z = (g.nz + 7) / 8;
     A.scale = scale;
+    A.order = nullptr;
     double c[3] = {0.0, 0.0, 0.0};
     for (int b = 0; b < n_beams; ++b) {
         A.beams[b] = beams[b];
@@ -2031,13 +2237,15 @@ static void launch_line_t(const PlanArgs &A, const float *wet, const PbLayer *la
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers, const float *geo,
                      const float *mu, float scale, float *dose, float *beam_dose,
-                     cudaStream_t st, int variant)
+                     cudaStream_t st, int variant, const int *order)
 {
     PlanArgs A;
     fill_args(A, g, beams, n_beams, scale);
     const unsigned tiles = (unsigned)((int64_t)A.tiles_x * A.tiles_y * A.tiles_z);
     const float4 *g4 = reinterpret_cast<const float4 *>(geo);
     if (variant < 0) variant = kDefaultDoseVariant;
+    // a tile order (pb_tile_order) is for the line-tile shape of the default
+    A.order = (variant_line(variant) && (beam_dose || variant == kLineShape)) ? order : nullptr;
     if (beam_dose) {
         // per-beam output: the default shape of the variant's family only
         if (variant_line(variant))
@@ -2118,10 +2326,11 @@ int dose_variant_threads(int variant)
 PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                         const float *wet, const PbLayer *layers, const float *geo,
                         const float *w, float scale, float *grad, cudaStream_t st,
-                        int variant)
+                        int variant, const int *order)
 {
     PlanArgs A;
     fill_args(A, g, beams, n_beams, scale);
+    A.order = variant_line(variant) ? order : nullptr;
     int total_spots = 0;
     for (int b = 0; b < n_beams; ++b) {
         const int e = beams[b].spot_start + beams[b].n_spots;
@@ -2193,6 +2402,38 @@ PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
     k_layer_bounds<<<dim3((unsigned)max_layers, (unsigned)n_beams), kBoundThreads, 0, st>>>(
         A, layers, reinterpret_cast<const float4 *>(geo));
     return check_launch("k_layer_bounds");
+}
+
+long long tile_order_count(const PbGrid &g) { return line_tiles(g, kLineTY, kLineTZ); }
+
+size_t tile_order_work_size(const PbGrid &g)
+{
+    const size_t n = (size_t)tile_order_count(g);
+    return ((n * sizeof(float) + 255) / 256) * 256 + kOrderBuckets * sizeof(int);
+}
+
+PbStatus launch_tile_order(const PbGrid &g, const PbBeam *beams, int n_beams, const float *wet,
+                           const PbLayer *layers, void *work, int *order, cudaStream_t st)
+{
+    PlanArgs A;
+    fill_args(A, g, beams, n_beams, 1.0f);
+    const long long n = tile_order_count(g);
+    if (n <= 0) return PB_OK;
+    if (n > (long long)INT_MAX) return set_error(PB_ERR_INVALID, "too many tiles for an order");
+    float *cost = static_cast<float *>(work);
+    int *hist = reinterpret_cast<int *>(static_cast<char *>(work) +
+                                        ((size_t)n * sizeof(float) + 255) / 256 * 256);
+    PbStatus s = check_cuda(cudaMemsetAsync(hist, 0, kOrderBuckets * sizeof(int), st),
+                            "cudaMemsetAsync(order buckets)");
+    if (s != PB_OK) return s;
+    k_tile_cost<kLineTY, kLineTZ><<<(unsigned)n, kLineTY * kLineTZ, 0, st>>>(A, wet, layers, cost);
+    s = check_launch("k_tile_cost");
+    if (s != PB_OK) return s;
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    k_order_hist<<<blocks, 256, 0, st>>>(cost, (int)n, hist);
+    k_order_scan<<<1, kOrderBuckets, 0, st>>>(hist);
+    k_order_scatter<<<blocks, 256, 0, st>>>(cost, (int)n, hist, order);
+    return check_launch("k_order_scatter");
 }
 
 PbStatus launch_count_evaluated(const PbGrid &g, const PbBeam *beams, int n_beams,

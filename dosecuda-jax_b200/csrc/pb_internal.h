@@ -63,7 +63,8 @@ void texture_destroy(uint64_t h);
 PbStatus launch_dose(const PbGrid &g, const PbBeam *beams, int n_beams,
                      const float *wet, const PbLayer *layers,
                      const float *geo, const float *mu, float scale,
-                     float *dose, float *beam_dose, cudaStream_t st, int variant = -1);
+                     float *dose, float *beam_dose, cudaStream_t st, int variant = -1,
+                     const int *order = nullptr);
 
 // variant < 0 selects the default forward shape (dose_variant_default);
 // the adjoint and the operation count use the kernel family of `variant`.
@@ -86,7 +87,12 @@ PbStatus launch_dose_batch(const void *plans_dev, int n_plans, long long n_items
 PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                         const float *wet, const PbLayer *layers,
                         const float *geo, const float *w, float scale,
-                        float *grad, cudaStream_t st, int variant = -1);
+                        float *grad, cudaStream_t st, int variant = -1,
+                        const int *order = nullptr);
+long long tile_order_count(const PbGrid &g);
+size_t tile_order_work_size(const PbGrid &g);
+PbStatus launch_tile_order(const PbGrid &g, const PbBeam *beams, int n_beams, const float *wet,
+                           const PbLayer *layers, void *work, int *order, cudaStream_t st);
 
 PbStatus launch_objective(const float *dose, const float *presc,
                           const float *weight, int64_t n, double *obj,

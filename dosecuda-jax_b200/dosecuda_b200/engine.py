@@ -179,6 +179,8 @@ class DevicePlan:
             self._cells = texture_pool.holder(self.device, self.shape, "cells")
         self.wet_mode = "texture"
         self._spec = beams
+        self._order: Optional[torch.Tensor] = None    # tile order for the current WET
+        self._order_work: Optional[torch.Tensor] = None
         self.spots_loaded = False
         if not defer_spots:
             self.load_spots()
@@ -308,12 +310,31 @@ class DevicePlan:
         self.wet = wet
         self.raw_wet = raw
         self.wet_mode = wet_mode
+        self._order = None
         return wet
 
     def set_wet(self, wet: torch.Tensor) -> None:
         if wet.numel() != self.n_beams * self.n_vox or wet.dtype != torch.float32:
             raise ValueError("wet must be float32 with n_beams x V elements")
         self.wet = wet.to(self.device).reshape(self.n_beams, self.n_vox).contiguous()
+        self._order = None
+
+    def tile_order(self) -> torch.Tensor:
+        """The default shape's tiles, most expensive first, for the current
+        WET (pb_tile_order); computed once per WET, stream-ordered."""
+        self._need_wet()
+        if self._order is None:
+            n = int(_lib.lib.pb_tile_order_count(ctypes.byref(self.grid)))
+            size = int(_lib.lib.pb_tile_order_work_size(ctypes.byref(self.grid)))
+            if self._order_work is None or self._order_work.numel() < size:
+                self._order_work = torch.empty(size, dtype=torch.uint8, device=self.device)
+            order = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+            check(_lib.lib.pb_tile_order(ctypes.byref(self.grid),
+                                         ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                                         ptr(self.wet), ptr(self.layers), ptr(self._order_work),
+                                         ptr(order), _stream(self.device)), "pb_tile_order")
+            self._order = order
+        return self._order
 
     def _need_wet(self):
         if not self.spots_loaded:
@@ -334,10 +355,12 @@ class DevicePlan:
                                                        device=self.device)
         bd = torch.empty((self.n_beams, self.n_vox), dtype=torch.float32,
                          device=self.device) if beam_doses else None
-        check(_lib.lib.pb_dose(ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p),
-                               self.n_beams, ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
-                               ptr(mu), float(scale), ptr(dose), ptr(bd),
-                               _stream(self.device)), "pb_dose")
+        order = self.tile_order()
+        check(_lib.lib.pb_dose_ordered(ctypes.byref(self.grid),
+                                       ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                                       ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
+                                       ptr(mu), float(scale), ptr(dose), ptr(bd), ptr(order),
+                                       _stream(self.device)), "pb_dose_ordered")
         return (dose, bd) if beam_doses else dose
 
     def forward_variant(self, variant: int, mu_sorted: Optional[torch.Tensor] = None,
@@ -367,11 +390,11 @@ class DevicePlan:
         grad = out if out is not None else torch.empty(max(self.n_spots, 1), dtype=torch.float32,
                                                        device=self.device)
         if variant is None:
-            check(_lib.lib.pb_dose_adjoint(ctypes.byref(self.grid),
-                                           ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
-                                           ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
-                                           ptr(w), float(scale), ptr(grad),
-                                           _stream(self.device)), "pb_dose_adjoint")
+            order = self.tile_order()
+            check(_lib.lib.pb_dose_adjoint_ordered(
+                ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
+                ptr(self.wet), ptr(self.layers), ptr(self.spot_geo), ptr(w), float(scale),
+                ptr(grad), ptr(order), _stream(self.device)), "pb_dose_adjoint_ordered")
         else:
             check(_lib.lib.pb_dose_adjoint_variant(
                 ctypes.byref(self.grid), ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,

@@ -337,6 +337,37 @@ PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
 PbStatus pb_batch_run(const PbBatchInfo *info, void *work_dev, int flags, int variant,
                       int blocks_per_sm, int *status_dev, void *stream);
 
+/* Tile order for pb_dose_ordered and pb_dose_adjoint_ordered.  The voxel
+ * tiles of the default kernel shape differ in work by more than two orders
+ * of magnitude (a tile every beam crosses near the target against one no
+ * spot reaches), and a launch that starts its longest tiles late ends on a
+ * few of them while the other SMs idle.  pb_tile_order estimates each
+ * tile's work from the WET and the layers (the layers the dose kernels keep
+ * for it and their spots within reach) and writes the tile indices, most
+ * expensive first, into order_dev (pb_tile_order_count ints).  work_dev:
+ * pb_tile_order_work_size bytes of scratch.  Stream-ordered, no
+ * allocation.  The order depends on the WET: compute it again when the WET
+ * changes (a stale order gives the same results, only its speed-up is
+ * lost).  No counterpart in the reference. */
+long long pb_tile_order_count(const PbGrid *grid);
+size_t pb_tile_order_work_size(const PbGrid *grid);
+PbStatus pb_tile_order(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                       const float *wet_dev, const PbLayer *layers_dev, void *work_dev,
+                       int *order_dev, void *stream);
+/* pb_dose and pb_dose_adjoint with the default shape's tiles taken in the
+ * order of order_dev (from pb_tile_order for this grid; NULL: the default
+ * order).  Each voxel's dose is the same bits as pb_dose's. */
+PbStatus pb_dose_ordered(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                         const float *wet_dev, const PbLayer *layers_dev,
+                         const float *spot_geo_dev, const float *mu_dev, float scale,
+                         float *dose_dev, float *beam_dose_dev, const int *order_dev,
+                         void *stream);
+PbStatus pb_dose_adjoint_ordered(const PbGrid *grid, const PbBeam *beams, int n_beams,
+                                 const float *wet_dev, const PbLayer *layers_dev,
+                                 const float *spot_geo_dev, const float *dobj_dose_dev,
+                                 float scale, float *grad_dev, const int *order_dev,
+                                 void *stream);
+
 /* Adjoint of pb_dose: grad_dev[s] = scale * sum_v dobj_dose_dev[v] * K(v,s)
  * for every spot s, where K(v,s) is the dose per unit weight of spot s at
  * voxel v.  Matrix-free: footprints are recomputed.  grad_dev is

@@ -505,6 +505,42 @@ def test_layer_bounds_change_no_result(pkg, small, which):
     assert torch.allclose(g1, g2, rtol=1e-5, atol=1e-6 * float(g1.abs().max()))
 
 
+@pytest.mark.parametrize("which", ["small", "full"])
+def test_tile_order_is_a_permutation_and_changes_no_result(pkg, small, which):
+    """pb_tile_order: every tile of the default shape once, the estimated
+    most expensive first; pb_dose_ordered gives pb_dose's dose and per-beam
+    doses bit for bit, pb_dose_adjoint_ordered its gradient to float
+    rounding (atomic order)."""
+    import ctypes
+    from dosecuda_b200 import _lib
+    case = small if which == "small" else pkg[2].config_gradient()
+    dp = case.grid.prepareIMPTPlan(case.plan, 0)
+    order = dp.tile_order().cpu().numpy()
+    n = int(_lib.lib.pb_tile_order_count(ctypes.byref(dp.grid)))
+    assert order.shape == (n,) and np.array_equal(np.sort(order), np.arange(n))
+    st = ctypes.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)
+    d0 = torch.empty(dp.n_vox, device=DEV)
+    b0 = torch.empty((dp.n_beams, dp.n_vox), device=DEV)
+    _lib.check(_lib.lib.pb_dose(ctypes.byref(dp.grid), ctypes.cast(dp.beams, ctypes.c_void_p),
+                                dp.n_beams, _lib.ptr(dp.wet), _lib.ptr(dp.layers),
+                                _lib.ptr(dp.spot_geo), _lib.ptr(dp.mu_sorted), 2.0,
+                                _lib.ptr(d0), _lib.ptr(b0), st), "pb_dose")
+    d1, b1 = dp.forward(scale=2.0, beam_doses=True)
+    assert torch.equal(d0, d1) and torch.equal(b0, b1)
+    assert torch.equal(dp.forward(), d0 / 2.0)      # scale 2 is exact
+    w = torch.from_numpy(np.random.default_rng(5).normal(size=dp.n_vox).astype(np.float32))
+    w = w.to(DEV)
+    g0 = torch.empty(max(dp.n_spots, 1), device=DEV)
+    _lib.check(_lib.lib.pb_dose_adjoint(ctypes.byref(dp.grid),
+                                        ctypes.cast(dp.beams, ctypes.c_void_p), dp.n_beams,
+                                        _lib.ptr(dp.wet), _lib.ptr(dp.layers),
+                                        _lib.ptr(dp.spot_geo), _lib.ptr(w), 1.0, _lib.ptr(g0), st),
+               "pb_dose_adjoint")
+    g1 = dp.adjoint(w)
+    m = float(g0.abs().max())
+    assert m > 0 and float((g0[: dp.n_spots] - g1).abs().max()) <= 1e-5 * m
+
+
 def test_adjoint_counts_follow_its_tile_skip(small):
     """pb_count_evaluated_adjoint: on a field nonzero everywhere it counts
     the forward's work; on a zero field nothing; on a field nonzero in one
