@@ -65,7 +65,7 @@ L2_NOTE = "flushed (256 MiB write) between timed iterations"
 # this workload (seed 3, texture WET) on the kernels as built now; the command
 # and the figures are in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md.
 # Reported only for that workload ("wet": k_raytrace + k_smooth).
-NCU_TRAFFIC = {"k_dose_line": 200_358_912, "k_adjoint_line": 130_179_328,
+NCU_TRAFFIC = {"k_dose_line": 206_854_400, "k_adjoint_line": 130_475_008,
                "wet": 849_633_024}
 NCU_TRAFFIC_WORKLOAD = {"seed": 3, "wet_mode": "texture"}
 
@@ -267,7 +267,7 @@ def run_mine(args, world, rank, local):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    kt = {"rlsp": [], "wet": [], "dose": [], "objective": [], "adjoint": []}
+    kt = {"rlsp": [], "wet": [], "order": [], "dose": [], "objective": [], "adjoint": []}
 
     def timed(name, fn, record):
         if record:
@@ -283,6 +283,8 @@ def run_mine(args, world, rank, local):
         timed("rlsp", lambda: engine.rlsp_from_hu(hu, *curve, out=rlsp), record)
         timed("wet", lambda: dp.compute_wet(rlsp, check_status=False, wet_mode=args.wet_mode),
               record)
+        # the tile order for this WET (pb_tile_order), then the dose with it
+        timed("order", dp.tile_order, record)
         timed("dose", lambda: dp.forward(dp.to_sorted(mu_plan), out=dose), record)
 
     obj_dev = [None]
@@ -379,9 +381,10 @@ def run_mine(args, world, rank, local):
                 "call": "IMPTDoseGrid.computeIMPTPlan" if args.mode == "forward"
                 else "engine.HostGradientStep"},
         # per forward step: HU->RLSP, [texture mode: five cell-record passes],
-        # ray trace, smoothing, pencil-beam sum; the grad step adds the
-        # objective (two) and the adjoint
-        "gpu_launches": ((9 if args.wet_mode == "texture" else 4) +
+        # ray trace, smoothing, the tile order (cost, histogram, scan,
+        # scatter), pencil-beam sum; the grad step adds the objective (two)
+        # and the adjoint
+        "gpu_launches": ((13 if args.wet_mode == "texture" else 8) +
                          (3 if args.mode == "grad" else 0)) * args.steps,
         "clocks": clk.summary(),
     }
