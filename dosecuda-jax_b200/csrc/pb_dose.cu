@@ -1465,8 +1465,8 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                                 AH[p] = __ffma2_rn(w, ex2x2(__fmul2_rn(HS[p], S)), AH[p]);
                             }
                         }
-                        // halo only
-#pragma unroll 2
+                        // halo only (unrolled by 4: 6.04 against 6.12 ms)
+#pragma unroll 4
                         for (int c = kCap - n1; c < kCap; ++c) {
                             const LineSpot r = sh.spot[c];
                             float S0, B1;
@@ -1525,10 +1525,15 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
 }
 
 // Resident blocks per SM the line-tile kernels are compiled for (their
-// register budget): 20 of 32 threads, 10 of 64, 5 of 128.
-template <int NT> constexpr int line_min_blocks()
+// register budget): 20 of 32 threads, 10 of 64, 5 of 128.  The kernels with
+// more live state per thread (the per-beam forward's extra sums, the
+// adjoint's weighted prefactors and spot groups) take 4 of 128 threads (128
+// registers): on the 4-beam 256x256x160 plan the adjoint went from 6.65 to
+// 6.43 ms and the per-beam forward from 6.78 to 6.47 ms, while the plain
+// forward is faster at 5 (6.12 against 6.25 ms).
+template <int NT, bool HEAVY = false> constexpr int line_min_blocks()
 {
-    return NT == 32 ? 20 : (NT == 64 ? 10 : 5);
+    return NT == 32 ? 20 : (NT == 64 ? 10 : (HEAVY ? 4 : 5));
 }
 
 #ifndef PB_TILE_ORDER
@@ -1589,7 +1594,7 @@ __device__ __forceinline__ bool line_tile_coords(const PlanArgs &A, long long ti
 }
 
 template <int TY, int TZ, int KCULL, bool BEAM_OUT>
-__global__ void __launch_bounds__(TY * TZ, line_min_blocks<TY * TZ>())
+__global__ void __launch_bounds__(TY * TZ, line_min_blocks<TY * TZ, BEAM_OUT>())
 k_dose_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
             const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
             const float *__restrict__ mu, float *__restrict__ dose,
@@ -1654,7 +1659,7 @@ k_dose_count_line(const __grid_constant__ PlanArgs A, const float *__restrict__ 
                                                               count, wfield);
 }
 
-__global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ>())
+__global__ void __launch_bounds__(kLineTY * kLineTZ, line_min_blocks<kLineTY * kLineTZ, true>())
 k_adjoint_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
                const PbLayer *__restrict__ layers, const float4 *__restrict__ geo,
                const float *__restrict__ wfield, float *__restrict__ grad)
@@ -1708,25 +1713,24 @@ __device__ __forceinline__ float layer_pair_cost(const PbLayer &L, const TileBou
     return kPairCost + (float)L.n_spots * frac;
 }
 
-// One block per line tile (raster index: x fastest): its box and depth
-// range per beam as line_tile forms them, then the estimated cost of every
-// layer pair it keeps.
+// One warp per line tile (raster index: x fastest; four tiles per block),
+// each lane a quarter of the tile's lines: the tile's box and depth range
+// per beam as line_tile forms them (warp reductions, no barrier), then the
+// estimated cost of every layer pair it keeps.
 template <int TY, int TZ>
-__global__ void __launch_bounds__(TY * TZ)
+__global__ void __launch_bounds__(128)
 k_tile_cost(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
-            const PbLayer *__restrict__ layers, float *__restrict__ cost)
+            const PbLayer *__restrict__ layers, float *__restrict__ cost, long long n_tiles)
 {
-    constexpr int NT = TY * TZ, kWarps = NT / 32;
-    __shared__ float s_red[kWarps][kRedSlots];
-    __shared__ float s_cost[kWarps];
+    constexpr int kLinesPerLane = TY * TZ / 32;
+    static_assert(TY * TZ % 32 == 0, "whole warps of lines");
+    const long long tile = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (tile >= n_tiles) return;   // the whole warp
+    const int lane = threadIdx.x & 31;
     const int nx8 = (A.g.nx + kLine - 1) / kLine, nty = (A.g.ny + TY - 1) / TY;
-    const long long tile = blockIdx.x;
     const int tx = (int)(tile % nx8), ty = (int)((tile / nx8) % nty);
     const int tz = (int)(tile / ((long long)nx8 * nty));
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int i0 = tx * kLine, j = ty * TY + t % TY, k = tz * TZ + t / TY;
-    const int nvalid = (j < A.g.ny && k < A.g.nz) ? min(kLine, A.g.nx - i0) : 0;
-    const int64_t vbase = i0 + (int64_t)A.g.nx * (j + (int64_t)A.g.ny * k);
+    const int i0 = tx * kLine;
     const int64_t V = (int64_t)A.g.nx * A.g.ny * A.g.nz;
     float c = 0.0f;
     for (int b = 0; b < A.n_beams; ++b) {
@@ -1734,68 +1738,52 @@ k_tile_cost(const __grid_constant__ PlanArgs A, const float *__restrict__ wet,
         float dX, dY, dZ;
         image_to_head(B.geom, A.g.spacing, 0.0f, 0.0f, dX, dY, dZ);
         const float dgx = -__fdiv_rn(dZ, B.geom.vsadx), dgy = -__fdiv_rn(dZ, B.geom.vsady);
-        float Xc, Yc, Zc;
-        {
-            float px, py, pz, X0, Y0, Z0;
-            vox_mm(B.geom, A.g.spacing, i0, j, k, px, py, pz);
-            image_to_head(B.geom, px, py, pz, X0, Y0, Z0);
-            Xc = __fmaf_rn(3.5f, dX, X0);
-            Yc = __fmaf_rn(3.5f, dY, Y0);
-            Zc = __fmaf_rn(3.5f, dZ, Z0);
-        }
-        const float gxc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsadx));
-        const float gyc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsady));
         float v[12] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
                        INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
 #pragma unroll
-        for (int q = 0; q < kLine; ++q) {
-            if (q >= nvalid) continue;
-            const float o = line_off(q);
-            const float X = __fmaf_rn(o, dX, Xc), Y = __fmaf_rn(o, dY, Yc);
-            const float Z = __fmaf_rn(o, dZ, Zc);
-            const float w = __fmul_rn(__ldg(wet + b * V + vbase + q), 10.0f);
-            const float dd = source_distance(B, X, Y, Z);
-            const float GX = __fmaf_rn(o, dgx, gxc), GY = __fmaf_rn(o, dgy, gyc);
-            v[0] = fminf(v[0], X);  v[1] = fmaxf(v[1], X);
-            v[2] = fminf(v[2], Y);  v[3] = fmaxf(v[3], Y);
-            v[4] = fminf(v[4], GX); v[5] = fmaxf(v[5], GX);
-            v[6] = fminf(v[6], GY); v[7] = fmaxf(v[7], GY);
-            v[8] = fminf(v[8], dd); v[9] = fmaxf(v[9], dd);
-            v[10] = fminf(v[10], w == w ? w : -INFINITY);
-            v[11] = fmaxf(v[11], w == w ? w : INFINITY);
+        for (int m = 0; m < kLinesPerLane; ++m) {
+            const int ln = lane + 32 * m;
+            const int j = ty * TY + ln % TY, k = tz * TZ + ln / TY;
+            const int nvalid = (j < A.g.ny && k < A.g.nz) ? min(kLine, A.g.nx - i0) : 0;
+            if (nvalid <= 0) continue;
+            const int64_t vbase = i0 + (int64_t)A.g.nx * (j + (int64_t)A.g.ny * k);
+            float px, py, pz, X0, Y0, Z0;
+            vox_mm(B.geom, A.g.spacing, i0, j, k, px, py, pz);
+            image_to_head(B.geom, px, py, pz, X0, Y0, Z0);
+            const float Xc = __fmaf_rn(3.5f, dX, X0), Yc = __fmaf_rn(3.5f, dY, Y0);
+            const float Zc = __fmaf_rn(3.5f, dZ, Z0);
+            const float gxc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsadx));
+            const float gyc = __fsub_rn(1.0f, __fdiv_rn(Zc, B.geom.vsady));
+#pragma unroll
+            for (int q = 0; q < kLine; ++q) {
+                if (q >= nvalid) continue;
+                const float o = line_off(q);
+                const float X = __fmaf_rn(o, dX, Xc), Y = __fmaf_rn(o, dY, Yc);
+                const float Z = __fmaf_rn(o, dZ, Zc);
+                const float w = __fmul_rn(__ldg(wet + b * V + vbase + q), 10.0f);
+                const float dd = source_distance(B, X, Y, Z);
+                const float GX = __fmaf_rn(o, dgx, gxc), GY = __fmaf_rn(o, dgy, gyc);
+                v[0] = fminf(v[0], X);  v[1] = fmaxf(v[1], X);
+                v[2] = fminf(v[2], Y);  v[3] = fmaxf(v[3], Y);
+                v[4] = fminf(v[4], GX); v[5] = fmaxf(v[5], GX);
+                v[6] = fminf(v[6], GY); v[7] = fmaxf(v[7], GY);
+                v[8] = fminf(v[8], dd); v[9] = fmaxf(v[9], dd);
+                v[10] = fminf(v[10], w == w ? w : -INFINITY);
+                v[11] = fmaxf(v[11], w == w ? w : INFINITY);
+            }
         }
 #pragma unroll
         for (int m = 0; m < 12; ++m) v[m] = (m & 1) ? warp_max(v[m]) : warp_min(v[m]);
-        if (lane == 0) {
-#pragma unroll
-            for (int m = 0; m < 12; ++m) s_red[warp][m] = v[m];
-        }
-        __syncthreads();
-        float r[12];
-#pragma unroll
-        for (int m = 0; m < 12; ++m) r[m] = s_red[0][m];
-        for (int w = 1; w < kWarps; ++w) {
-#pragma unroll
-            for (int m = 0; m < 12; ++m)
-                r[m] = (m & 1) ? fmaxf(r[m], s_red[w][m]) : fminf(r[m], s_red[w][m]);
-        }
         TileBounds tb;
-        tb.x0 = r[0]; tb.x1 = r[1]; tb.y0 = r[2]; tb.y1 = r[3];
-        tb.gx0 = r[4]; tb.gx1 = r[5]; tb.gy0 = r[6]; tb.gy1 = r[7];
-        tb.d0 = r[8]; tb.d1 = r[9]; tb.w0 = r[10]; tb.w1 = r[11];
-        for (int l = t; l < B.n_layers; l += NT)
+        tb.x0 = v[0]; tb.x1 = v[1]; tb.y0 = v[2]; tb.y1 = v[3];
+        tb.gx0 = v[4]; tb.gx1 = v[5]; tb.gy0 = v[6]; tb.gy1 = v[7];
+        tb.d0 = v[8]; tb.d1 = v[9]; tb.w0 = v[10]; tb.w1 = v[11];
+        for (int l = lane; l < B.n_layers; l += 32)
             c += layer_pair_cost(layers[B.layer_start + l], tb, B);
-        __syncthreads();   // s_red is rewritten by the next beam
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) s_cost[warp] = c;
-    __syncthreads();
-    if (t == 0) {
-        float total = 0.0f;
-        for (int w = 0; w < kWarps; ++w) total += s_cost[w];
-        cost[tile] = total;
-    }
+    if (lane == 0) cost[tile] = c;
 }
 
 // Bucket of a cost, most expensive last: 32 buckets per octave.
@@ -2426,7 +2414,8 @@ PbStatus launch_tile_order(const PbGrid &g, const PbBeam *beams, int n_beams, co
     PbStatus s = check_cuda(cudaMemsetAsync(hist, 0, kOrderBuckets * sizeof(int), st),
                             "cudaMemsetAsync(order buckets)");
     if (s != PB_OK) return s;
-    k_tile_cost<kLineTY, kLineTZ><<<(unsigned)n, kLineTY * kLineTZ, 0, st>>>(A, wet, layers, cost);
+    k_tile_cost<kLineTY, kLineTZ><<<(unsigned)((n + 3) / 4), 128, 0, st>>>(A, wet, layers, cost,
+                                                                          n);
     s = check_launch("k_tile_cost");
     if (s != PB_OK) return s;
     const unsigned blocks = (unsigned)((n + 255) / 256);
