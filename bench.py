@@ -65,7 +65,7 @@ L2_NOTE = "flushed (256 MiB write) between timed iterations"
 # this workload (seed 3, texture WET) on the kernels as built now; the command
 # and the figures are in profiles/pencil_beam_kernels_heterogeneous_256x256x160_4beams.md.
 # Reported only for that workload ("wet": k_raytrace + k_smooth).
-NCU_TRAFFIC = {"k_dose_line": 206_854_400, "k_adjoint_line": 130_475_008,
+NCU_TRAFFIC = {"k_dose_line": 208_208_128, "k_adjoint_line": 129_612_544,
                "wet": 849_633_024}
 NCU_TRAFFIC_WORKLOAD = {"seed": 3, "wet_mode": "texture"}
 
