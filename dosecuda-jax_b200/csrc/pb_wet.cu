@@ -834,21 +834,26 @@ k_cell_flat(const float *__restrict__ rho, PbGrid g, float *__restrict__ value)
 }
 
 // Separable L-infinity distance to the nearest non-flat cell, capped at
-// kRunCap: axis 0 starts from the flat flags, axes 1 and 2 combine the
-// previous pass with max(|offset|, d).
-template <int AXIS>
+// kRunCap.  The distances are bytes in rows padded to a multiple of 4 cells
+// (cell_row).  Axis x starts from the flat flags, one cell per thread;
+// axes y and z combine the previous pass with max(|offset|, d) four cells
+// at a time, with byte-wise SIMD max/min on 32-bit words.
+__host__ __device__ __forceinline__ int cell_row(int nx) { return (nx + 1 + 3) & ~3; }
+
 __global__ void __launch_bounds__(256, 4)
-k_cell_dist(PbGrid g, const float *__restrict__ value, const unsigned char *__restrict__ din,
-            unsigned char *__restrict__ dout)
+k_cell_dist_x(PbGrid g, const float *__restrict__ value, unsigned char *__restrict__ dout)
 {
-    const int cx = g.nx + 1, cy = g.ny + 1, cz = g.nz + 1;
-    const int64_t n = (int64_t)cx * cy * cz;
-    const int len = AXIS == 0 ? cx : (AXIS == 1 ? cy : cz);
-    const int64_t stride = AXIS == 0 ? 1 : (AXIS == 1 ? (int64_t)cx : (int64_t)cx * cy);
+    const int cx = g.nx + 1, cy = g.ny + 1, cz = g.nz + 1, row = cell_row(g.nx);
+    const int64_t n = (int64_t)row * cy * cz;
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
          c += (int64_t)gridDim.x * blockDim.x) {
-        const int pos = AXIS == 0 ? (int)(c % cx)
-                                  : (AXIS == 1 ? (int)((c / cx) % cy) : (int)(c / ((int64_t)cx * cy)));
+        const int pos = (int)(c % row);
+        const int64_t line = c / row;
+        if (pos >= cx) {   // row padding
+            dout[c] = 0;
+            continue;
+        }
+        const float *v = value + line * cx + pos;
         // every tap, unrolled and without branches, so that all the loads
         // are in flight at once (a tap with |k| >= best cannot lower best,
         // so taking it changes nothing)
@@ -858,17 +863,38 @@ k_cell_dist(PbGrid g, const float *__restrict__ value, const unsigned char *__re
             const int q = pos + k;
             const int ak = k < 0 ? -k : k;
             int d = 0;
-            if (q >= 0 && q < len) {
-                if (AXIS == 0) {
-                    const float v = __ldg(value + c + k);
-                    d = (v == v) ? kRunCap : 0;
-                } else {
-                    d = __ldg(din + c + k * stride);
-                }
+            if (q >= 0 && q < cx) {
+                const float x = __ldg(v + k);
+                d = (x == x) ? kRunCap : 0;
             }
             best = min(best, max(ak, d));
         }
         dout[c] = (unsigned char)best;
+    }
+}
+
+template <int AXIS>
+__global__ void __launch_bounds__(256, 4)
+k_cell_dist4(PbGrid g, const unsigned int *__restrict__ din, unsigned int *__restrict__ dout)
+{
+    static_assert(AXIS == 1 || AXIS == 2, "y or z");
+    const int cy = g.ny + 1, cz = g.nz + 1, words = cell_row(g.nx) / 4;
+    const int64_t n = (int64_t)words * cy * cz;
+    const int len = AXIS == 1 ? cy : cz;
+    const int64_t stride = AXIS == 1 ? (int64_t)words : (int64_t)words * cy;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int pos = AXIS == 1 ? (int)((c / words) % cy) : (int)(c / ((int64_t)words * cy));
+        unsigned int best = kRunCap * 0x01010101u;
+#pragma unroll
+        for (int k = -kRunCap; k <= kRunCap; ++k) {
+            const int q = pos + k;
+            const unsigned int ak = (unsigned int)(k < 0 ? -k : k) * 0x01010101u;
+            // outside the grid counts as non-flat (distance 0)
+            const unsigned int d = (q >= 0 && q < len) ? __ldg(din + c + k * stride) : 0u;
+            best = __vminu4(best, __vmaxu4(ak, d));
+        }
+        dout[c] = best;
     }
 }
 
@@ -877,11 +903,13 @@ __global__ void __launch_bounds__(256)
 k_cell_records(PbGrid g, const float *__restrict__ value, const unsigned char *__restrict__ dist,
                float2 *__restrict__ rec)
 {
-    const int64_t n = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+    const int cx = g.nx + 1, row = cell_row(g.nx);
+    const int64_t n = (int64_t)cx * (g.ny + 1) * (g.nz + 1);
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
          c += (int64_t)gridDim.x * blockDim.x) {
         const float v = value[c];
-        rec[c] = make_float2(v == v ? v : 0.0f, v == v ? (float)dist[c] : 0.0f);
+        const unsigned char d = dist[(c / cx) * row + c % cx];
+        rec[c] = make_float2(v == v ? v : 0.0f, v == v ? (float)d : 0.0f);
     }
 }
 
@@ -912,9 +940,11 @@ static PbStatus texture_fill(RlspTexture *t, const float *rlsp, cudaStream_t st)
     const PbGrid g{t->nx, t->ny, t->nz, 1.0f};
     const int blocks = 148 * 8;
     k_cell_flat<<<blocks, 256, 0, st>>>(rlsp, g, t->value);
-    k_cell_dist<0><<<blocks, 256, 0, st>>>(g, t->value, nullptr, t->d0);
-    k_cell_dist<1><<<blocks, 256, 0, st>>>(g, t->value, t->d0, t->d1);
-    k_cell_dist<2><<<blocks, 256, 0, st>>>(g, t->value, t->d1, t->d0);
+    k_cell_dist_x<<<blocks, 256, 0, st>>>(g, t->value, t->d0);
+    k_cell_dist4<1><<<blocks, 256, 0, st>>>(g, reinterpret_cast<const unsigned int *>(t->d0),
+                                            reinterpret_cast<unsigned int *>(t->d1));
+    k_cell_dist4<2><<<blocks, 256, 0, st>>>(g, reinterpret_cast<const unsigned int *>(t->d1),
+                                            reinterpret_cast<unsigned int *>(t->d0));
     k_cell_records<<<blocks, 256, 0, st>>>(g, t->value, t->d0, t->rec);
     return check_launch("cell records");
 }
@@ -950,8 +980,10 @@ PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaS
                        "cudaMalloc3DArray");
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->rec, sizeof(float2) * ncell), "cudaMalloc");
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->value, sizeof(float) * ncell), "cudaMalloc");
-    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d0, ncell), "cudaMalloc");
-    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d1, ncell), "cudaMalloc");
+    // distance passes: rows padded to 4 cells (32-bit words)
+    const size_t npad = (size_t)cell_row(g.nx) * (g.ny + 1) * (g.nz + 1);
+    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d0, npad), "cudaMalloc");
+    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d1, npad), "cudaMalloc");
     if (s == PB_OK && with_texture) {
         cudaResourceDesc rd{};
         rd.resType = cudaResourceTypeArray;
