@@ -805,12 +805,19 @@ PbStatus launch_wet_batch(const void *items_dev, int n_items, long long n_bricks
 // equal.  Two adjacent flat cells share texels, so a connected flat region
 // has one value.
 constexpr int kRunCap = 15;   // largest stored distance (cells)
+constexpr int kFlagPad = 16;  // zero bytes before and after each row of flat flags
+
+// Row lengths (bytes) of the distance passes' work arrays: cells padded to
+// a multiple of 4, and the flat flags with kFlagPad bytes on each side.
+__host__ __device__ __forceinline__ int cell_row(int nx) { return (nx + 1 + 3) & ~3; }
+__host__ __device__ __forceinline__ int flag_row(int nx) { return cell_row(nx) + 2 * kFlagPad; }
 
 // Pass 0: flat cells -> their value, else NaN; 1-D distance along x to the
 // nearest non-flat cell (cells outside the cell grid count as non-flat),
 // capped at kRunCap.
 __global__ void __launch_bounds__(256)
-k_cell_flat(const float *__restrict__ rho, PbGrid g, float *__restrict__ value)
+k_cell_flat(const float *__restrict__ rho, PbGrid g, float *__restrict__ value,
+            unsigned char *__restrict__ flag)
 {
     const int cx = g.nx + 1, cy = g.ny + 1, cz = g.nz + 1;
     const int64_t n = (int64_t)cx * cy * cz;
@@ -829,47 +836,48 @@ k_cell_flat(const float *__restrict__ rho, PbGrid g, float *__restrict__ value)
             if (t == 0) v0 = v;
             else flat &= (v == v0);
         }
-        value[c] = (flat && v0 == v0) ? v0 : __int_as_float(0x7fc00000);
+        const bool f = flat && v0 == v0;
+        value[c] = f ? v0 : __int_as_float(0x7fc00000);
+        // the x distance pass's input: kRunCap where flat, in rows with
+        // kFlagPad zero bytes before and after (flag_row)
+        flag[(c / cx) * flag_row(g.nx) + kFlagPad + ci] = f ? (unsigned char)kRunCap : 0;
     }
 }
 
 // Separable L-infinity distance to the nearest non-flat cell, capped at
-// kRunCap.  The distances are bytes in rows padded to a multiple of 4 cells
-// (cell_row).  Axis x starts from the flat flags, one cell per thread;
-// axes y and z combine the previous pass with max(|offset|, d) four cells
-// at a time, with byte-wise SIMD max/min on 32-bit words.
-__host__ __device__ __forceinline__ int cell_row(int nx) { return (nx + 1 + 3) & ~3; }
-
+// kRunCap: min over |k| <= kRunCap of max(|k|, d(pos + k)), a cell outside
+// the grid counting as non-flat (d = 0).  All three passes work on four
+// cells per 32-bit word with byte-wise SIMD max/min.  The distances are
+// bytes in rows padded to a multiple of 4 cells (cell_row); the x pass reads
+// the flat flags (kRunCap or 0) in rows with kFlagPad zero bytes on each
+// side (flag_row), so that every tap of a word is two aligned words and a
+// funnel shift.
 __global__ void __launch_bounds__(256, 4)
-k_cell_dist_x(PbGrid g, const float *__restrict__ value, unsigned char *__restrict__ dout)
+k_cell_dist_x(PbGrid g, const unsigned char *__restrict__ flag, unsigned int *__restrict__ dout)
 {
-    const int cx = g.nx + 1, cy = g.ny + 1, cz = g.nz + 1, row = cell_row(g.nx);
-    const int64_t n = (int64_t)row * cy * cz;
+    static_assert(kFlagPad == 16 && kRunCap == 15, "taps span kFlagPad +/- kRunCap bytes");
+    const int cy = g.ny + 1, cz = g.nz + 1, words = cell_row(g.nx) / 4, frow = flag_row(g.nx);
+    const int64_t n = (int64_t)words * cy * cz;
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
          c += (int64_t)gridDim.x * blockDim.x) {
-        const int pos = (int)(c % row);
-        const int64_t line = c / row;
-        if (pos >= cx) {   // row padding
-            dout[c] = 0;
-            continue;
-        }
-        const float *v = value + line * cx + pos;
-        // every tap, unrolled and without branches, so that all the loads
-        // are in flight at once (a tap with |k| >= best cannot lower best,
-        // so taking it changes nothing)
-        int best = kRunCap;
+        const int w = (int)(c % words);
+        const int64_t line = c / words;
+        // cells 4w - 15 .. 4w + 18: flag bytes 4w + 1 .. 4w + 34 of the row,
+        // within its words w .. w + 8 (the last ends at the row's last byte)
+        const unsigned int *src =
+            reinterpret_cast<const unsigned int *>(flag + line * frow + 4 * w);
+        unsigned int W[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) W[j] = __ldg(src + j);
+        unsigned int best = kRunCap * 0x01010101u;
 #pragma unroll
         for (int k = -kRunCap; k <= kRunCap; ++k) {
-            const int q = pos + k;
-            const int ak = k < 0 ? -k : k;
-            int d = 0;
-            if (q >= 0 && q < cx) {
-                const float x = __ldg(v + k);
-                d = (x == x) ? kRunCap : 0;
-            }
-            best = min(best, max(ak, d));
+            const int b = kFlagPad + k;   // first byte of the window, 1 .. 31
+            const unsigned int d = __funnelshift_r(W[b >> 2], W[(b >> 2) + 1], 8 * (b & 3));
+            const unsigned int ak = (unsigned int)(k < 0 ? -k : k) * 0x01010101u;
+            best = __vminu4(best, __vmaxu4(ak, d));
         }
-        dout[c] = (unsigned char)best;
+        dout[c] = best;
     }
 }
 
@@ -922,6 +930,7 @@ struct RlspTexture {
     float2 *rec = nullptr;            // (nx+1)(ny+1)(nz+1) cell records
     float *value = nullptr;           // work: flat values
     unsigned char *d0 = nullptr, *d1 = nullptr;  // work: distance passes
+    unsigned char *flag = nullptr;    // work: flat flags (zero-padded rows)
     int nx = 0, ny = 0, nz = 0;
 };
 
@@ -939,8 +948,8 @@ static PbStatus texture_fill(RlspTexture *t, const float *rlsp, cudaStream_t st)
     }
     const PbGrid g{t->nx, t->ny, t->nz, 1.0f};
     const int blocks = 148 * 8;
-    k_cell_flat<<<blocks, 256, 0, st>>>(rlsp, g, t->value);
-    k_cell_dist_x<<<blocks, 256, 0, st>>>(g, t->value, t->d0);
+    k_cell_flat<<<blocks, 256, 0, st>>>(rlsp, g, t->value, t->flag);
+    k_cell_dist_x<<<blocks, 256, 0, st>>>(g, t->flag, reinterpret_cast<unsigned int *>(t->d0));
     k_cell_dist4<1><<<blocks, 256, 0, st>>>(g, reinterpret_cast<const unsigned int *>(t->d0),
                                             reinterpret_cast<unsigned int *>(t->d1));
     k_cell_dist4<2><<<blocks, 256, 0, st>>>(g, reinterpret_cast<const unsigned int *>(t->d1),
@@ -957,6 +966,7 @@ static void texture_free(RlspTexture *t)
     cudaFree(t->value);
     cudaFree(t->d0);
     cudaFree(t->d1);
+    cudaFree(t->flag);
     delete t;
 }
 
@@ -984,6 +994,11 @@ PbStatus texture_create(const float *rlsp, const PbGrid &g, uint64_t *out, cudaS
     const size_t npad = (size_t)cell_row(g.nx) * (g.ny + 1) * (g.nz + 1);
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d0, npad), "cudaMalloc");
     if (s == PB_OK) s = check_cuda(cudaMalloc(&t->d1, npad), "cudaMalloc");
+    // flat flags: the padding bytes stay zero, the cells are rewritten by
+    // every fill
+    const size_t nflag = (size_t)flag_row(g.nx) * (g.ny + 1) * (g.nz + 1);
+    if (s == PB_OK) s = check_cuda(cudaMalloc(&t->flag, nflag), "cudaMalloc");
+    if (s == PB_OK) s = check_cuda(cudaMemset(t->flag, 0, nflag), "cudaMemset");
     if (s == PB_OK && with_texture) {
         cudaResourceDesc rd{};
         rd.resType = cudaResourceTypeArray;
