@@ -505,7 +505,7 @@ struct DevBuf {
 };
 
 enum { kBufRlsp, kBufRaw, kBufWet, kBufDose, kBufLayers, kBufGeo, kBufMu, kBufDvp,
-       kBufDep, kBufSig, kBufIdd, kBufStatus, kBufCount };
+       kBufDep, kBufSig, kBufIdd, kBufStatus, kBufOrderWork, kBufOrder, kBufCount };
 
 struct DevState {
     std::mutex m;
@@ -651,6 +651,8 @@ PbStatus pb_proton_spot_host(int gpu_id, double vsadx, double vsady, const float
     PB_TRY(ensure(D.buf[kBufDep], tb));
     PB_TRY(ensure(D.buf[kBufSig], tb));
     PB_TRY(ensure(D.buf[kBufIdd], tb));
+    PB_TRY(ensure(D.buf[kBufOrderWork], tile_order_work_size(g)));
+    PB_TRY(ensure(D.buf[kBufOrder], sizeof(int) * (size_t)tile_order_count(g)));
     cudaStream_t st = 0;
     auto h2d = [&](int slot, const void *src, size_t bytes) -> PbStatus {
         if (!bytes) return PB_OK;
@@ -686,11 +688,16 @@ PbStatus pb_proton_spot_host(int gpu_id, double vsadx, double vsady, const float
         B.dvp_len = dvp_len;
         PB_TRY(launch_layer_bounds(&B, 1, static_cast<PbLayer *>(D.buf[kBufLayers].p),
                                    static_cast<const float *>(D.buf[kBufGeo].p), st));
+        // the tiles in the order of their estimated work (pb_tile_order)
+        PB_TRY(launch_tile_order(g, &B, 1, static_cast<const float *>(D.buf[kBufWet].p),
+                                 static_cast<const PbLayer *>(D.buf[kBufLayers].p),
+                                 D.buf[kBufOrderWork].p, static_cast<int *>(D.buf[kBufOrder].p),
+                                 st));
         PB_TRY(launch_dose(g, &B, 1, static_cast<const float *>(D.buf[kBufWet].p),
                            static_cast<const PbLayer *>(D.buf[kBufLayers].p),
                            static_cast<const float *>(D.buf[kBufGeo].p),
                            static_cast<const float *>(D.buf[kBufMu].p), 1.0f, d_dose, nullptr,
-                           st));
+                           st, -1, static_cast<const int *>(D.buf[kBufOrder].p)));
     }
     PB_TRY(check_cuda(cudaMemcpyAsync(dose_out, d_dose, vb, cudaMemcpyDeviceToHost, st),
                       "D2H dose"));

@@ -541,6 +541,34 @@ def test_tile_order_is_a_permutation_and_changes_no_result(pkg, small, which):
     assert m > 0 and float((g0[: dp.n_spots] - g1).abs().max()) <= 1e-5 * m
 
 
+def test_tile_order_on_grids_smaller_than_a_tile(pkg, small):
+    """Grids of fewer voxels than one line tile (and fewer tiles than a warp
+    of the cost kernel takes): the order still names every tile once and
+    the ordered dose equals the unordered one bit for bit."""
+    import ctypes
+    from dosecuda_b200 import _lib, engine
+    beam = small.plan.beam_list[0]
+    model = _model(small.plan, beam)
+    spots = np.asarray(beam.spot_list, np.float32).reshape(-1, 4)[:40]
+    for shape in [(3, 5, 9), (9, 17, 8)]:
+        spacing = 3.0
+        origin = np.asarray(beam.iso, np.float32) - 0.5 * spacing * np.array(shape[::-1], np.float32)
+        dp = engine.DevicePlan(shape, spacing, origin,
+                               [engine.BeamSpec(beam.gantry_angle, beam.couch_angle, beam.iso,
+                                                spots, model)], DEV)
+        dp.compute_wet(torch.ones(int(np.prod(shape)), device=DEV))
+        order = dp.tile_order().cpu().numpy()
+        n = int(_lib.lib.pb_tile_order_count(ctypes.byref(dp.grid)))
+        assert n >= 1 and np.array_equal(np.sort(order[:n]), np.arange(n)), shape
+        d0 = torch.empty(dp.n_vox, device=DEV)
+        st = ctypes.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)
+        _lib.check(_lib.lib.pb_dose(ctypes.byref(dp.grid),
+                                    ctypes.cast(dp.beams, ctypes.c_void_p), dp.n_beams,
+                                    _lib.ptr(dp.wet), _lib.ptr(dp.layers), _lib.ptr(dp.spot_geo),
+                                    _lib.ptr(dp.mu_sorted), 1.0, _lib.ptr(d0), None, st), "pb_dose")
+        assert torch.equal(dp.forward(), d0), shape
+
+
 def test_adjoint_counts_follow_its_tile_skip(small):
     """pb_count_evaluated_adjoint: on a field nonzero everywhere it counts
     the forward's work; on a zero field nothing; on a field nonzero in one
