@@ -855,24 +855,26 @@ k_cell_flat(const float *__restrict__ rho, PbGrid g, float *__restrict__ value,
 __global__ void __launch_bounds__(256, 4)
 k_cell_dist_x(PbGrid g, const unsigned char *__restrict__ flag, unsigned int *__restrict__ dout)
 {
-    static_assert(kFlagPad == 16 && kRunCap == 15, "taps span kFlagPad +/- kRunCap bytes");
+    static_assert(kFlagPad > kRunCap && kFlagPad % 4 == 0, "every tap inside the padded row");
+    constexpr int kWords = (kFlagPad + kRunCap) / 4 + 2;   // words w .. w + kWords - 1
     const int cy = g.ny + 1, cz = g.nz + 1, words = cell_row(g.nx) / 4, frow = flag_row(g.nx);
     const int64_t n = (int64_t)words * cy * cz;
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
          c += (int64_t)gridDim.x * blockDim.x) {
         const int w = (int)(c % words);
         const int64_t line = c / words;
-        // cells 4w - 15 .. 4w + 18: flag bytes 4w + 1 .. 4w + 34 of the row,
-        // within its words w .. w + 8 (the last ends at the row's last byte)
+        // cells 4w - kRunCap .. 4w + 3 + kRunCap: flag bytes from
+        // 4w + kFlagPad - kRunCap on, within the row's words from w (the last
+        // word read ends at most at the row's last byte)
         const unsigned int *src =
             reinterpret_cast<const unsigned int *>(flag + line * frow + 4 * w);
-        unsigned int W[9];
+        unsigned int W[kWords];
 #pragma unroll
-        for (int j = 0; j < 9; ++j) W[j] = __ldg(src + j);
+        for (int j = 0; j < kWords; ++j) W[j] = __ldg(src + j);
         unsigned int best = kRunCap * 0x01010101u;
 #pragma unroll
         for (int k = -kRunCap; k <= kRunCap; ++k) {
-            const int b = kFlagPad + k;   // first byte of the window, 1 .. 31
+            const int b = kFlagPad + k;   // first byte of the window
             const unsigned int d = __funnelshift_r(W[b >> 2], W[(b >> 2) + 1], 8 * (b & 3));
             const unsigned int ak = (unsigned int)(k < 0 ? -k : k) * 0x01010101u;
             best = __vminu4(best, __vmaxu4(ak, d));
