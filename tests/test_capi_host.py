@@ -136,6 +136,23 @@ def test_invalid_arguments_return_status_without_a_gpu():
     assert L.pb_proton_raytrace_host(0, 1340.0, 1930.0, _lib.ptr(buf), _lib.ptr(dims),
                                      ctypes.c_float(2.0), _lib.ptr(buf), _lib.ptr(buf), 0.0, 0.0,
                                      _lib.ptr(buf)) == _lib.PB_ERR_INVALID
+    # the tile order: sizes from the grid alone; bad grids, beams or buffers
+    # are rejected before any device work
+    g = _lib.PbGrid(256, 256, 160, 2.0)
+    n = L.pb_tile_order_count(ctypes.byref(g))
+    assert n == 32 * 16 * 20                          # 8 x 16 x 8 voxel tiles
+    assert L.pb_tile_order_work_size(ctypes.byref(g)) >= 4 * n + 4096
+    bad = _lib.PbGrid(0, 4, 4, 2.0)
+    assert L.pb_tile_order_count(ctypes.byref(bad)) == -1
+    assert L.pb_tile_order_work_size(ctypes.byref(bad)) == 0
+    assert L.pb_tile_order(ctypes.byref(bad), None, 1, None, None, None, None,
+                           None) == _lib.PB_ERR_INVALID
+    assert L.pb_tile_order(ctypes.byref(g), None, 0, None, None, None, None,
+                           None) == _lib.PB_ERR_INVALID
+    assert L.pb_dose_ordered(ctypes.byref(g), None, 1, None, None, None, None, 1.0, None, None,
+                             None, None) == _lib.PB_ERR_INVALID
+    assert L.pb_dose_adjoint_ordered(ctypes.byref(g), None, 1, None, None, None, None, 1.0,
+                                     None, None, None) == _lib.PB_ERR_INVALID
 
 
 def _smoothing_cases(n):
