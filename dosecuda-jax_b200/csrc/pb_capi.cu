@@ -317,20 +317,6 @@ PbStatus pb_dose(const PbGrid *grid, const PbBeam *beams, int n_beams, const flo
                        dose_dev, beam_dose_dev, static_cast<cudaStream_t>(stream));
 }
 
-PbStatus pb_host_device_pointer(const void *host_ptr, void **device_ptr)
-{
-    if (!host_ptr || !device_ptr) return set_error(PB_ERR_INVALID, "NULL argument");
-    *device_ptr = nullptr;
-    void *d = nullptr;
-    const cudaError_t e = cudaHostGetDevicePointer(&d, const_cast<void *>(host_ptr), 0);
-    if (e != cudaSuccess) {
-        cudaGetLastError();   // not mapped: no error left for the next launch check
-        return set_error(PB_ERR_CUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(e));
-    }
-    *device_ptr = d;
-    return PB_OK;
-}
-
 long long pb_tile_order_count(const PbGrid *grid)
 {
     return check_grid(grid) == PB_OK ? tile_order_count(*grid) : -1;

@@ -139,7 +139,6 @@ _SIGS = {
     "pb_dose_adjoint_positions": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _VP,
                                        _F, _VP, _VP, _VP, _VP]),
     "pb_count_evaluated": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _VP]),
-    "pb_host_device_pointer": (_I, [_VP, ctypes.POINTER(ctypes.c_void_p)]),
     "pb_tile_order_count": (ctypes.c_longlong, [ctypes.POINTER(PbGrid)]),
     "pb_tile_order_work_size": (ctypes.c_size_t, [ctypes.POINTER(PbGrid)]),
     "pb_tile_order": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _VP]),

@@ -363,39 +363,6 @@ class DevicePlan:
                                        _stream(self.device)), "pb_dose_ordered")
         return (dose, bd) if beam_doses else dose
 
-    def forward_to_host(self, dose_host: torch.Tensor,
-                        beam_doses_host: Optional[torch.Tensor] = None, scale: float = 1.0,
-                        mu_sorted: Optional[torch.Tensor] = None) -> bool:
-        """The forward written by the kernel straight into page-locked host
-        tensors (dose: V, per-beam doses: n_beams x V), so that the copy back
-        overlaps the computation.  Stream-ordered: synchronise before
-        reading.  False, with nothing launched, when the host memory is not
-        mapped for this device (pb_host_device_pointer); copy through the
-        device then."""
-        self._need_wet()
-        mu = (self.mu_sorted if mu_sorted is None else mu_sorted).contiguous()
-        ptrs = []
-        for t, n in ((dose_host, self.n_vox), (beam_doses_host, self.n_beams * self.n_vox)):
-            if t is None:
-                ptrs.append(None)
-                continue
-            if (t.device.type != "cpu" or not t.is_pinned() or t.dtype != torch.float32
-                    or t.numel() != n or not t.is_contiguous()):
-                raise ValueError("host outputs must be contiguous page-locked float32 tensors")
-            d = ctypes.c_void_p()
-            if _lib.lib.pb_host_device_pointer(ctypes.c_void_p(t.data_ptr()),
-                                               ctypes.byref(d)) != _lib.PB_OK or not d.value:
-                return False
-            ptrs.append(d.value)
-        order = self.tile_order()
-        check(_lib.lib.pb_dose_ordered(ctypes.byref(self.grid),
-                                       ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
-                                       ptr(self.wet), ptr(self.layers), ptr(self.spot_geo),
-                                       ptr(mu), float(scale), ctypes.c_void_p(ptrs[0]),
-                                       ctypes.c_void_p(ptrs[1]) if ptrs[1] else None,
-                                       ptr(order), _stream(self.device)), "pb_dose_ordered")
-        return True
-
     def forward_variant(self, variant: int, mu_sorted: Optional[torch.Tensor] = None,
                         scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Forward dose with one of the kernel shapes of pb_dose_variant."""

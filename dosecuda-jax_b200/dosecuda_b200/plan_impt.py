@@ -253,19 +253,10 @@ class IMPTDoseGrid(DoseGrid):
             with torch.cuda.stream(side):
                 dp.load_spots()
             main.wait_stream(side)
-            # the kernel writes the doses straight into page-locked host
-            # memory, so that their way back overlaps the computation; where
-            # that memory is not mapped for the device, through device memory
-            V = dp.n_vox
-            dose_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
-            bd_h = torch.empty((dp.n_beams, V), dtype=torch.float32, pin_memory=True)
-            if not dp.forward_to_host(dose_h, bd_h, scale=float(plan.n_fractions)):
-                dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
-                bd_h = _pinned_copy(bd)
-                dose_h = _pinned_copy(dose)
-                keep += [dose, bd]
-            beams_h.append((bd_h, dp.n_beams))
-            keep.append(dp)
+            dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
+            beams_h.append((_pinned_copy(bd), dp.n_beams))
+            dose_h = _pinned_copy(dose)
+            keep += [dose, bd, dp]
         else:
             for chunk in chunks:
                 dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)

@@ -337,14 +337,6 @@ PbStatus pb_batch_setup(const PbBatchPlan *plans, int n_plans, void *work_dev,
 PbStatus pb_batch_run(const PbBatchInfo *info, void *work_dev, int flags, int variant,
                       int blocks_per_sm, int *status_dev, void *stream);
 
-/* The device address of page-locked host memory (cudaHostGetDevicePointer),
- * for outputs that a kernel writes straight to the host while it runs (for
- * pb_dose_ordered's dose and per-beam doses: the copy back then overlaps
- * the computation).  PB_ERR_CUDA, and *device_ptr = NULL, when the memory
- * is not mapped for the current device: copy through device memory then.
- * No counterpart in the reference. */
-PbStatus pb_host_device_pointer(const void *host_ptr, void **device_ptr);
-
 /* Tile order for pb_dose_ordered and pb_dose_adjoint_ordered.  The voxel
  * tiles of the default kernel shape differ in work by more than two orders
  * of magnitude (a tile every beam crosses near the target against one no

@@ -569,25 +569,6 @@ def test_tile_order_on_grids_smaller_than_a_tile(pkg, small):
         assert torch.equal(dp.forward(), d0), shape
 
 
-def test_forward_written_straight_to_host_memory(small):
-    """forward_to_host: the kernel writes dose and per-beam doses into
-    page-locked host tensors, the same bits as the forward into device
-    memory; other host tensors are refused."""
-    dp = small.grid.prepareIMPTPlan(small.plan, 0)
-    d, bd = dp.forward(scale=3.0, beam_doses=True)
-    dh = torch.full((dp.n_vox,), -1.0).pin_memory()
-    bh = torch.full((dp.n_beams, dp.n_vox), -1.0).pin_memory()
-    assert dp.forward_to_host(dh, bh, scale=3.0)
-    torch.cuda.synchronize(DEV)
-    assert torch.equal(dh, d.cpu()) and torch.equal(bh, bd.cpu())
-    dh2 = torch.full((dp.n_vox,), -1.0).pin_memory()
-    assert dp.forward_to_host(dh2, scale=3.0)          # dose alone
-    torch.cuda.synchronize(DEV)
-    assert torch.equal(dh2, d.cpu())
-    with pytest.raises(ValueError, match="page-locked"):
-        dp.forward_to_host(torch.zeros(dp.n_vox))     # pageable
-
-
 def test_adjoint_counts_follow_its_tile_skip(small):
     """pb_count_evaluated_adjoint: on a field nonzero everywhere it counts
     the forward's work; on a zero field nothing; on a field nonzero in one
