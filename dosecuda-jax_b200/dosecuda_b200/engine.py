@@ -180,6 +180,7 @@ class DevicePlan:
         self.wet_mode = "texture"
         self._spec = beams
         self._order: Optional[torch.Tensor] = None    # tile order for the current WET
+        self._beam_orders: Optional[list] = None      # each beam's own tile order
         self._order_work: Optional[torch.Tensor] = None
         self.spots_loaded = False
         if not defer_spots:
@@ -311,6 +312,7 @@ class DevicePlan:
         self.raw_wet = raw
         self.wet_mode = wet_mode
         self._order = None
+        self._beam_orders = None
         return wet
 
     def set_wet(self, wet: torch.Tensor) -> None:
@@ -318,23 +320,43 @@ class DevicePlan:
             raise ValueError("wet must be float32 with n_beams x V elements")
         self.wet = wet.to(self.device).reshape(self.n_beams, self.n_vox).contiguous()
         self._order = None
+        self._beam_orders = None
+
+    def _beam_ptr(self, b: int) -> ctypes.c_void_p:
+        return ctypes.c_void_p(ctypes.addressof(self.beams) + b * ctypes.sizeof(PbBeam))
+
+    def _make_order(self, beams: ctypes.c_void_p, n_beams: int,
+                    wet: torch.Tensor) -> torch.Tensor:
+        n = int(_lib.lib.pb_tile_order_count(ctypes.byref(self.grid)))
+        size = int(_lib.lib.pb_tile_order_work_size(ctypes.byref(self.grid)))
+        if self._order_work is None or self._order_work.numel() < size:
+            self._order_work = torch.empty(size, dtype=torch.uint8, device=self.device)
+        order = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        check(_lib.lib.pb_tile_order(ctypes.byref(self.grid), beams, n_beams, ptr(wet),
+                                     ptr(self.layers), ptr(self._order_work), ptr(order),
+                                     _stream(self.device)), "pb_tile_order")
+        return order
 
     def tile_order(self) -> torch.Tensor:
         """The default shape's tiles, most expensive first, for the current
         WET (pb_tile_order); computed once per WET, stream-ordered."""
         self._need_wet()
         if self._order is None:
-            n = int(_lib.lib.pb_tile_order_count(ctypes.byref(self.grid)))
-            size = int(_lib.lib.pb_tile_order_work_size(ctypes.byref(self.grid)))
-            if self._order_work is None or self._order_work.numel() < size:
-                self._order_work = torch.empty(size, dtype=torch.uint8, device=self.device)
-            order = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
-            check(_lib.lib.pb_tile_order(ctypes.byref(self.grid),
-                                         ctypes.cast(self.beams, ctypes.c_void_p), self.n_beams,
-                                         ptr(self.wet), ptr(self.layers), ptr(self._order_work),
-                                         ptr(order), _stream(self.device)), "pb_tile_order")
-            self._order = order
+            self._order = self._make_order(ctypes.cast(self.beams, ctypes.c_void_p),
+                                           self.n_beams, self.wet)
         return self._order
+
+    def beam_tile_order(self, b: int) -> torch.Tensor:
+        """Beam b's tiles alone, most expensive first (pb_tile_order on that
+        beam); computed once per WET, stream-ordered."""
+        self._need_wet()
+        if not 0 <= b < self.n_beams:
+            raise IndexError(f"beam {b} of {self.n_beams}")
+        if self._beam_orders is None:
+            self._beam_orders = [None] * self.n_beams
+        if self._beam_orders[b] is None:
+            self._beam_orders[b] = self._make_order(self._beam_ptr(b), 1, self.wet[b])
+        return self._beam_orders[b]
 
     def _need_wet(self):
         if not self.spots_loaded:
@@ -362,6 +384,26 @@ class DevicePlan:
                                        ptr(mu), float(scale), ptr(dose), ptr(bd), ptr(order),
                                        _stream(self.device)), "pb_dose_ordered")
         return (dose, bd) if beam_doses else dose
+
+    def forward_beam(self, b: int, mu_sorted: Optional[torch.Tensor] = None,
+                     scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Beam b's dose alone (V): the kernel run on that beam, in its own
+        tile order; the same values as forward()'s per-beam dose of b."""
+        self._need_wet()
+        mu = self.mu_sorted if mu_sorted is None else mu_sorted
+        if mu.dtype != torch.float32 or mu.numel() != self.n_spots:
+            raise ValueError("mu must be float32 with one entry per spot")
+        mu = mu.contiguous()
+        order = self.beam_tile_order(b)
+        dose = out if out is not None else torch.empty(self.n_vox, dtype=torch.float32,
+                                                       device=self.device)
+        if dose.numel() != self.n_vox or not dose.is_contiguous():
+            raise ValueError("out must be a contiguous tensor of V floats")
+        check(_lib.lib.pb_dose_ordered(ctypes.byref(self.grid), self._beam_ptr(b), 1,
+                                       ptr(self.wet[b]), ptr(self.layers), ptr(self.spot_geo),
+                                       ptr(mu), float(scale), ptr(dose), None, ptr(order),
+                                       _stream(self.device)), "pb_dose_ordered")
+        return dose
 
     def forward_variant(self, variant: int, mu_sorted: Optional[torch.Tensor] = None,
                         scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:

@@ -218,8 +218,11 @@ class IMPTDoseGrid(DoseGrid):
 
         The results come back into page-locked host memory from torch's
         pinned-memory cache (reused once the previous call's arrays are
-        released), and the RLSP volume's copy runs on a second stream while
-        the WET and dose are computed."""
+        released).  The RLSP volume's copy runs on a second stream while the
+        WET and dose are computed, and the beams' doses are computed one
+        beam at a time (engine.DevicePlan.forward_beam), each copied back
+        while the next is computed; the plan dose is their float32 sum times
+        n_fractions, as the reference forms it."""
         self.beam_doses = []
         self._check_isotropic()
         if not plan.beam_list:
@@ -253,8 +256,29 @@ class IMPTDoseGrid(DoseGrid):
             with torch.cuda.stream(side):
                 dp.load_spots()
             main.wait_stream(side)
-            dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
-            beams_h.append((_pinned_copy(bd), dp.n_beams))
+            # one beam at a time, each in its own tile order, so that each
+            # beam's dose goes back to the host while the next is computed;
+            # the plan dose is the beams' sum as the reference forms it
+            # (plan_impt.py:201-206)
+            nf = float(plan.n_fractions)
+            V, nb = dp.n_vox, dp.n_beams
+            bd = torch.empty((nb, V), dtype=torch.float32, device=device)
+            dose = torch.empty(V, dtype=torch.float32, device=device)
+            bd_h = torch.empty((nb, V), dtype=torch.float32, pin_memory=True)
+            for b in range(nb):
+                dp.forward_beam(b, out=bd[b])
+                if b == 0:
+                    dose.copy_(bd[0])
+                else:
+                    dose.add_(bd[b])
+                if nf != 1.0:
+                    bd[b].mul_(nf)
+                side.wait_stream(main)
+                with torch.cuda.stream(side):
+                    bd_h[b].copy_(bd[b], non_blocking=True)
+            if nf != 1.0:
+                dose.mul_(nf)
+            beams_h.append((bd_h, nb))
             dose_h = _pinned_copy(dose)
             keep += [dose, bd, dp]
         else:

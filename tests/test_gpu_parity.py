@@ -569,6 +569,33 @@ def test_tile_order_on_grids_smaller_than_a_tile(pkg, small):
         assert torch.equal(dp.forward(), d0), shape
 
 
+def test_beam_at_a_time_forward_and_compute_plan(small):
+    """forward_beam(b), each beam alone in its own tile order, gives the
+    bits of the all-beam launch's per-beam dose; computeIMPTPlan, which
+    runs the beams one at a time, returns those doses times n_fractions and
+    their float32 sum times n_fractions, as the reference forms them
+    (plan_impt.py:201-206)."""
+    g, plan = small.grid, small.plan
+    dp = g.prepareIMPTPlan(plan, 0)
+    _, bd = dp.forward(beam_doses=True)
+    for b in range(dp.n_beams):
+        order = dp.beam_tile_order(b).cpu()
+        assert torch.equal(order.sort().values, torch.arange(order.numel(), dtype=order.dtype))
+        assert torch.equal(dp.forward_beam(b), bd[b])
+    bd = bd.cpu().numpy()
+    plan.n_fractions = 3
+    try:
+        g.computeIMPTPlan(plan, 0)
+    finally:
+        plan.n_fractions = 1
+    want = np.zeros(bd.shape[1], np.float32)
+    for b in range(bd.shape[0]):
+        assert np.array_equal(g.beam_doses[b].reshape(-1), bd[b] * np.float32(3))
+        want += bd[b]
+    want *= np.float32(3)
+    assert np.array_equal(g.dose.reshape(-1), want)
+
+
 def test_adjoint_counts_follow_its_tile_skip(small):
     """pb_count_evaluated_adjoint: on a field nonzero everywhere it counts
     the forward's work; on a zero field nothing; on a field nonzero in one
