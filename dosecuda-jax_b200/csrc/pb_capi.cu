@@ -322,6 +322,13 @@ long long pb_tile_order_count(const PbGrid *grid)
     return check_grid(grid) == PB_OK ? tile_order_count(*grid) : -1;
 }
 
+PbStatus pb_tile_order_tile(int *tile_voxels)
+{
+    if (!tile_voxels) return set_error(PB_ERR_INVALID, "tile_voxels is NULL");
+    tile_order_tile(tile_voxels);
+    return PB_OK;
+}
+
 size_t pb_tile_order_work_size(const PbGrid *grid)
 {
     return check_grid(grid) == PB_OK ? tile_order_work_size(*grid) : 0;

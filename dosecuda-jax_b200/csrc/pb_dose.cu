@@ -2394,6 +2394,13 @@ PbStatus launch_layer_bounds(const PbBeam *beams, int n_beams, PbLayer *layers,
 
 long long tile_order_count(const PbGrid &g) { return line_tiles(g, kLineTY, kLineTZ); }
 
+void tile_order_tile(int *voxels)
+{
+    voxels[0] = kLine;
+    voxels[1] = kLineTY;
+    voxels[2] = kLineTZ;
+}
+
 size_t tile_order_work_size(const PbGrid &g)
 {
     const size_t n = (size_t)tile_order_count(g);

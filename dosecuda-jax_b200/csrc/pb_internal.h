@@ -90,6 +90,7 @@ PbStatus launch_adjoint(const PbGrid &g, const PbBeam *beams, int n_beams,
                         float *grad, cudaStream_t st, int variant = -1,
                         const int *order = nullptr);
 long long tile_order_count(const PbGrid &g);
+void tile_order_tile(int *voxels);
 size_t tile_order_work_size(const PbGrid &g);
 PbStatus launch_tile_order(const PbGrid &g, const PbBeam *beams, int n_beams, const float *wet,
                            const PbLayer *layers, void *work, int *order, cudaStream_t st);

@@ -140,6 +140,7 @@ _SIGS = {
                                        _F, _VP, _VP, _VP, _VP]),
     "pb_count_evaluated": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _VP]),
     "pb_tile_order_count": (ctypes.c_longlong, [ctypes.POINTER(PbGrid)]),
+    "pb_tile_order_tile": (_I, [ctypes.POINTER(ctypes.c_int)]),
     "pb_tile_order_work_size": (ctypes.c_size_t, [ctypes.POINTER(PbGrid)]),
     "pb_tile_order": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, _VP]),
     "pb_dose_ordered": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP, ctypes.c_float,

@@ -385,16 +385,45 @@ class DevicePlan:
                                        _stream(self.device)), "pb_dose_ordered")
         return (dose, bd) if beam_doses else dose
 
+    def beam_tile_order_halves(self, b: int):
+        """Beam b's tile order split at the middle z slab of tiles: (lower,
+        upper, v_split), each order padded with -1 to the full count (the
+        kernel skips those entries), the lower one covering exactly the
+        first v_split voxels (z fastest-varying last).  v_split is 0, and
+        lower None, when the grid has a single slab of tiles."""
+        order = self.beam_tile_order(b)
+        tile = (ctypes.c_int * 3)()
+        check(_lib.lib.pb_tile_order_tile(tile), "pb_tile_order_tile")
+        nx, ny, nz = self.grid.nx, self.grid.ny, self.grid.nz
+        per_slab = -(-nx // tile[0]) * -(-ny // tile[1])
+        slabs_lo = (-(-nz // tile[2])) // 2
+        if slabs_lo == 0:
+            return None, order, 0
+        n_lo = per_slab * slabs_lo
+        upper = (order >= n_lo).to(torch.int8)
+        ranked = order[torch.sort(upper, stable=True).indices]
+        pad = torch.full((order.numel(),), -1, dtype=order.dtype, device=order.device)
+        lower = torch.cat([ranked[:n_lo], pad[n_lo:]])
+        higher = torch.cat([ranked[n_lo:], pad[:n_lo]])
+        return lower, higher, nx * ny * tile[2] * slabs_lo
+
     def forward_beam(self, b: int, mu_sorted: Optional[torch.Tensor] = None,
-                     scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+                     scale: float = 1.0, out: Optional[torch.Tensor] = None,
+                     order: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Beam b's dose alone (V): the kernel run on that beam, in its own
-        tile order; the same values as forward()'s per-beam dose of b."""
+        tile order; the same values as forward()'s per-beam dose of b.  With
+        `order` (beam_tile_order_halves) only the tiles it lists are
+        computed."""
         self._need_wet()
         mu = self.mu_sorted if mu_sorted is None else mu_sorted
         if mu.dtype != torch.float32 or mu.numel() != self.n_spots:
             raise ValueError("mu must be float32 with one entry per spot")
         mu = mu.contiguous()
-        order = self.beam_tile_order(b)
+        if order is None:
+            order = self.beam_tile_order(b)
+        elif (order.dtype != torch.int32 or order.device != self.device
+              or order.numel() != self.beam_tile_order(b).numel()):
+            raise ValueError("order must be an int32 device tensor of the full tile count")
         dose = out if out is not None else torch.empty(self.n_vox, dtype=torch.float32,
                                                        device=self.device)
         if dose.numel() != self.n_vox or not dose.is_contiguous():

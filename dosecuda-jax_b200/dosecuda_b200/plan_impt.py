@@ -241,54 +241,66 @@ class IMPTDoseGrid(DoseGrid):
         with torch.cuda.stream(side):
             rlsp_h = _pinned_copy(rlsp)
         chunks = self._beam_chunks(plan)
-        total, beams_h, keep = None, [], []
-        if len(chunks) == 1:
-            # the WET is queued first; the spots are sorted into layers and
-            # uploaded on the copy stream while it runs
-            pool = self.__dict__.get("_pb_texture_pool")
-            if pool is None:
-                pool = self._pb_texture_pool = _engine().TexturePool()
-            dp = _engine().DevicePlan(shape, float(self.spacing[0]),
-                                      np.asarray(self.origin, dtype=np.single),
-                                      self._specs(plan, chunks[0]), device, texture_pool=pool,
-                                      defer_spots=True)
-            dp.compute_wet(rlsp.reshape(-1), check_status=False, wet_mode=wet_mode)
-            with torch.cuda.stream(side):
-                dp.load_spots()
-            main.wait_stream(side)
+        beams_h, keep = [], []
+        nf = float(plan.n_fractions)
+        V = int(np.prod(shape))
+        dose = torch.empty(V, dtype=torch.float32, device=device)
+        dose_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
+        keep.append(dose)
+        n_done = 0
+        for chunk in chunks:
+            if len(chunks) == 1:
+                # the WET is queued first; the spots are sorted into layers
+                # and uploaded on the copy stream while it runs
+                pool = self.__dict__.get("_pb_texture_pool")
+                if pool is None:
+                    pool = self._pb_texture_pool = _engine().TexturePool()
+                dp = _engine().DevicePlan(shape, float(self.spacing[0]),
+                                          np.asarray(self.origin, dtype=np.single),
+                                          self._specs(plan, chunk), device, texture_pool=pool,
+                                          defer_spots=True)
+                dp.compute_wet(rlsp.reshape(-1), check_status=False, wet_mode=wet_mode)
+                with torch.cuda.stream(side):
+                    dp.load_spots()
+                main.wait_stream(side)
+            else:
+                dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
             # one beam at a time, each in its own tile order, so that each
             # beam's dose goes back to the host while the next is computed;
-            # the plan dose is the beams' sum as the reference forms it
-            # (plan_impt.py:201-206)
-            nf = float(plan.n_fractions)
-            V, nb = dp.n_vox, dp.n_beams
+            # the plan dose is the beams' float32 sum times n_fractions, as
+            # the reference forms it (plan_impt.py:201-206)
+            # The plan's last beam runs as two launches, the lower and the
+            # upper half of the z slabs of tiles, so that the lower half of
+            # its dose and of the plan dose go back during the second.
+            nb = dp.n_beams
             bd = torch.empty((nb, V), dtype=torch.float32, device=device)
-            dose = torch.empty(V, dtype=torch.float32, device=device)
             bd_h = torch.empty((nb, V), dtype=torch.float32, pin_memory=True)
             for b in range(nb):
-                dp.forward_beam(b, out=bd[b])
-                if b == 0:
-                    dose.copy_(bd[0])
-                else:
-                    dose.add_(bd[b])
-                if nf != 1.0:
-                    bd[b].mul_(nf)
-                side.wait_stream(main)
-                with torch.cuda.stream(side):
-                    bd_h[b].copy_(bd[b], non_blocking=True)
-            if nf != 1.0:
-                dose.mul_(nf)
+                last = chunk is chunks[-1] and b == nb - 1
+                parts = [(None, 0, V)]
+                if last:
+                    lower, upper, vs = dp.beam_tile_order_halves(b)
+                    if lower is not None:
+                        parts = [(lower, 0, vs), (upper, vs, V)]
+                for order, v0, v1 in parts:
+                    dp.forward_beam(b, out=bd[b], order=order)
+                    d, db = dose[v0:v1], bd[b, v0:v1]
+                    if n_done == 0:
+                        d.copy_(db)
+                    else:
+                        d.add_(db)
+                    if nf != 1.0:
+                        db.mul_(nf)
+                        if last:
+                            d.mul_(nf)
+                    side.wait_stream(main)
+                    with torch.cuda.stream(side):
+                        bd_h[b, v0:v1].copy_(db, non_blocking=True)
+                        if last:
+                            dose_h[v0:v1].copy_(d, non_blocking=True)
+                n_done += 1
             beams_h.append((bd_h, nb))
-            dose_h = _pinned_copy(dose)
-            keep += [dose, bd, dp]
-        else:
-            for chunk in chunks:
-                dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
-                dose, bd = dp.forward(scale=float(plan.n_fractions), beam_doses=True)
-                beams_h.append((_pinned_copy(bd), dp.n_beams))
-                keep.append(bd)
-                total = dose if total is None else total + dose
-            dose_h = _pinned_copy(total)
+            keep += [bd, dp]
         main.synchronize()
         side.synchronize()
         if len(chunks) == 1 and int(dp._status.item()) & _engine()._lib.PB_ERR_RAY_CAP:

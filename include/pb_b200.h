@@ -348,8 +348,14 @@ PbStatus pb_batch_run(const PbBatchInfo *info, void *work_dev, int flags, int va
  * pb_tile_order_work_size bytes of scratch.  Stream-ordered, no
  * allocation.  The order depends on the WET: compute it again when the WET
  * changes (a stale order gives the same results, only its speed-up is
- * lost).  No counterpart in the reference. */
+ * lost).  Tile index o is raster order, x fastest: with the tile extent
+ * (tx, ty, tz) voxels from pb_tile_order_tile and nx8 = ceil(nx / tx),
+ * nty = ceil(ny / ty), tile o covers z slab o / (nx8 * nty).  An order
+ * entry outside [0, count) is skipped: an order padded with -1 runs only
+ * the tiles it lists and leaves the other voxels' doses unwritten.  No
+ * counterpart in the reference. */
 long long pb_tile_order_count(const PbGrid *grid);
+PbStatus pb_tile_order_tile(int *tile_voxels);   /* 3 ints: x, y, z extent */
 size_t pb_tile_order_work_size(const PbGrid *grid);
 PbStatus pb_tile_order(const PbGrid *grid, const PbBeam *beams, int n_beams,
                        const float *wet_dev, const PbLayer *layers_dev, void *work_dev,

@@ -141,6 +141,9 @@ def test_invalid_arguments_return_status_without_a_gpu():
     g = _lib.PbGrid(256, 256, 160, 2.0)
     n = L.pb_tile_order_count(ctypes.byref(g))
     assert n == 32 * 16 * 20                          # 8 x 16 x 8 voxel tiles
+    tile = (ctypes.c_int * 3)()
+    assert L.pb_tile_order_tile(tile) == _lib.PB_OK and list(tile) == [8, 16, 8]
+    assert L.pb_tile_order_tile(None) == _lib.PB_ERR_INVALID
     assert L.pb_tile_order_work_size(ctypes.byref(g)) >= 4 * n + 4096
     bad = _lib.PbGrid(0, 4, 4, 2.0)
     assert L.pb_tile_order_count(ctypes.byref(bad)) == -1

@@ -582,6 +582,18 @@ def test_beam_at_a_time_forward_and_compute_plan(small):
         order = dp.beam_tile_order(b).cpu()
         assert torch.equal(order.sort().values, torch.arange(order.numel(), dtype=order.dtype))
         assert torch.equal(dp.forward_beam(b), bd[b])
+    # the last beam in two launches, the lower and the upper z slabs of tiles
+    b = dp.n_beams - 1
+    lower, upper, vs = dp.beam_tile_order_halves(b)
+    assert lower is not None and 0 < vs < dp.n_vox
+    n = lower.numel()
+    both = torch.cat([lower[lower >= 0], upper[upper >= 0]]).cpu()
+    assert torch.equal(both.sort().values, torch.arange(n, dtype=both.dtype))
+    out = torch.full((dp.n_vox,), float("nan"), device=DEV)
+    dp.forward_beam(b, out=out, order=lower)
+    assert torch.equal(out[:vs], bd[b, :vs]) and bool(torch.isnan(out[vs:]).all())
+    dp.forward_beam(b, out=out, order=upper)
+    assert torch.equal(out, bd[b])
     bd = bd.cpu().numpy()
     plan.n_fractions = 3
     try:
