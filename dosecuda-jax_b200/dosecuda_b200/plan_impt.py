@@ -105,10 +105,26 @@ class IMPTBeamModel():
         return energy_row.index[0]
 
 
+_HU_CURVES = {}
+
+
 def _hu_curve(machine_name):
-    df = pd.read_csv(resource_filename(os.path.join("lookuptables", "protons", machine_name,
-                                                    "HU_RLSP.csv")))
-    return df["HU"].to_numpy(dtype=np.float64), df["RLSP"].to_numpy(dtype=np.float64)
+    """The machine's HU -> RLSP curve (HU_RLSP.csv), read again only when
+    the file changes (the reference reads it on every call,
+    plan_impt.py:158-168)."""
+    path = resource_filename(os.path.join("lookuptables", "protons", machine_name,
+                                          "HU_RLSP.csv"))
+    st = os.stat(path)
+    key = (st.st_mtime_ns, st.st_size)
+    hit = _HU_CURVES.get(path)
+    if hit is None or hit[0] != key:
+        df = pd.read_csv(path)
+        xh = df["HU"].to_numpy(dtype=np.float64)
+        yh = df["RLSP"].to_numpy(dtype=np.float64)
+        xh.setflags(write=False)
+        yh.setflags(write=False)
+        hit = _HU_CURVES[path] = (key, xh, yh)
+    return hit[1], hit[2]
 
 
 def _pinned_copy(t: torch.Tensor) -> torch.Tensor:
@@ -236,7 +252,9 @@ class IMPTDoseGrid(DoseGrid):
         rlsp = self._rlsp_device(plan.machine_name, device)
         side = self.__dict__.get("_pb_copy_stream")
         if side is None or side.device != device:
-            side = self._pb_copy_stream = torch.cuda.Stream(device)
+            # high priority: its small kernels (tile orders) start while the
+            # main stream's dose kernel still has blocks waiting
+            side = self._pb_copy_stream = torch.cuda.Stream(device, priority=-1)
         side.wait_stream(main)
         with torch.cuda.stream(side):
             rlsp_h = _pinned_copy(rlsp)
@@ -272,16 +290,29 @@ class IMPTDoseGrid(DoseGrid):
             # The plan's last beam runs as two launches, the lower and the
             # upper half of the z slabs of tiles, so that the lower half of
             # its dose and of the plan dose go back during the second.
+            # The first beam's tile order on the main stream, the others'
+            # (and the last beam's halves) on the copy stream while the
+            # first beam's dose is computed.
             nb = dp.n_beams
+            final = chunk is chunks[-1]
             bd = torch.empty((nb, V), dtype=torch.float32, device=device)
             bd_h = torch.empty((nb, V), dtype=torch.float32, pin_memory=True)
+            dp.beam_tile_order(0)
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                for b in range(1, nb):
+                    dp.beam_tile_order(b)
+                halves = dp.beam_tile_order_halves(nb - 1) if final else None
+                orders_ready = torch.cuda.Event()
+                orders_ready.record(side)
             for b in range(nb):
-                last = chunk is chunks[-1] and b == nb - 1
+                if b == 1 or (b == 0 and final and nb == 1):
+                    main.wait_event(orders_ready)
+                last = final and b == nb - 1
                 parts = [(None, 0, V)]
-                if last:
-                    lower, upper, vs = dp.beam_tile_order_halves(b)
-                    if lower is not None:
-                        parts = [(lower, 0, vs), (upper, vs, V)]
+                if last and halves[0] is not None:
+                    lower, upper, vs = halves
+                    parts = [(lower, 0, vs), (upper, vs, V)]
                 for order, v0, v1 in parts:
                     dp.forward_beam(b, out=bd[b], order=order)
                     d, db = dose[v0:v1], bd[b, v0:v1]
