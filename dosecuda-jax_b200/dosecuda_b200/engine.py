@@ -385,34 +385,43 @@ class DevicePlan:
                                        _stream(self.device)), "pb_dose_ordered")
         return (dose, bd) if beam_doses else dose
 
-    def beam_tile_order_halves(self, b: int):
-        """Beam b's tile order split at the middle z slab of tiles: (lower,
-        upper, v_split), each order padded with -1 to the full count (the
-        kernel skips those entries), the lower one covering exactly the
-        first v_split voxels (z fastest-varying last).  v_split is 0, and
-        lower None, when the grid has a single slab of tiles."""
+    def beam_tile_order_parts(self, b: int, n_parts: int):
+        """Beam b's tile order split into up to n_parts groups of whole z
+        slabs of tiles, lowest z first: a list of (order, v0, v1), each order
+        the group's tiles most expensive first, padded with -1 to the full
+        count (the kernel skips those entries), covering exactly voxels
+        v0 <= v < v1 (z varies slowest).  One group when the grid has a
+        single slab of tiles."""
         order = self.beam_tile_order(b)
         tile = (ctypes.c_int * 3)()
         check(_lib.lib.pb_tile_order_tile(tile), "pb_tile_order_tile")
         nx, ny, nz = self.grid.nx, self.grid.ny, self.grid.nz
         per_slab = -(-nx // tile[0]) * -(-ny // tile[1])
-        slabs_lo = (-(-nz // tile[2])) // 2
-        if slabs_lo == 0:
-            return None, order, 0
-        n_lo = per_slab * slabs_lo
-        upper = (order >= n_lo).to(torch.int8)
-        ranked = order[torch.sort(upper, stable=True).indices]
+        n_slabs = -(-nz // tile[2])
+        n_parts = max(1, min(int(n_parts), n_slabs))
+        if n_parts == 1:
+            return [(order, 0, self.n_vox)]
+        # group of slab tz: tz * n_parts // n_slabs (non-decreasing in tz)
+        group = (order // per_slab) * n_parts // n_slabs
+        ranked = order[torch.sort(group, stable=True).indices]
         pad = torch.full((order.numel(),), -1, dtype=order.dtype, device=order.device)
-        lower = torch.cat([ranked[:n_lo], pad[n_lo:]])
-        higher = torch.cat([ranked[n_lo:], pad[:n_lo]])
-        return lower, higher, nx * ny * tile[2] * slabs_lo
+        parts, t0, z0 = [], 0, 0
+        for p in range(n_parts):
+            z1 = z0
+            while z1 < n_slabs and z1 * n_parts // n_slabs == p:
+                z1 += 1
+            t1 = t0 + (z1 - z0) * per_slab
+            part = torch.cat([ranked[t0:t1], pad[:order.numel() - (t1 - t0)]])
+            parts.append((part, nx * ny * min(z0 * tile[2], nz), nx * ny * min(z1 * tile[2], nz)))
+            t0, z0 = t1, z1
+        return parts
 
     def forward_beam(self, b: int, mu_sorted: Optional[torch.Tensor] = None,
                      scale: float = 1.0, out: Optional[torch.Tensor] = None,
                      order: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Beam b's dose alone (V): the kernel run on that beam, in its own
         tile order; the same values as forward()'s per-beam dose of b.  With
-        `order` (beam_tile_order_halves) only the tiles it lists are
+        `order` (one of beam_tile_order_parts) only the tiles it lists are
         computed."""
         self._need_wet()
         mu = self.mu_sorted if mu_sorted is None else mu_sorted

@@ -107,6 +107,9 @@ class IMPTBeamModel():
 
 _HU_CURVES = {}
 
+# launches of a plan's last beam in computeIMPTPlan (groups of z slabs)
+_TAIL_PARTS = 4
+
 
 def _hu_curve(machine_name):
     """The machine's HU -> RLSP curve (HU_RLSP.csv), read again only when
@@ -265,7 +268,10 @@ class IMPTDoseGrid(DoseGrid):
         dose = torch.empty(V, dtype=torch.float32, device=device)
         dose_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
         keep.append(dose)
-        n_done = 0
+        first_beam = True
+        comp = self.__dict__.get("_pb_compute_stream")
+        if comp is None or comp.device != device:
+            comp = self._pb_compute_stream = torch.cuda.Stream(device)
         for chunk in chunks:
             if len(chunks) == 1:
                 # the WET is queued first; the spots are sorted into layers
@@ -291,8 +297,11 @@ class IMPTDoseGrid(DoseGrid):
             # upper half of the z slabs of tiles, so that the lower half of
             # its dose and of the plan dose go back during the second.
             # The first beam's tile order on the main stream, the others'
-            # (and the last beam's halves) on the copy stream while the
-            # first beam's dose is computed.
+            # (and the last beam's z groups) on the copy stream while the
+            # first beam's dose is computed.  The plan's last beam runs as
+            # _TAIL_PARTS launches over groups of z slabs of tiles, so that
+            # only the last group's doses remain to be copied back after
+            # the last launch.
             nb = dp.n_beams
             final = chunk is chunks[-1]
             bd = torch.empty((nb, V), dtype=torch.float32, device=device)
@@ -302,21 +311,30 @@ class IMPTDoseGrid(DoseGrid):
             with torch.cuda.stream(side):
                 for b in range(1, nb):
                     dp.beam_tile_order(b)
-                halves = dp.beam_tile_order_halves(nb - 1) if final else None
+                parts = dp.beam_tile_order_parts(nb - 1, _TAIL_PARTS) if final else None
                 orders_ready = torch.cuda.Event()
                 orders_ready.record(side)
-            for b in range(nb):
-                if b == 1 or (b == 0 and final and nb == 1):
-                    main.wait_event(orders_ready)
-                last = final and b == nb - 1
-                parts = [(None, 0, V)]
-                if last and halves[0] is not None:
-                    lower, upper, vs = halves
-                    parts = [(lower, 0, vs), (upper, vs, V)]
-                for order, v0, v1 in parts:
+            launches = [(b, None, 0, V) for b in range(nb)]
+            if final and len(parts) > 1:
+                launches[-1:] = [(nb - 1, o, v0, v1) for o, v0, v1 in parts]
+            # The launches alternate between two compute streams, so that a
+            # launch's last blocks share the SMs with the next launch's
+            # first ones; the copy stream adds each finished part into the
+            # plan dose, in beam order, and copies it back.
+            comp.wait_stream(main)
+            for idx, (b, order, v0, v1) in enumerate(launches):
+                st = main if idx % 2 == 0 else comp
+                if idx > 0 or order is not None:
+                    st.wait_event(orders_ready)
+                with torch.cuda.stream(st):
                     dp.forward_beam(b, out=bd[b], order=order)
+                    done = torch.cuda.Event()
+                    done.record(st)
+                side.wait_event(done)
+                last = final and b == nb - 1
+                with torch.cuda.stream(side):
                     d, db = dose[v0:v1], bd[b, v0:v1]
-                    if n_done == 0:
+                    if first_beam and b == 0:
                         d.copy_(db)
                     else:
                         d.add_(db)
@@ -324,12 +342,11 @@ class IMPTDoseGrid(DoseGrid):
                         db.mul_(nf)
                         if last:
                             d.mul_(nf)
-                    side.wait_stream(main)
-                    with torch.cuda.stream(side):
-                        bd_h[b, v0:v1].copy_(db, non_blocking=True)
-                        if last:
-                            dose_h[v0:v1].copy_(d, non_blocking=True)
-                n_done += 1
+                    bd_h[b, v0:v1].copy_(db, non_blocking=True)
+                    if last:
+                        dose_h[v0:v1].copy_(d, non_blocking=True)
+            first_beam = False
+            main.wait_stream(comp)
             beams_h.append((bd_h, nb))
             keep += [bd, dp]
         main.synchronize()

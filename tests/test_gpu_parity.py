@@ -582,18 +582,20 @@ def test_beam_at_a_time_forward_and_compute_plan(small):
         order = dp.beam_tile_order(b).cpu()
         assert torch.equal(order.sort().values, torch.arange(order.numel(), dtype=order.dtype))
         assert torch.equal(dp.forward_beam(b), bd[b])
-    # the last beam in two launches, the lower and the upper z slabs of tiles
+    # the last beam in launches over groups of z slabs of tiles (5 slabs
+    # here): each fills exactly its voxel range, together the whole volume
     b = dp.n_beams - 1
-    lower, upper, vs = dp.beam_tile_order_halves(b)
-    assert lower is not None and 0 < vs < dp.n_vox
-    n = lower.numel()
-    both = torch.cat([lower[lower >= 0], upper[upper >= 0]]).cpu()
-    assert torch.equal(both.sort().values, torch.arange(n, dtype=both.dtype))
-    out = torch.full((dp.n_vox,), float("nan"), device=DEV)
-    dp.forward_beam(b, out=out, order=lower)
-    assert torch.equal(out[:vs], bd[b, :vs]) and bool(torch.isnan(out[vs:]).all())
-    dp.forward_beam(b, out=out, order=upper)
-    assert torch.equal(out, bd[b])
+    n = dp.beam_tile_order(b).numel()
+    for k in (1, 2, 4, 9):
+        parts = dp.beam_tile_order_parts(b, k)
+        assert len(parts) == min(k, 5) and parts[0][1] == 0 and parts[-1][2] == dp.n_vox
+        listed = torch.cat([o[o >= 0] for o, _, _ in parts]).cpu()
+        assert torch.equal(listed.sort().values, torch.arange(n, dtype=listed.dtype))
+        out = torch.full((dp.n_vox,), float("nan"), device=DEV)
+        for o, v0, v1 in parts:
+            assert v0 < v1
+            dp.forward_beam(b, out=out, order=o)
+            assert torch.equal(out[:v1], bd[b, :v1]) and bool(torch.isnan(out[v1:]).all())
     bd = bd.cpu().numpy()
     plan.n_fractions = 3
     try:
