@@ -1450,8 +1450,9 @@ __device__ __forceinline__ void line_tile(const PlanArgs &A, int tx, int ty, int
                             sh.gsum[sl] = 0.0f;
                         }
                     } else {
-                        // both terms
-#pragma unroll 2
+                        // both terms (unrolled by 4: the per-beam forward
+                        // 6.37 against 6.49 ms, the plain one unchanged)
+#pragma unroll 4
                         for (int c = 0; c < n2; ++c) {
                             const LineSpot r = sh.spot[c];
                             float S0, B1;
@@ -1684,8 +1685,11 @@ k_adjoint_line(const __grid_constant__ PlanArgs A, const float *__restrict__ wet
 // work is done, not what each tile computes.
 
 // Cost units: one spot evaluated over a tile; a kept (tile, layer) pair
-// also pays its per-voxel Gaussian parameters and the cull, about this many.
-constexpr float kPairCost = 24.0f;
+// also pays its per-voxel Gaussian parameters, the cull and its barriers,
+// about this many.  Measured on the 4-beam 256x256x160 plan (forward /
+// adjoint): 24 -> 6.04 / 6.43 ms, 48 -> 6.03 / 6.41, 96 -> 6.02 / 6.39,
+// 192 -> 6.02 / 6.38.
+constexpr float kPairCost = 192.0f;
 constexpr int kOrderBuckets = 1024;
 
 // Estimated work of a kept (tile, layer) pair: kPairCost plus the layer's
