@@ -22,9 +22,10 @@ metric  spot-voxel evals/s = E / t_step, where E is the reference kernel's
 
 `value` is timed with the inputs already in HBM.  `e2e` is the same step
 through the public host API: in forward mode IMPTDoseGrid.computeIMPTPlan
-(host HU in; host dose, per-beam doses and RLSP out, as the reference's
-computeIMPTPlan returns them), in grad mode the library's host-buffer
-optimiser step.
+(host HU in, the grid's own numpy array, which that call page-locks in
+place from its second use; host dose, per-beam doses and RLSP out, as the
+reference's computeIMPTPlan returns them), in grad mode the library's
+host-buffer optimiser step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
                     [--mode forward|grad] [--workload plan|batch|optimize]
@@ -301,9 +302,10 @@ def run_mine(args, world, rank, local):
     def e2e_grad():
         host_step(hu_h, presc_h, wts_h, mu_h, dose_out, grad_out, obj_out)
 
-    # the step's input in page-locked host memory (the same values): the
-    # HU volume goes up asynchronously
-    g.HU = hu_h.numpy().reshape(np.shape(g.HU))
+    # the step's input is the grid's own float32 numpy array, as a caller
+    # of the reference has it; computeIMPTPlan page-locks it in place on its
+    # second use (a warm-up call), so the timed calls upload it by DMA
+    assert g.HU.dtype == np.float32 and g.HU.flags.c_contiguous
 
     def e2e_forward():
         # the reference's call: host HU in; host dose, per-beam doses and

@@ -472,6 +472,28 @@ PbStatus pb_count_evaluated_adjoint(const PbGrid *grid, const PbBeam *beams, int
                                   dobj_dose_dev, scale);
 }
 
+PbStatus pb_host_register(void *host_ptr, size_t bytes)
+{
+    if (!host_ptr || bytes == 0) return set_error(PB_ERR_INVALID, "NULL or empty host range");
+    const cudaError_t e = cudaHostRegister(host_ptr, bytes, cudaHostRegisterDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();   // leave no error behind for the next launch check
+        return set_error(PB_ERR_CUDA, "cudaHostRegister: %s", cudaGetErrorString(e));
+    }
+    return PB_OK;
+}
+
+PbStatus pb_host_unregister(void *host_ptr)
+{
+    if (!host_ptr) return set_error(PB_ERR_INVALID, "NULL host pointer");
+    const cudaError_t e = cudaHostUnregister(host_ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PB_ERR_CUDA, "cudaHostUnregister: %s", cudaGetErrorString(e));
+    }
+    return PB_OK;
+}
+
 PbStatus pb_measure_ex2_rate(double *ops_per_s, void *stream)
 {
     if (!ops_per_s) return set_error(PB_ERR_INVALID, "ops_per_s is NULL");

@@ -150,6 +150,8 @@ _SIGS = {
     "pb_count_evaluated_adjoint": (_I, [ctypes.POINTER(PbGrid), _VP, _I, _VP, _VP, _VP, _VP,
                                         ctypes.c_float, _VP, _VP]),
     "pb_measure_ex2_rate": (_I, [ctypes.POINTER(ctypes.c_double), _VP]),
+    "pb_host_register": (_I, [_VP, ctypes.c_size_t]),
+    "pb_host_unregister": (_I, [_VP]),
     "pb_proton_raytrace_host": (_I, [_I, _D, _D, _VP, _VP, _F, _VP, _VP, _D, _D, _VP]),
     "pb_proton_spot_host": (_I, [_I, _D, _D, _VP, _VP, _VP, _VP, _I, _I, _I, _VP, _VP, _F,
                                  _VP, _VP, _D, _D, _VP, _I, _VP]),

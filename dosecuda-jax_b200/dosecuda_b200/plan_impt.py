@@ -12,8 +12,10 @@ Beyond the reference:
 """
 from __future__ import annotations
 
+import ctypes
 import os
 import sys
+import weakref
 
 import numpy as np
 import pandas as pd
@@ -130,6 +132,44 @@ def _hu_curve(machine_name):
     return hit[1], hit[2]
 
 
+# Caller HU arrays seen once (address, bytes) -> weak reference, and those
+# page-locked in place.
+_HOST_SEEN = {}
+_HOST_LOCKED = set()
+
+
+def _lock_in_place(arr: np.ndarray) -> None:
+    """Page-lock a caller's array in place (pb_host_register) on its second
+    use, so that its upload is an asynchronous DMA from then on, as from a
+    pinned tensor.  One use costs nothing extra; the lock is released when
+    the array is garbage-collected.  A failure (the range overlaps one
+    locked already, say) leaves the array pageable."""
+    if arr.nbytes < (1 << 18) or not arr.flags.c_contiguous:
+        return
+    key = (arr.ctypes.data, arr.nbytes)
+    if key in _HOST_LOCKED:
+        return
+    seen = _HOST_SEEN.get(key)
+    if seen is None or seen() is not arr:
+        _HOST_SEEN[key] = weakref.ref(arr)
+        return
+    del _HOST_SEEN[key]
+    lib = _engine()._lib
+    if lib.lib.pb_host_register(ctypes.c_void_p(key[0]), key[1]) != lib.PB_OK:
+        return
+    _HOST_LOCKED.add(key)
+    weakref.finalize(arr, _unlock, key)
+
+
+def _unlock(key) -> None:
+    if key in _HOST_LOCKED:
+        _HOST_LOCKED.discard(key)
+        try:
+            _engine()._lib.lib.pb_host_unregister(ctypes.c_void_p(key[0]))
+        except Exception:
+            pass
+
+
 def _pinned_copy(t: torch.Tensor) -> torch.Tensor:
     """An asynchronous copy of a device tensor into page-locked host memory
     (torch's pinned-memory cache), on the current stream."""
@@ -173,8 +213,14 @@ class IMPTDoseGrid(DoseGrid):
                             "resampling CT")
 
     def _rlsp_device(self, machine_name, device):
-        # an HU array in page-locked memory goes up asynchronously
-        hu_h = torch.from_numpy(np.ascontiguousarray(self.HU, dtype=np.single))
+        # an HU array in page-locked memory goes up asynchronously; a
+        # float32 array of the caller's is page-locked in place on its
+        # second use
+        hu_np = np.ascontiguousarray(self.HU, dtype=np.single)
+        hu_h = torch.from_numpy(hu_np)
+        if hu_np is self.HU and not hu_h.is_pinned():
+            _lock_in_place(hu_np)
+            hu_h = torch.from_numpy(hu_np)
         hu = hu_h.to(device, non_blocking=hu_h.is_pinned())
         xh, yh = _hu_curve(machine_name)
         rlsp = _engine().rlsp_from_hu(hu, xh, yh)

@@ -272,6 +272,15 @@ PbStatus pb_count_evaluated_adjoint(const PbGrid *grid, const PbBeam *beams, int
  * reference. */
 PbStatus pb_measure_ex2_rate(double *ops_per_s, void *stream);
 
+/* Page-lock an existing host range in place (cudaHostRegister), so that
+ * copies from it are asynchronous DMA, and release it again.  A failure
+ * leaves no pending CUDA error behind.  The range must stay allocated until
+ * it is unregistered, and no copy from it may be in flight then.  No
+ * counterpart in the reference (it copies from pageable memory on every
+ * call). */
+PbStatus pb_host_register(void *host_ptr, size_t bytes);
+PbStatus pb_host_unregister(void *host_ptr);
+
 /* Forward kernel shapes the autotuner chooses from, in two families:
  * "t<threads>_v<voxels per thread>_c<k>" works on 8x8x8 voxel tiles, each
  * thread evaluating its voxels one by one; "l8x<TY>x<TZ>_c<k>" works on

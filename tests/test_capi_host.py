@@ -141,6 +141,12 @@ def test_invalid_arguments_return_status_without_a_gpu():
     g = _lib.PbGrid(256, 256, 160, 2.0)
     n = L.pb_tile_order_count(ctypes.byref(g))
     assert n == 32 * 16 * 20                          # 8 x 16 x 8 voxel tiles
+    # page-locking a host range: NULL or empty ranges are refused without a
+    # CUDA call
+    assert L.pb_host_register(None, 4096) == _lib.PB_ERR_INVALID
+    buf = (ctypes.c_char * 4096)()
+    assert L.pb_host_register(buf, 0) == _lib.PB_ERR_INVALID
+    assert L.pb_host_unregister(None) == _lib.PB_ERR_INVALID
     tile = (ctypes.c_int * 3)()
     assert L.pb_tile_order_tile(tile) == _lib.PB_OK and list(tile) == [8, 16, 8]
     assert L.pb_tile_order_tile(None) == _lib.PB_ERR_INVALID

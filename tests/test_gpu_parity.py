@@ -610,6 +610,31 @@ def test_beam_at_a_time_forward_and_compute_plan(small):
     assert np.array_equal(g.dose.reshape(-1), want)
 
 
+def test_caller_hu_locked_in_place_on_second_use(pkg):
+    """computeIMPTPlan page-locks a caller's float32 HU array in place on its
+    second use (pb_host_register) and releases it when the array is
+    collected; the results do not change."""
+    import gc
+    from dosecuda_b200 import plan_impt
+    case = pkg[2].small_heterogeneous()
+    g, plan = case.grid, case.plan
+    hu = np.ascontiguousarray(g.HU, dtype=np.float32).copy()
+    g.HU = hu
+    key = (hu.ctypes.data, hu.nbytes)
+    assert hu.nbytes >= 1 << 18
+    g.computeIMPTPlan(plan, 0)
+    first = g.dose.copy()
+    assert key not in plan_impt._HOST_LOCKED and not torch.from_numpy(hu).is_pinned()
+    g.computeIMPTPlan(plan, 0)
+    assert key in plan_impt._HOST_LOCKED and torch.from_numpy(hu).is_pinned()
+    g.computeIMPTPlan(plan, 0)
+    assert np.array_equal(g.dose, first)
+    g.HU = hu.copy()
+    del hu
+    gc.collect()
+    assert key not in plan_impt._HOST_LOCKED
+
+
 def test_adjoint_counts_follow_its_tile_skip(small):
     """pb_count_evaluated_adjoint: on a field nonzero everywhere it counts
     the forward's work; on a zero field nothing; on a field nonzero in one
