@@ -318,83 +318,93 @@ class IMPTDoseGrid(DoseGrid):
         comp = self.__dict__.get("_pb_compute_stream")
         if comp is None or comp.device != device:
             comp = self._pb_compute_stream = torch.cuda.Stream(device)
-        for chunk in chunks:
-            if len(chunks) == 1:
-                # the WET is queued first; the spots are sorted into layers
-                # and uploaded on the copy stream while it runs
-                pool = self.__dict__.get("_pb_texture_pool")
-                if pool is None:
-                    pool = self._pb_texture_pool = _engine().TexturePool()
-                dp = _engine().DevicePlan(shape, float(self.spacing[0]),
-                                          np.asarray(self.origin, dtype=np.single),
-                                          self._specs(plan, chunk), device, texture_pool=pool,
-                                          defer_spots=True)
-                dp.compute_wet(rlsp.reshape(-1), check_status=False, wet_mode=wet_mode)
+        try:
+            for chunk in chunks:
+                if len(chunks) == 1:
+                    # the WET is queued first; the spots are sorted into layers
+                    # and uploaded on the copy stream while it runs
+                    pool = self.__dict__.get("_pb_texture_pool")
+                    if pool is None:
+                        pool = self._pb_texture_pool = _engine().TexturePool()
+                    dp = _engine().DevicePlan(shape, float(self.spacing[0]),
+                                              np.asarray(self.origin, dtype=np.single),
+                                              self._specs(plan, chunk), device, texture_pool=pool,
+                                              defer_spots=True)
+                    dp.compute_wet(rlsp.reshape(-1), check_status=False, wet_mode=wet_mode)
+                    with torch.cuda.stream(side):
+                        dp.load_spots()
+                    main.wait_stream(side)
+                else:
+                    dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
+                # one beam at a time, each in its own tile order, so that each
+                # beam's dose goes back to the host while the next is computed;
+                # the plan dose is the beams' float32 sum times n_fractions, as
+                # the reference forms it (plan_impt.py:201-206)
+                # The plan's last beam runs as two launches, the lower and the
+                # upper half of the z slabs of tiles, so that the lower half of
+                # its dose and of the plan dose go back during the second.
+                # The first beam's tile order on the main stream, the others'
+                # (and the last beam's z groups) on the copy stream while the
+                # first beam's dose is computed.  The plan's last beam runs as
+                # _TAIL_PARTS launches over groups of z slabs of tiles, so that
+                # only the last group's doses remain to be copied back after
+                # the last launch.
+                nb = dp.n_beams
+                final = chunk is chunks[-1]
+                bd = torch.empty((nb, V), dtype=torch.float32, device=device)
+                bd_h = torch.empty((nb, V), dtype=torch.float32, pin_memory=True)
+                dp.beam_tile_order(0)
+                side.wait_stream(main)
                 with torch.cuda.stream(side):
-                    dp.load_spots()
-                main.wait_stream(side)
-            else:
-                dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
-            # one beam at a time, each in its own tile order, so that each
-            # beam's dose goes back to the host while the next is computed;
-            # the plan dose is the beams' float32 sum times n_fractions, as
-            # the reference forms it (plan_impt.py:201-206)
-            # The plan's last beam runs as two launches, the lower and the
-            # upper half of the z slabs of tiles, so that the lower half of
-            # its dose and of the plan dose go back during the second.
-            # The first beam's tile order on the main stream, the others'
-            # (and the last beam's z groups) on the copy stream while the
-            # first beam's dose is computed.  The plan's last beam runs as
-            # _TAIL_PARTS launches over groups of z slabs of tiles, so that
-            # only the last group's doses remain to be copied back after
-            # the last launch.
-            nb = dp.n_beams
-            final = chunk is chunks[-1]
-            bd = torch.empty((nb, V), dtype=torch.float32, device=device)
-            bd_h = torch.empty((nb, V), dtype=torch.float32, pin_memory=True)
-            dp.beam_tile_order(0)
-            side.wait_stream(main)
-            with torch.cuda.stream(side):
-                for b in range(1, nb):
-                    dp.beam_tile_order(b)
-                parts = dp.beam_tile_order_parts(nb - 1, _TAIL_PARTS) if final else None
-                orders_ready = torch.cuda.Event()
-                orders_ready.record(side)
-            launches = [(b, None, 0, V) for b in range(nb)]
-            if final and len(parts) > 1:
-                launches[-1:] = [(nb - 1, o, v0, v1) for o, v0, v1 in parts]
-            # The launches alternate between two compute streams, so that a
-            # launch's last blocks share the SMs with the next launch's
-            # first ones; the copy stream adds each finished part into the
-            # plan dose, in beam order, and copies it back.
-            comp.wait_stream(main)
-            for idx, (b, order, v0, v1) in enumerate(launches):
-                st = main if idx % 2 == 0 else comp
-                if idx > 0 or order is not None:
-                    st.wait_event(orders_ready)
-                with torch.cuda.stream(st):
-                    dp.forward_beam(b, out=bd[b], order=order)
-                    done = torch.cuda.Event()
-                    done.record(st)
-                side.wait_event(done)
-                last = final and b == nb - 1
-                with torch.cuda.stream(side):
-                    d, db = dose[v0:v1], bd[b, v0:v1]
-                    if first_beam and b == 0:
-                        d.copy_(db)
-                    else:
-                        d.add_(db)
-                    if nf != 1.0:
-                        db.mul_(nf)
+                    for b in range(1, nb):
+                        dp.beam_tile_order(b)
+                    parts = dp.beam_tile_order_parts(nb - 1, _TAIL_PARTS) if final else None
+                    orders_ready = torch.cuda.Event()
+                    orders_ready.record(side)
+                launches = [(b, None, 0, V) for b in range(nb)]
+                if final and len(parts) > 1:
+                    launches[-1:] = [(nb - 1, o, v0, v1) for o, v0, v1 in parts]
+                # The launches alternate between two compute streams, so that a
+                # launch's last blocks share the SMs with the next launch's
+                # first ones; the copy stream adds each finished part into the
+                # plan dose, in beam order, and copies it back.
+                comp.wait_stream(main)
+                for idx, (b, order, v0, v1) in enumerate(launches):
+                    st = main if idx % 2 == 0 else comp
+                    if idx > 0 or order is not None:
+                        st.wait_event(orders_ready)
+                    with torch.cuda.stream(st):
+                        dp.forward_beam(b, out=bd[b], order=order)
+                        done = torch.cuda.Event()
+                        done.record(st)
+                    side.wait_event(done)
+                    last = final and b == nb - 1
+                    with torch.cuda.stream(side):
+                        d, db = dose[v0:v1], bd[b, v0:v1]
+                        if first_beam and b == 0:
+                            d.copy_(db)
+                        else:
+                            d.add_(db)
+                        if nf != 1.0:
+                            db.mul_(nf)
+                            if last:
+                                d.mul_(nf)
+                        bd_h[b, v0:v1].copy_(db, non_blocking=True)
                         if last:
-                            d.mul_(nf)
-                    bd_h[b, v0:v1].copy_(db, non_blocking=True)
-                    if last:
-                        dose_h[v0:v1].copy_(d, non_blocking=True)
-            first_beam = False
-            main.wait_stream(comp)
-            beams_h.append((bd_h, nb))
-            keep += [bd, dp]
+                            dose_h[v0:v1].copy_(d, non_blocking=True)
+                first_beam = False
+                main.wait_stream(comp)
+                beams_h.append((bd_h, nb))
+                keep += [bd, dp]
+        except BaseException:
+            # nothing queued may still use this call's buffers once they
+            # are released
+            for st in (main, comp, side):
+                try:
+                    st.synchronize()
+                except Exception:
+                    pass
+            raise
         main.synchronize()
         side.synchronize()
         if len(chunks) == 1 and int(dp._status.item()) & _engine()._lib.PB_ERR_RAY_CAP:
