@@ -141,6 +141,37 @@ class TexturePool:
         self.close()
 
 
+def split_order_by_slabs(order: torch.Tensor, dims, tile, n_parts: int):
+    """A tile order (a permutation of the raster tile indices, x fastest, for
+    a grid of dims = (nx, ny, nz) voxels in tiles of tile = (tx, ty, tz)
+    voxels) split into up to n_parts groups of whole z slabs of tiles,
+    lowest z first: a list of (order, v0, v1).  Each order keeps the group's
+    tiles in their given order and is padded with -1 to the full count; it
+    covers exactly voxels v0 <= v < v1 (z varies slowest).  Stream-ordered
+    on the order's device."""
+    nx, ny, nz = (int(v) for v in dims)
+    per_slab = -(-nx // int(tile[0])) * -(-ny // int(tile[1]))
+    n_slabs = -(-nz // int(tile[2]))
+    n_parts = max(1, min(int(n_parts), n_slabs))
+    if n_parts == 1:
+        return [(order, 0, nx * ny * nz)]
+    # group of slab tz: tz * n_parts // n_slabs (non-decreasing in tz)
+    group = (order // per_slab) * n_parts // n_slabs
+    ranked = order[torch.sort(group, stable=True).indices]
+    pad = torch.full((order.numel(),), -1, dtype=order.dtype, device=order.device)
+    parts, t0, z0 = [], 0, 0
+    for p in range(n_parts):
+        z1 = z0
+        while z1 < n_slabs and z1 * n_parts // n_slabs == p:
+            z1 += 1
+        t1 = t0 + (z1 - z0) * per_slab
+        part = torch.cat([ranked[t0:t1], pad[:order.numel() - (t1 - t0)]])
+        parts.append((part, nx * ny * min(z0 * int(tile[2]), nz),
+                      nx * ny * min(z1 * int(tile[2]), nz)))
+        t0, z0 = t1, z1
+    return parts
+
+
 class DevicePlan:
     """A plan prepared on one GPU (see module docstring)."""
 
@@ -395,26 +426,8 @@ class DevicePlan:
         order = self.beam_tile_order(b)
         tile = (ctypes.c_int * 3)()
         check(_lib.lib.pb_tile_order_tile(tile), "pb_tile_order_tile")
-        nx, ny, nz = self.grid.nx, self.grid.ny, self.grid.nz
-        per_slab = -(-nx // tile[0]) * -(-ny // tile[1])
-        n_slabs = -(-nz // tile[2])
-        n_parts = max(1, min(int(n_parts), n_slabs))
-        if n_parts == 1:
-            return [(order, 0, self.n_vox)]
-        # group of slab tz: tz * n_parts // n_slabs (non-decreasing in tz)
-        group = (order // per_slab) * n_parts // n_slabs
-        ranked = order[torch.sort(group, stable=True).indices]
-        pad = torch.full((order.numel(),), -1, dtype=order.dtype, device=order.device)
-        parts, t0, z0 = [], 0, 0
-        for p in range(n_parts):
-            z1 = z0
-            while z1 < n_slabs and z1 * n_parts // n_slabs == p:
-                z1 += 1
-            t1 = t0 + (z1 - z0) * per_slab
-            part = torch.cat([ranked[t0:t1], pad[:order.numel() - (t1 - t0)]])
-            parts.append((part, nx * ny * min(z0 * tile[2], nz), nx * ny * min(z1 * tile[2], nz)))
-            t0, z0 = t1, z1
-        return parts
+        return split_order_by_slabs(order, (self.grid.nx, self.grid.ny, self.grid.nz),
+                                    tuple(tile), n_parts)
 
     def forward_beam(self, b: int, mu_sorted: Optional[torch.Tensor] = None,
                      scale: float = 1.0, out: Optional[torch.Tensor] = None,

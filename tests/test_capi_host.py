@@ -230,3 +230,41 @@ def test_smoothing_table_rejects_bad_arguments():
         _lib.smooth_table((10, 10, 10), 2.0, [geom], 1)
     with pytest.raises(_lib.PbError):
         _lib.smooth_table((10, 0, 10), 2.0, [geom], 0)
+
+
+@pytest.mark.parametrize("dims,n_parts", [((256, 256, 160), 4), ((56, 48, 40), 2),
+                                          ((56, 48, 40), 9), ((20, 17, 7), 4),
+                                          ((33, 40, 41), 3)])
+def test_tile_order_split_by_z_slabs(dims, n_parts):
+    """The split computeIMPTPlan uses for a plan's last beam: groups of whole
+    z slabs of tiles, in the given order within each group, -1 padded, each
+    covering exactly its voxel range (host logic, CPU tensors)."""
+    import torch
+    from dosecuda_b200.engine import split_order_by_slabs
+    tile = (8, 16, 8)
+    nx, ny, nz = dims
+    tx, ty, tz = (-(-nx // tile[0]), -(-ny // tile[1]), -(-nz // tile[2]))
+    n = tx * ty * tz
+    order = torch.randperm(n, generator=torch.Generator().manual_seed(n)).to(torch.int32)
+    parts = split_order_by_slabs(order, dims, tile, n_parts)
+    assert len(parts) == min(n_parts, tz)
+    assert parts[0][1] == 0 and parts[-1][2] == nx * ny * nz
+    seen = []
+    for (o, v0, v1), nxt in zip(parts, parts[1:] + [None]):
+        assert o.numel() == n and o.dtype == torch.int32
+        listed = o[o >= 0]
+        assert bool((o[listed.numel():] == -1).all())
+        # the group's tiles in the order's own sequence
+        pos = torch.empty(n, dtype=torch.long)
+        pos[order.long()] = torch.arange(n)
+        assert bool((pos[listed.long()].diff() > 0).all()) if listed.numel() > 1 else True
+        # exactly the tiles whose z slab lies in [v0, v1)
+        slabs = listed // (tx * ty)
+        assert v0 == nx * ny * min(int(slabs.min()) * tile[2], nz)
+        assert v1 == nx * ny * min((int(slabs.max()) + 1) * tile[2], nz)
+        assert listed.numel() == (int(slabs.max()) - int(slabs.min()) + 1) * tx * ty
+        if nxt is not None:
+            assert nxt[1] == v1
+        seen.append(listed)
+    allt = torch.cat(seen).sort().values
+    assert torch.equal(allt, torch.arange(n, dtype=torch.int32))
