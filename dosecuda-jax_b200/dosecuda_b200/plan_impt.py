@@ -336,16 +336,13 @@ class IMPTDoseGrid(DoseGrid):
                     main.wait_stream(side)
                 else:
                     dp = self._transient(plan, gpu_id, chunk, wet_mode, rlsp)
-                # one beam at a time, each in its own tile order, so that each
+                # One beam at a time, each in its own tile order, so that each
                 # beam's dose goes back to the host while the next is computed;
                 # the plan dose is the beams' float32 sum times n_fractions, as
-                # the reference forms it (plan_impt.py:201-206)
-                # The plan's last beam runs as two launches, the lower and the
-                # upper half of the z slabs of tiles, so that the lower half of
-                # its dose and of the plan dose go back during the second.
-                # The first beam's tile order on the main stream, the others'
-                # (and the last beam's z groups) on the copy stream while the
-                # first beam's dose is computed.  The plan's last beam runs as
+                # the reference forms it (plan_impt.py:201-206).  The first
+                # beam's tile order on the main stream, the others' (and the
+                # last beam's z groups) on the copy stream while the first
+                # beam's dose is computed.  The plan's last beam runs as
                 # _TAIL_PARTS launches over groups of z slabs of tiles, so that
                 # only the last group's doses remain to be copied back after
                 # the last launch.
