@@ -151,6 +151,9 @@ def _lock_in_place(arr: np.ndarray) -> None:
         return
     seen = _HOST_SEEN.get(key)
     if seen is None or seen() is not arr:
+        if len(_HOST_SEEN) >= 64:   # forget arrays that are gone
+            for k in [k for k, r in _HOST_SEEN.items() if r() is None]:
+                del _HOST_SEEN[k]
         _HOST_SEEN[key] = weakref.ref(arr)
         return
     del _HOST_SEEN[key]
