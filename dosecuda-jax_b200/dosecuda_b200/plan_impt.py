@@ -109,8 +109,10 @@ class IMPTBeamModel():
 
 _HU_CURVES = {}
 
-# launches of a plan's last beam in computeIMPTPlan (groups of z slabs)
+# launches of a plan's last beam in computeIMPTPlan (groups of z slabs), and
+# of each other beam (splitting those too measured slower)
 _TAIL_PARTS = 4
+_BEAM_PARTS = 1
 
 
 def _hu_curve(machine_name):
@@ -356,14 +358,17 @@ class IMPTDoseGrid(DoseGrid):
                 dp.beam_tile_order(0)
                 side.wait_stream(main)
                 with torch.cuda.stream(side):
-                    for b in range(1, nb):
+                    launches = []
+                    for b in range(nb):
+                        k = _TAIL_PARTS if final and b == nb - 1 else _BEAM_PARTS
                         dp.beam_tile_order(b)
-                    parts = dp.beam_tile_order_parts(nb - 1, _TAIL_PARTS) if final else None
+                        if k > 1:
+                            launches += [(b, o, v0, v1)
+                                         for o, v0, v1 in dp.beam_tile_order_parts(b, k)]
+                        else:
+                            launches.append((b, None, 0, V))
                     orders_ready = torch.cuda.Event()
                     orders_ready.record(side)
-                launches = [(b, None, 0, V) for b in range(nb)]
-                if final and len(parts) > 1:
-                    launches[-1:] = [(nb - 1, o, v0, v1) for o, v0, v1 in parts]
                 # The launches alternate between two compute streams, so that a
                 # launch's last blocks share the SMs with the next launch's
                 # first ones; the copy stream adds each finished part into the
